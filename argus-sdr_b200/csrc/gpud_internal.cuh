@@ -1,0 +1,170 @@
+// gpud_internal.cuh -- device-side data layout and helpers shared by the
+// sm_100a kernels of libgpudemod_kernels.so.
+//
+// Layout in HBM (one runner):
+//   ChanParams[max_ch]   per-slot constants (written by the host on admit/update)
+//   ChanState [max_ch]   per-slot state carried across blocks (device-resident)
+//   taps arena           per slot: extraction taps, phase-major p*L+u, zero-padded
+//   history arena        per slot: 2 ping-pong buffers of HCAP shifted samples
+//   WFM arenas           per slot: 100-sample delay lines of the composite,
+//                        L-R and mono-audio filters, RDS shifted history
+//   per-block buffers    extracted IQ, composite, pilot/bpf/lpr/lr work arrays
+//   output arena         results table | audio | RDS | emitted IQ (one D2H)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#ifndef GPUD_PI
+#define GPUD_PI 3.14159265358979323846
+#endif
+
+namespace gpud {
+
+// ---------------------------------------------------------------------------
+// NCO phase as an unsigned Q0.64 fraction of a turn.  Sample i of a block has
+// phase u0 + i*inc (mod 2^64) exactly, so a block's per-sample phases are
+// computed in parallel with no accumulated rounding, and the carried phase
+// never drifts.  (The reference carries float64 radians and adds the
+// increment sample by sample, streaming_host_core.go:56-61; the two agree to
+// ~1e-10 rad per 2^20 samples, far below float32 resolution of the rotator.)
+// ---------------------------------------------------------------------------
+__host__ __device__ inline uint64_t rad_to_q64(double rad) {
+    double t = rad * (1.0 / (2.0 * GPUD_PI));
+    t -= floor(t);  // [0, 1)
+    double s = t * 4294967296.0;
+    double hi = floor(s);
+    double lo = (s - hi) * 4294967296.0;
+    uint64_t h = (uint64_t)hi;
+    uint64_t l = (uint64_t)lo;
+    return (h << 32) + l;
+}
+
+// Phase in [-pi, pi) radians (float64) of a Q0.64 turn count.
+__host__ __device__ inline double q64_to_rad(uint64_t q) {
+    int64_t s = (int64_t)q;  // two's complement: [-2^63, 2^63) <-> [-0.5, 0.5) turn
+    return (double)s * (2.0 * GPUD_PI / 18446744073709551616.0);
+}
+
+// Unit phasor exp(j*2*pi*q/2^64) in float32.  sincospif on the signed top 32
+// bits: argument resolution 2^-31 half-turns, result within ~1 ulp.
+__device__ __forceinline__ float2 q64_phasor(uint64_t q) {
+    int32_t top = (int32_t)(q >> 32);
+    float x = (float)top * 4.656612873077393e-10f;  // 2^-31 -> half-turns in [-1, 1)
+    float s, c;
+    sincospif(x, &s, &c);
+    return make_float2(c, s);
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// ---------------------------------------------------------------------------
+// Per-slot constants
+// ---------------------------------------------------------------------------
+struct ChanParams {
+    uint64_t inc_q;   // NCO increment (Q0.64 turns per input sample)
+    double inc_rad;   // -2*pi*offset/fs
+    int32_t decim;    // D
+    int32_t ntaps;    // T (taps applied)
+    int32_t nphase;   // P = min(D, T): phases carrying taps
+    int32_t plen;     // L = ceil(T / D)
+    int32_t mode;     // GPUD_MODE_*
+    int32_t flags;    // GPUD_CH_*
+    int32_t out_rate;
+    int32_t taps_off; // float offset into the taps arena (phase-major P*L)
+    int32_t dtaps_off;// float offset of the direct-form taps h[0..T-1]
+    int32_t hist_off; // float2 offset of the history pair (2 * hcap)
+    int32_t hcap;     // history capacity (>= T-1)
+    int32_t wfm_idx;  // index into WFM arenas (-1 when not WFM)
+    int32_t rds_dr;   // RDS decimation floor(out_rate/19000)
+    int32_t pad0;
+    double ssb_inc;   // 2*pi*(+-700)/out_rate for USB/LSB/CW
+    double pll_alpha, pll_beta, pll_lpa;   // stereo PLL constants
+    double pll_fmin, pll_fmax;             // freq clamp (rad/sample)
+    double rds_inc;                        // 2*pi*57000/out_rate
+    int32_t rds_tab;                       // binade table id for the RDS phase
+    int32_t pad1;
+};
+
+// Per-slot state carried across blocks.
+struct ChanState {
+    uint64_t nco_q;      // NCO phase at the start of the next block
+    float2 last_iq;      // discriminator bridge sample
+    int32_t has_last;
+    int32_t pad0;
+    // stereo pilot PLL (recorder/streamer.go:1560-1619)
+    double pll_phase, pll_freq, pll_i, pll_q, err_avg;
+    int32_t on_count, off_count, enabled, locked;
+    float coherence, pilot_hz, last_err_avg, pad1;
+    // RDS baseband stream
+    int64_t rds_count;   // composite samples consumed
+    int32_t rds_hist_len;
+    int32_t pad2;
+};
+
+// Per-block per-slot descriptor (host-built; all integer bookkeeping is
+// mirrored on the host, so output sizes are known before launch).
+struct SlotBlock {
+    int32_t slot;
+    int32_t pc;        // phase count before the block
+    int32_t n_out;     // extraction outputs this block
+    int32_t hist_len;  // history length before the block
+    int32_t hist_sel;  // ping-pong buffer holding the current history
+    int32_t ext_off;   // float2 offset of this slot's extracted IQ
+    int32_t n_disc;    // discriminator outputs
+    int32_t bridge;    // 1: first output uses last_iq
+    int32_t comp_off;  // float offset of composite/work arrays
+    int32_t audio_off; // float offset into the audio output region
+    int32_t n_audio;   // floats written to audio
+    int32_t rds_off;   // float2 offset into the RDS output region
+    int32_t n_rds;
+    int32_t rds_first; // first composite index of this block that is kept (-1: none)
+    int32_t comp_hist_len; // valid samples in the composite delay line (<= 100)
+    int32_t res_idx;   // index into the results table
+};
+
+// Results table row written by the device each block.
+struct DevResult {
+    double nco_phase;
+    int32_t flags;
+    float coherence, pilot_hz, err_avg;
+    int32_t status;
+    int32_t pad[3];
+};
+
+// Exact sequential float64 accumulation x_k = fl(x_{k-1} + inc), x_0 = 0
+// (dsp.FreqShift's `phase += inc`, dsp/freqshift.go:13-15), evaluated in
+// closed form per binade: inside one binade every value is a multiple of the
+// binade's ulp, so the rounded step is a constant multiple of that ulp and
+// x_k = x_start + (k - k_start) * q exactly.  The host builds the table by
+// walking binade boundaries with the same float64 additions.
+struct BinadeEntry {
+    int64_t k_start;  // first index covered by this entry
+    double x_start;   // x_{k_start}
+    double q;         // exact step inside the entry
+};
+constexpr int kMaxBinades = 96;
+struct BinadeTable {
+    int32_t count;
+    int32_t pad;
+    BinadeEntry e[kMaxBinades];
+};
+
+__device__ __forceinline__ double binade_value(const BinadeTable &t, int64_t k) {
+    int lo = 0, hi = t.count - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (t.e[mid].k_start <= k) lo = mid; else hi = mid - 1;
+    }
+    const BinadeEntry &b = t.e[lo];
+    return b.x_start + (double)(k - b.k_start) * b.q;
+}
+
+constexpr int kWfmTaps = 101;      // stereo / RDS filter length (streamer.go:1531-1545, fm.go:155)
+constexpr int kWfmHist = 100;
+
+}  // namespace gpud
+
+// Kernel launch accounting (host side).
+extern "C" void gpud_count_launch(int n);

@@ -1,0 +1,738 @@
+// runner_kernels.cu -- sm_100a kernels of the batched / serving runner.
+//
+// One IQ block flows through, in stream order:
+//   k_extract_dense<L> / k_extract_wide   NCO + polyphase FIR + decimation
+//   k_demod, k_am                         FM discriminator (with bridge), SSB/CW, AM
+//   k_wfm_fir                             stereo FIR bank: L+R, L-R band, pilot band
+//   k_pll                                 19 kHz pilot PLL, L-R product, lock decision
+//   k_wfm_out                             L-R 15 kHz LPF and L/R matrix, or mono fallback
+//   k_rds                                 57 kHz RDS baseband (exact FreqShift phase)
+//   k_post                                per-slot state carry (histories, phases)
+// Every kernel takes a work list of (slot-block index, tile) pairs so channels
+// with uneven taps / decimation run in the same launch.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gpud_internal.cuh"
+
+namespace gpud {
+
+// ===========================================================================
+// Extraction: NCO shift -> FIR -> decimate  (streaming_host_core.go:5-64)
+// ===========================================================================
+//
+// Output j of a block takes the input sample n_j = (D - pc - 1) + j*D as its
+// newest sample (exports.cu:583) and y_j = sum_{k<T} h[k] * s(n_j - k), where
+// s(i) = x[i] * exp(j*phi_i) for i >= 0 and the carried shifted history for
+// i < 0 (zero before the stream start).
+//
+// Dense form (L = ceil(T/D) >= 2): the rotated samples of a tile are staged in
+// shared memory transposed into the D polyphase components,
+//     Z[p][m] = s(s0 + m*D - p),   p < D,
+// so that y_j = sum_p sum_u h[p + u*D] * Z[p][j - u].  Warp w owns the phases
+// p = w, w+8, ...; each lane owns R = 8 consecutive outputs and keeps a
+// register window of R + L - 1 samples per phase (R*L FMAs per R+L-1 shared
+// loads).  A row stride padded by one slot every 8 keeps the lane-strided
+// window loads free of bank conflicts.  The 8 warps' partial sums are reduced
+// through shared memory at the end.
+constexpr int kDenseR = 8;
+constexpr int kDenseOT = 32 * kDenseR;  // outputs per tile
+constexpr int kDenseThreads = 256;
+
+__host__ __device__ inline int dense_row_stride(int L) {
+    int M = kDenseOT + L - 1;
+    return M + (M >> 3) + 1;
+}
+
+__host__ __device__ inline int dense_smem_bytes(int P, int L) {
+    int z = P * dense_row_stride(L) * 8;
+    int red = 8 * (kDenseOT + kDenseOT / 8) * 8;
+    int a = z > red ? z : red;
+    return a + P * L * 4 + 16;
+}
+
+__device__ __forceinline__ float2 shifted_sample(int i, int n, const float2 *__restrict__ x, uint64_t u0,
+                                                 uint64_t inc, const float2 *__restrict__ hist, int H) {
+    if (i >= 0) {
+        if (i >= n) return make_float2(0.f, 0.f);
+        return cmulf(__ldg(x + i), q64_phasor(u0 + (uint64_t)i * inc));
+    }
+    int hi = H + i;
+    return hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
+}
+
+template <int L>
+__global__ void __launch_bounds__(kDenseThreads, 2)
+k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+                const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+                const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
+                float2 *__restrict__ ext) {
+    constexpr int R = kDenseR;
+    extern __shared__ float4 smem4[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int j0 = w.y * kDenseOT;
+    if (j0 >= sb.n_out) return;
+    const ChanParams &cp = prm[sb.slot];
+    const int D = cp.decim;
+    const int P = cp.nphase;
+    const int M = kDenseOT + L - 1;
+    const int Mp = dense_row_stride(L);
+    float2 *Z = reinterpret_cast<float2 *>(smem4);
+    const int zbytes = dense_smem_bytes(P, L) - P * L * 4 - 16;
+    float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smem4) + zbytes);
+
+    const float *tg = taps_arena + cp.taps_off;
+    for (int i = threadIdx.x; i < P * L; i += kDenseThreads) tsm[i] = tg[i];
+
+    const int s0 = D - sb.pc - 1;
+    const int m_base = j0 - (L - 1);
+    const uint64_t u0 = st[sb.slot].nco_q;
+    const uint64_t inc = cp.inc_q;
+    const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+    const int H = sb.hist_len;
+    const float invP = 1.0f / (float)P;
+    const int total = P * M;
+    for (int f = threadIdx.x; f < total; f += kDenseThreads) {
+        int mr = (int)(((float)f + 0.5f) * invP);
+        int p = f - mr * P;
+        int i = s0 + (m_base + mr) * D - p;
+        Z[p * Mp + mr + (mr >> 3)] = shifted_sample(i, n, x, u0, inc, hist, H);
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float ar[R], ai[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
+    for (int p = warp; p < P; p += 8) {
+        const float2 *zrow = Z + p * Mp;
+        float2 win[R + L - 1];
+#pragma unroll
+        for (int t = 0; t < R + L - 1; ++t) {
+            int c = lane * R + t;
+            win[t] = zrow[c + (c >> 3)];
+        }
+        float h[L];
+#pragma unroll
+        for (int u = 0; u < L; ++u) h[u] = tsm[p * L + u];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+#pragma unroll
+            for (int u = 0; u < L; ++u) {
+                float2 z = win[r + L - 1 - u];
+                ar[r] = fmaf(h[u], z.x, ar[r]);
+                ai[r] = fmaf(h[u], z.y, ai[r]);
+            }
+        }
+    }
+    __syncthreads();
+    constexpr int RS = kDenseOT + kDenseOT / 8;
+    float2 *red = Z;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        int o = lane * R + r;
+        red[warp * RS + o + (o >> 3)] = make_float2(ar[r], ai[r]);
+    }
+    __syncthreads();
+    {
+        int o = threadIdx.x;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int wv = 0; wv < 8; ++wv) {
+            float2 v = red[wv * RS + o + (o >> 3)];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        int j = j0 + o;
+        if (j < sb.n_out) ext[sb.ext_off + j] = s;
+    }
+}
+
+// Wide form (short polyphase arms, or tiles too large for shared memory): one
+// warp per output, lanes stride the taps, warp-shuffle reduction.
+constexpr int kWideOPW = 4;                  // outputs per warp
+constexpr int kWideOT = 8 * kWideOPW;        // outputs per 256-thread tile
+
+__global__ void __launch_bounds__(256)
+k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+               const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+               const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
+               float2 *__restrict__ ext) {
+    extern __shared__ float smemf[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int j0 = w.y * kWideOT;
+    if (j0 >= sb.n_out) return;
+    const ChanParams &cp = prm[sb.slot];
+    const int T = cp.ntaps, D = cp.decim;
+    for (int i = threadIdx.x; i < T; i += 256) smemf[i] = taps_arena[cp.dtaps_off + i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s0 = D - sb.pc - 1;
+    const uint64_t u0 = st[sb.slot].nco_q;
+    const uint64_t inc = cp.inc_q;
+    const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+    const int H = sb.hist_len;
+    for (int o = 0; o < kWideOPW; ++o) {
+        int j = j0 + warp * kWideOPW + o;
+        if (j >= sb.n_out) break;
+        int nj = s0 + j * D;
+        float ar = 0.f, ai = 0.f;
+        for (int k = lane; k < T; k += 32) {
+            float2 v = shifted_sample(nj - k, n, x, u0, inc, hist, H);
+            float h = smemf[k];
+            ar = fmaf(h, v.x, ar);
+            ai = fmaf(h, v.y, ai);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            ar += __shfl_xor_sync(0xffffffffu, ar, off);
+            ai += __shfl_xor_sync(0xffffffffu, ai, off);
+        }
+        if (lane == 0) ext[sb.ext_off + j] = make_float2(ar, ai);
+    }
+}
+
+// ===========================================================================
+// Demodulators (internal/demod/*.go; bridge per recorder/streamer.go:1287-1302)
+// ===========================================================================
+constexpr int kDemodOT = 1024;
+
+__global__ void __launch_bounds__(256)
+k_demod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+        const ChanState *__restrict__ st, const float2 *__restrict__ ext, float *__restrict__ comp,
+        float *__restrict__ audio) {
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const int q0 = w.y * kDemodOT;
+    const float2 *iq = ext + sb.ext_off;
+    const int mode = cp.mode;
+    if (mode == 1 || mode == 2 || mode == 3) {  // NFM / WFM / WFM_STEREO: fmDiscrimInto (fm.go:179-196)
+        const float2 last = st[sb.slot].last_iq;
+        float *dst = (mode == 1) ? (audio + sb.audio_off) : (comp + sb.comp_off);
+        for (int q = q0 + threadIdx.x; q < q0 + kDemodOT && q < sb.n_disc; q += blockDim.x) {
+            float2 p, c;
+            if (sb.bridge) {
+                p = q == 0 ? last : iq[q - 1];
+                c = iq[q];
+            } else {
+                p = iq[q];
+                c = iq[q + 1];
+            }
+            double num = (double)p.x * (double)c.y - (double)p.y * (double)c.x;
+            double den = (double)p.x * (double)c.x + (double)p.y * (double)c.y;
+            dst[q] = (float)atan2(num, den);
+        }
+    } else if (mode == 5 || mode == 6 || mode == 7) {  // ssb.go:19-39, cw.go:11-26
+        float *dst = audio + sb.audio_off;
+        for (int q = q0 + threadIdx.x; q < q0 + kDemodOT && q < sb.n_out; q += blockDim.x) {
+            double ph = (double)(q + 1) * cp.ssb_inc;
+            double s, c;
+            sincos(ph, &s, &c);
+            float2 v = iq[q];
+            dst[q] = (mode == 7) ? (float)((double)v.x * c) : (float)((double)v.x * c - (double)v.y * s);
+        }
+    }
+}
+
+// AM.Demod (am.go:11-27): envelope minus the per-call mean.  One CTA per slot.
+__global__ void __launch_bounds__(256)
+k_am(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const float2 *__restrict__ ext,
+     float *__restrict__ audio) {
+    __shared__ double red[256];
+    const SlotBlock sb = sbt[work[blockIdx.x].x];
+    const float2 *iq = ext + sb.ext_off;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < sb.n_out; q += 256) acc += hypot((double)iq[q].x, (double)iq[q].y);
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    const float mean = (float)(red[0] / (double)sb.n_out);
+    float *dst = audio + sb.audio_off;
+    for (int q = threadIdx.x; q < sb.n_out; q += 256) {
+        float mag = (float)hypot((double)iq[q].x, (double)iq[q].y);
+        dst[q] = mag - mean;
+    }
+}
+
+// ===========================================================================
+// WFM multiplex (recorder/streamer.go:1525-1644)
+// ===========================================================================
+//
+// Rate-class tables: the stereo filters as float taps padded to 104
+//   x = LPF 15 kHz (L+R and L-R lowpass), y = LPF 53 kHz - LPF 23 kHz (L-R
+//   band), z = LPF 21 kHz - LPF 17 kHz (pilot band); the band-pass pairs are
+//   differenced in float64 before rounding, one filter each instead of two;
+// and the RDS lowpass (7.5 kHz, fm.go:155) in float64.
+constexpr int kWfmTapsPad = 104;
+struct WfmTaps {
+    float4 t[kWfmTapsPad];
+    double rds[kWfmTaps];
+};
+
+// Composite-rate work arrays (all float, same offsets comp_off):
+//   work + 0*W comp (discriminator output), 1*W lpr, 2*W bpf, 3*W pilot, 4*W lr
+constexpr int kFirOT = 1024;   // composite samples per tile
+constexpr int kAudioDlStride = kWfmHist + 4;  // 100 samples + valid count
+constexpr int kFirThreads = 128;  // 8 outputs each
+
+__host__ __device__ constexpr int padi(int e) { return e + (e >> 3); }
+
+// Loads composite samples [q0-104, q0+kFirOT) into shared memory; indices
+// below 0 come from the 100-sample delay line `dl` (oldest first, newest at
+// 99) with `valid` trailing entries, zero before that.
+__device__ __forceinline__ void stage_window(float *win, const float *__restrict__ src, int q0, int nvalid,
+                                             const float *__restrict__ dl, int valid) {
+    for (int i = threadIdx.x; i < kFirOT + kWfmTapsPad; i += blockDim.x) {
+        int q = q0 - kWfmTapsPad + i;
+        float v = 0.f;
+        if (q >= 0) {
+            if (q < nvalid) v = src[q];
+        } else if (q >= -valid) {
+            v = dl[kWfmHist + q];
+        }
+        win[padi(i)] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kFirThreads)
+k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+          const WfmTaps *__restrict__ taps, float *__restrict__ wk, int W, const float *__restrict__ comp_dl) {
+    __shared__ float win[padi(kFirOT + kWfmTapsPad) + 8];
+    __shared__ float4 tp[kWfmTapsPad];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const int q0 = w.y * kFirOT;
+    if (q0 >= sb.n_disc) return;
+    const WfmTaps &tb = taps[cp.rds_tab];
+    for (int i = threadIdx.x; i < kWfmTapsPad; i += kFirThreads) tp[i] = tb.t[i];
+    const float *comp = wk + sb.comp_off;
+    stage_window(win, comp, q0, sb.n_disc, comp_dl + cp.wfm_idx * kWfmHist, sb.comp_hist_len);
+    __syncthreads();
+    const int t = threadIdx.x;
+    // window index of composite sample q0 + 8t + r - k is 8t + r - k + 104
+    const int base = 8 * t + kWfmTapsPad;
+    float a[8], b[8], c[8], ring[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) a[r] = b[r] = c[r] = 0.f;
+#pragma unroll
+    for (int j = 1; j < 8; ++j) ring[j] = win[padi(base + j)];
+    for (int kb = 0; kb < kWfmTapsPad; kb += 8) {
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            const int k = kb + kk;
+            ring[(8 - kk) & 7] = win[padi(base - k)];
+            const float4 h = tp[k];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float v = ring[(r - kk + 8) & 7];
+                a[r] = fmaf(h.x, v, a[r]);
+                b[r] = fmaf(h.y, v, b[r]);
+                c[r] = fmaf(h.z, v, c[r]);
+            }
+        }
+    }
+    float *lpr = wk + 1 * W + sb.comp_off, *bpf = wk + 2 * W + sb.comp_off, *pil = wk + 3 * W + sb.comp_off;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        int q = q0 + 8 * t + r;
+        if (q < sb.n_disc) {
+            lpr[q] = a[r];
+            bpf[q] = b[r];
+            pil[q] = c[r];
+        }
+    }
+}
+
+// Pilot PLL, serial per channel (one lane per WFM_STEREO slot).  Phase,
+// frequency and the I/Q lowpass states are float64 (the frequency integrator
+// moves by ~1e-10 rad/sample, below float32 resolution); the loop's sin/cos and
+// atan2 are float32.  Writes lr = bpf * float32(2 sin(2 phase)) and the
+// per-call lock decision with its hysteresis (streamer.go:1363-1380,1615-1635).
+__global__ void __launch_bounds__(32)
+k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
+      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W) {
+    const int idx = blockIdx.x * 32 + threadIdx.x;
+    if (idx >= count) return;
+    const SlotBlock sb = sbt[list[idx]];
+    const int n = sb.n_disc;
+    if (n <= 0) return;
+    const ChanParams &cp = prm[sb.slot];
+    ChanState &s = st[sb.slot];
+    const float *pil = wk + 3 * W + sb.comp_off;
+    const float *bpf = wk + 2 * W + sb.comp_off;
+    float *lr = wk + 4 * W + sb.comp_off;
+    double ph = s.pll_phase, fr = s.pll_freq, I = s.pll_i, Q = s.pll_q;
+    const double alpha = cp.pll_alpha, beta = cp.pll_beta, lpa = cp.pll_lpa;
+    const double fmin = cp.pll_fmin, fmax = cp.pll_fmax;
+    const double twopi = 2.0 * GPUD_PI;
+    double pp = 0.0, es = 0.0;
+    for (int q = 0; q < n; ++q) {
+        const double p = (double)pil[q];
+        const float bq = bpf[q];
+        float sf, cf;
+        __sincosf((float)(ph - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sin/-cos(ph - pi)
+        const double cp_ = -(double)cf, sp_ = -(double)sf;
+        I += lpa * (p * cp_ - I);
+        Q += lpa * (p * -sp_ - Q);
+        const double err = (double)atan2f((float)Q, (float)I);
+        fr += beta * err;
+        fr = fr < fmin ? fmin : (fr > fmax ? fmax : fr);
+        ph += fr + alpha * err;
+        if (ph > twopi) ph -= twopi;
+        else if (ph < 0.0) ph += twopi;
+        pp += p * p;
+        es += fabs(err);
+        double t2 = 2.0 * ph;  // [0, 4pi]
+        t2 -= twopi * rint(t2 * (1.0 / twopi));
+        lr[q] = bq * (2.0f * sinf((float)t2));
+    }
+    s.pll_phase = ph;
+    s.pll_freq = fr;
+    s.pll_i = I;
+    s.pll_q = Q;
+    const double block_err = es / (double)n;
+    const double ea = 0.9 * s.err_avg + 0.1 * block_err;
+    s.err_avg = ea;
+    double coherence = 0.0;
+    if (pp > 1e-12) coherence = (I * I + Q * Q) * (double)n / pp;
+    const double fhz = fr * (double)cp.out_rate / twopi;
+    const int locked = coherence > 0.15 && fabs(fhz - 19000.0) < 250.0 && ea < 0.35;
+    s.locked = locked;
+    s.coherence = (float)coherence;
+    s.pilot_hz = (float)fhz;
+    s.last_err_avg = (float)ea;
+    if (locked) {
+        s.on_count += 1;
+        s.off_count = 0;
+        if (s.on_count >= 4) s.enabled = 1;
+    } else {
+        s.on_count = 0;
+        s.off_count += 1;
+        if (s.off_count >= 10) s.enabled = 0;
+    }
+}
+
+// L-R lowpass and L/R matrix when stereo is enabled; otherwise the 15 kHz mono
+// fallback filter (its own delay line, advanced only on fallback blocks) duplicated
+// to both channels.  WFM (mono) mode always takes the mono filter, one channel.
+__global__ void __launch_bounds__(kFirThreads)
+k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+          const ChanState *__restrict__ st, const WfmTaps *__restrict__ taps, const float *__restrict__ wk, int W,
+          const float *__restrict__ lr_dl, const float *__restrict__ audio_dl, float *__restrict__ audio) {
+    __shared__ float win[padi(kFirOT + kWfmTapsPad) + 8];
+    __shared__ float tp[kWfmTapsPad];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const int q0 = w.y * kFirOT;
+    if (q0 >= sb.n_disc) return;
+    const bool stereo = (cp.mode == 3) && st[sb.slot].enabled;
+    const WfmTaps &tb = taps[cp.rds_tab];
+    for (int i = threadIdx.x; i < kWfmTapsPad; i += kFirThreads) tp[i] = tb.t[i].x;
+    if (stereo) {
+        stage_window(win, wk + 4 * W + sb.comp_off, q0, sb.n_disc, lr_dl + cp.wfm_idx * kWfmHist,
+                     sb.comp_hist_len);
+    } else {
+        // The fallback filter's delay line holds composite samples of earlier
+        // fallback blocks only; its valid count sits after the 100 samples.
+        const float *adl = audio_dl + cp.wfm_idx * kAudioDlStride;
+        stage_window(win, wk + sb.comp_off, q0, sb.n_disc, adl, __float_as_int(adl[kWfmHist]));
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int base = 8 * t + kWfmTapsPad;
+    float a[8], ring[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) a[r] = 0.f;
+#pragma unroll
+    for (int j = 1; j < 8; ++j) ring[j] = win[padi(base + j)];
+    for (int kb = 0; kb < kWfmTapsPad; kb += 8) {
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            const int k = kb + kk;
+            ring[(8 - kk) & 7] = win[padi(base - k)];
+            const float h = tp[k];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) a[r] = fmaf(h, ring[(r - kk + 8) & 7], a[r]);
+        }
+    }
+    float *dst = audio + sb.audio_off;
+    if (cp.mode == 2) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            int q = q0 + 8 * t + r;
+            if (q < sb.n_disc) dst[q] = a[r];
+        }
+    } else if (stereo) {
+        const float *lpr = wk + 1 * W + sb.comp_off;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            int q = q0 + 8 * t + r;
+            if (q < sb.n_disc) {
+                float l = lpr[q];
+                dst[2 * q] = 0.5f * (l + a[r]);
+                dst[2 * q + 1] = 0.5f * (l - a[r]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            int q = q0 + 8 * t + r;
+            if (q < sb.n_disc) {
+                dst[2 * q] = a[r];
+                dst[2 * q + 1] = a[r];
+            }
+        }
+    }
+}
+
+// RDS baseband (fm.go:143-163 / 234-271) over the continuous discriminator
+// stream: cplx[g] = disc[g] * exp(j x_{g+1}) with x the exact sequential
+// float64 FreqShift phase, a 101-tap lowpass accumulated in float64 in the
+// reference's order (separate multiply and add, as Go's amd64 code does), and
+// every Dr-th stream sample kept.
+constexpr int kRdsOT = 64;
+
+__global__ void __launch_bounds__(128)
+k_rds(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+      const ChanState *__restrict__ st, const WfmTaps *__restrict__ taps, const BinadeTable *__restrict__ tabs,
+      const float *__restrict__ wk, const float2 *__restrict__ rds_dl, float2 *__restrict__ rds_out) {
+    extern __shared__ float2 cpl[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int r0 = w.y * kRdsOT;
+    if (r0 >= sb.n_rds) return;
+    const ChanParams &cp = prm[sb.slot];
+    const int dr = cp.rds_dr;
+    const int r1 = min(r0 + kRdsOT, sb.n_rds);
+    const int qlo = sb.rds_first + r0 * dr - (kWfmTaps - 1);
+    const int qhi = sb.rds_first + (r1 - 1) * dr;
+    const int span = qhi - qlo + 1;
+    const ChanState &s = st[sb.slot];
+    const int64_t c0 = s.rds_count;
+    const BinadeTable &tab = tabs[cp.rds_tab];
+    const float *comp = wk + sb.comp_off;
+    const float2 *dl = rds_dl + cp.wfm_idx * kWfmHist;
+    for (int i = threadIdx.x; i < span; i += blockDim.x) {
+        int q = qlo + i;
+        float2 v = make_float2(0.f, 0.f);
+        if (q >= 0) {
+            double ph = binade_value(tab, c0 + q + 1);
+            double sn, cs;
+            sincos(ph, &sn, &cs);
+            double b = (double)comp[q];
+            v = make_float2((float)(b * cs), (float)(b * sn));
+        } else if (q >= -s.rds_hist_len) {
+            v = dl[kWfmHist + q];
+        }
+        cpl[i] = v;
+    }
+    __syncthreads();
+    const WfmTaps &tb = taps[cp.rds_tab];
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        const int qr = sb.rds_first + r * dr;
+        const int li = qr - qlo;
+        double ar = 0.0, ai = 0.0;
+        for (int k = 0; k < kWfmTaps; ++k) {
+            const float2 v = cpl[li - k];
+            ar = __dadd_rn(ar, __dmul_rn((double)v.x, tb.rds[k]));
+            ai = __dadd_rn(ai, __dmul_rn((double)v.y, tb.rds[k]));
+        }
+        rds_out[sb.rds_off + r] = make_float2((float)ar, (float)ai);
+    }
+}
+
+// ===========================================================================
+// Per-slot state carry, one CTA per slot, after every other kernel.
+// ===========================================================================
+__device__ void shift_delay_line(float *dl, const float *__restrict__ src, int n) {
+    // dl: 100 floats oldest-first; append src[0..n) and keep the last 100.
+    __shared__ float tmp[kWfmHist];
+    for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) {
+        int g = n + i - kWfmHist;  // index into (dl ++ src) shifted so dl occupies [-100, 0)
+        tmp[i] = g >= 0 ? src[g] : dl[kWfmHist + g];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) dl[i] = tmp[i];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(128)
+k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
+       const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, const float2 *__restrict__ ext,
+       const float *__restrict__ wk, int W, float *__restrict__ comp_dl, float *__restrict__ lr_dl,
+       float *__restrict__ audio_dl, float2 *__restrict__ rds_dl, const BinadeTable *__restrict__ tabs,
+       DevResult *__restrict__ res) {
+    const SlotBlock sb = sbt[blockIdx.x];
+    const ChanParams &cp = prm[sb.slot];
+    ChanState &s = st[sb.slot];
+    const uint64_t u0 = s.nco_q;
+    // extraction history: last min(T-1, H+n) samples of (history ++ shifted block)
+    {
+        const int keep = cp.ntaps - 1;
+        const int H = sb.hist_len;
+        const int newH = min(keep, H + n);
+        const float2 *hold = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+        float2 *hnew = hist_arena + cp.hist_off + (1 - sb.hist_sel) * cp.hcap;
+        for (int q = threadIdx.x; q < newH; q += blockDim.x) {
+            int g = H + n - newH + q;
+            hnew[q] = g < H ? hold[g] : cmulf(__ldg(x + (g - H)), q64_phasor(u0 + (uint64_t)(g - H) * cp.inc_q));
+        }
+    }
+    __syncthreads();
+    if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
+        const float *comp = wk + sb.comp_off;
+        const bool fallback = (cp.mode == 2) || !s.enabled;
+        if (fallback) {
+            float *adl = audio_dl + cp.wfm_idx * kAudioDlStride;
+            int valid = __float_as_int(adl[kWfmHist]);
+            shift_delay_line(adl, comp, sb.n_disc);
+            if (threadIdx.x == 0) adl[kWfmHist] = __int_as_float(min(kWfmHist, valid + sb.n_disc));
+            __syncthreads();
+        }
+        if (cp.mode == 3) shift_delay_line(lr_dl + cp.wfm_idx * kWfmHist, wk + 4 * W + sb.comp_off, sb.n_disc);
+        // RDS shifted history: the last 100 values of cplx over the stream
+        if (cp.flags & 2) {
+            __shared__ float2 rtmp[kWfmHist];
+            const BinadeTable &tab = tabs[cp.rds_tab];
+            float2 *dl = rds_dl + cp.wfm_idx * kWfmHist;
+            const int64_t c0 = s.rds_count;
+            for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) {
+                int q = sb.n_disc + i - kWfmHist;
+                float2 v = make_float2(0.f, 0.f);
+                if (q >= 0) {
+                    double ph = binade_value(tab, c0 + q + 1);
+                    double sn, cs;
+                    sincos(ph, &sn, &cs);
+                    double b = (double)comp[q];
+                    v = make_float2((float)(b * cs), (float)(b * sn));
+                } else {
+                    v = dl[kWfmHist + q];
+                }
+                rtmp[i] = v;
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) dl[i] = rtmp[i];
+            __syncthreads();
+        }
+        shift_delay_line(comp_dl + cp.wfm_idx * kWfmHist, comp, sb.n_disc);
+    }
+    if (threadIdx.x == 0) {
+        s.nco_q = u0 + (uint64_t)n * cp.inc_q;
+        if (sb.n_out > 0) {
+            s.last_iq = ext[sb.ext_off + sb.n_out - 1];
+            s.has_last = 1;
+        }
+        if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
+            s.rds_count += sb.n_disc;
+            s.rds_hist_len = (int)min((int64_t)kWfmHist, s.rds_count);
+        }
+        DevResult &o = res[sb.res_idx];
+        o.nco_phase = q64_to_rad(s.nco_q);
+        o.flags = (cp.mode == 3 && sb.n_disc > 0) ? ((s.locked ? 1 : 0) | (s.enabled ? 2 : 0))
+                                                  : (s.enabled ? 2 : 0);
+        o.coherence = s.coherence;
+        o.pilot_hz = s.pilot_hz;
+        o.err_avg = s.last_err_avg;
+        o.status = 0;
+    }
+}
+
+// ===========================================================================
+// launch helpers (host)
+// ===========================================================================
+template <int L>
+static cudaError_t launch_dense_L(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                  const float2 *hist, const float *taps, float2 *ext) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_extract_dense<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        attr_set = true;
+    }
+    k_extract_dense<L><<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract_dense(int L, int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                 const float2 *hist, const float *taps, float2 *ext) {
+    switch (L) {
+#define GPUD_CASE(LL) \
+    case LL: return launch_dense_L<LL>(grid, smem, sm, work, sbt, prm, st, x, n, hist, taps, ext);
+        GPUD_CASE(2) GPUD_CASE(3) GPUD_CASE(4) GPUD_CASE(5) GPUD_CASE(6) GPUD_CASE(7) GPUD_CASE(8)
+        GPUD_CASE(9) GPUD_CASE(10) GPUD_CASE(11) GPUD_CASE(12) GPUD_CASE(13) GPUD_CASE(14)
+        GPUD_CASE(15) GPUD_CASE(16)
+#undef GPUD_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                const float2 *hist, const float *taps, float2 *ext) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_extract_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        attr_set = true;
+    }
+    k_extract_wide<<<grid, 256, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_demod(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                         const ChanState *st, const float2 *ext, float *comp, float *audio) {
+    k_demod<<<grid, 256, 0, sm>>>(work, sbt, prm, st, ext, comp, audio);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_am(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const float2 *ext,
+                      float *audio) {
+    k_am<<<grid, 256, 0, sm>>>(work, sbt, ext, audio);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                           const WfmTaps *taps, float *wk, int W, const float *comp_dl) {
+    k_wfm_fir<<<grid, kFirThreads, 0, sm>>>(work, sbt, prm, taps, wk, W, comp_dl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
+                       ChanState *st, float *wk, int W) {
+    k_pll<<<(count + 31) / 32, 32, 0, sm>>>(list, count, sbt, prm, st, wk, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                           const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
+                           const float *audio_dl, float *audio) {
+    k_wfm_out<<<grid, kFirThreads, 0, sm>>>(work, sbt, prm, st, taps, wk, W, lr_dl, audio_dl, audio);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                       const ChanParams *prm, const ChanState *st, const WfmTaps *taps, const BinadeTable *tabs,
+                       const float *wk, const float2 *rds_dl, float2 *rds_out) {
+    k_rds<<<grid, 128, smem, sm>>>(work, sbt, prm, st, taps, tabs, wk, rds_dl, rds_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                        const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, int W,
+                        float *comp_dl, float *lr_dl, float *audio_dl, float2 *rds_dl, const BinadeTable *tabs,
+                        DevResult *res) {
+    k_post<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, W, comp_dl, lr_dl, audio_dl, rds_dl, tabs, res);
+    return cudaGetLastError();
+}
+
+int rds_smem_bytes(int dr) { return (kRdsOT * dr + kWfmTaps + 8) * 8; }
+
+}  // namespace gpud

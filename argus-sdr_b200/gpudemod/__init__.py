@@ -1,0 +1,304 @@
+"""gpudemod -- Python mirror of the reference's Go package
+`internal/demod/gpudemod` over libgpudemod_kernels.so.
+
+Same names and argument meaning as the Go API (gpudemod.go, batch_runner.go,
+streaming_types.go, streaming_gpu_stub.go), so tests read like the
+reference's own: `NewBatchRunner(maxSamples, sampleRate)`,
+`runner.StreamingExtractGPU(iq, jobs)`, `ExactIntegerDecimation`, ...  Plus
+`ChannelRunner`, the batched / serving runner (admit / retire / process_block
+/ results / stats / snapshot).
+
+All compute runs in the CUDA library; nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import ChannelResult, ChannelSpec, RunnerStats, lib
+
+# DemodType (gpudemod.go:69-76) -> runner modes
+DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
+MODE_IQ, MODE_NFM, MODE_WFM, MODE_WFM_STEREO, MODE_AM, MODE_USB, MODE_LSB, MODE_CW = range(8)
+MODE_BY_NAME = {"IQ": MODE_IQ, "NFM": MODE_NFM, "WFM": MODE_WFM, "WFM_STEREO": MODE_WFM_STEREO, "AM": MODE_AM,
+                "USB": MODE_USB, "LSB": MODE_LSB, "CW": MODE_CW}
+CH_EMIT_IQ, CH_RDS = 1, 2
+SCHED_BATCHED, SCHED_PLAIN = 0, 1
+
+E_ARG, E_DECIM, E_TAPS, E_BUDGET, E_SLOTS, E_SLOT, E_BLOCK, E_TIMEOUT, E_CUDA, E_MODE, E_DEVICE_STATUS, E_STATE = \
+    -20, -21, -22, -23, -24, -25, -26, -27, -28, -29, -30, -31
+
+
+class ErrUnavailable(RuntimeError):
+    """gpudemod.ErrUnavailable (errors.go)."""
+
+
+class GPUDError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gpudemod error {code}: {msg}")
+        self.code = code
+
+
+def Available() -> bool:
+    """gpudemod.Available (gpudemod.go:95-101)."""
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        return False
+
+
+def ExactIntegerDecimation(sample_rate: int, out_rate: int) -> int:
+    """cpu_oracle.go:155-163."""
+    if sample_rate <= 0 or out_rate <= 0:
+        raise ValueError(f"invalid sampleRate/outRate: {sample_rate}/{out_rate}")
+    if sample_rate % out_rate != 0:
+        raise ValueError(f"streaming polyphase extractor requires integer decimation: "
+                         f"sampleRate={sample_rate} outRate={out_rate}")
+    return sample_rate // out_rate
+
+
+def StreamingConfigHash(signal_id: int, offset_hz: float, bandwidth: float, out_rate: int, num_taps: int,
+                        sample_rate: int) -> int:
+    """streaming_types.go:58-72 (offset and bandwidth are not hashed)."""
+    return int(lib.gpud_streaming_config_hash(int(signal_id), int(out_rate), int(num_taps), int(sample_rate)))
+
+
+def BuildPolyphaseTapsPhaseMajor(base, decim: int) -> np.ndarray:
+    """polyphase.go:6-20: out[p*L + k] = base[p + k*D], L = ceil(len/D)."""
+    base = np.asarray(base, dtype=np.float32)
+    if decim <= 0 or base.size == 0:
+        return np.zeros(0, np.float32)
+    L = (base.size + decim - 1) // decim
+    out = np.zeros(decim * L, np.float32)
+    for p in range(decim):
+        src = p + decim * np.arange(L)
+        ok = src < base.size
+        out[p * L: p * L + L][ok] = base[src[ok]]
+    return out
+
+
+@dataclass
+class StreamingExtractJob:
+    SignalID: int
+    OffsetHz: float
+    Bandwidth: float
+    OutRate: int
+    NumTaps: int
+    ConfigHash: int
+
+
+@dataclass
+class StreamingExtractResult:
+    SignalID: int
+    IQ: np.ndarray
+    Rate: int
+    NOut: int
+    PhaseCount: int
+    HistoryLen: int
+    NCOPhase: float = 0.0
+
+
+def _check(r, rc: int):
+    if rc != 0:
+        msg = lib.gpud_runner_last_error(r).decode() if r else ""
+        raise GPUDError(rc, msg)
+
+
+def _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash=0, mode=MODE_IQ, flags=0) -> ChannelSpec:
+    return ChannelSpec(int(signal_id), float(offset_hz), float(bandwidth), int(out_rate), int(num_taps),
+                       int(config_hash) & ((1 << 64) - 1), int(mode), int(flags))
+
+
+def _iq_ptr(iq):
+    """(pointer, n, on_device, keepalive) for numpy (host) or torch (host or cuda)."""
+    try:
+        import torch
+        if isinstance(iq, torch.Tensor):
+            t = iq.contiguous()
+            if t.dtype != torch.complex64:
+                t = t.to(torch.complex64)
+            return t.data_ptr(), t.numel(), 1 if t.is_cuda else 0, t
+    except ImportError:  # pragma: no cover
+        pass
+    a = np.ascontiguousarray(iq, dtype=np.complex64)
+    return (a.ctypes.data if a.size else None), a.size, 0, a
+
+
+class ChannelRunner:
+    """Batched / serving runner (gpud_runner_*): device-resident channel slots,
+    one launch sequence per IQ block for all channels."""
+
+    def __init__(self, sample_rate: int, max_block: int, max_channels: int = 64, max_taps: int = 1024,
+                 device_mem_budget: int = 0):
+        self._r = C.c_void_p()
+        rc = lib.gpud_runner_create(int(sample_rate), int(max_block), int(max_channels), int(max_taps),
+                                    int(device_mem_budget), C.byref(self._r))
+        if rc != 0:
+            raise GPUDError(rc, "gpud_runner_create failed")
+        self.sample_rate = sample_rate
+        self.max_block = max_block
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if self._r:
+            lib.gpud_runner_destroy(self._r)
+            self._r = C.c_void_p()
+
+    Close = close
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, signal_id, offset_hz, bandwidth, out_rate, num_taps=101, mode=MODE_IQ, flags=0,
+              config_hash=0) -> int:
+        slot = C.c_int()
+        spec = _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash, mode, flags)
+        _check(self._r, lib.gpud_runner_admit(self._r, C.byref(spec), C.byref(slot)))
+        return slot.value
+
+    def footprint(self, out_rate, mode=MODE_IQ, flags=0, num_taps=101) -> int:
+        b = C.c_uint64()
+        spec = _spec(0, 0, 0, out_rate, num_taps, 0, mode, flags)
+        _check(self._r, lib.gpud_runner_channel_footprint(self._r, C.byref(spec), C.byref(b)))
+        return b.value
+
+    def retire(self, slot: int):
+        _check(self._r, lib.gpud_runner_retire(self._r, int(slot)))
+
+    def update(self, slot: int, offset_hz: float, bandwidth: float):
+        _check(self._r, lib.gpud_runner_update(self._r, int(slot), float(offset_hz), float(bandwidth)))
+
+    def set_schedule(self, schedule: int):
+        _check(self._r, lib.gpud_runner_set_schedule(self._r, int(schedule)))
+
+    # -- blocks ------------------------------------------------------------
+    def process_block(self, iq):
+        ptr, n, dev, keep = _iq_ptr(iq)
+        _check(self._r, lib.gpud_runner_process_block(self._r, ptr, n, dev))
+        del keep
+
+    def submit(self, iq) -> int:
+        ptr, n, dev, keep = _iq_ptr(iq)
+        t = C.c_uint64()
+        _check(self._r, lib.gpud_runner_submit(self._r, ptr, n, dev, C.byref(t)))
+        self._keep = keep
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 10000):
+        _check(self._r, lib.gpud_runner_wait(self._r, int(ticket), int(timeout_ms)))
+
+    def result(self, slot: int) -> dict:
+        res = ChannelResult()
+        _check(self._r, lib.gpud_runner_result(self._r, int(slot), C.byref(res)))
+
+        def arr(ptr, n, dt, width):
+            if not ptr or n <= 0:
+                return np.zeros(0, dt)
+            buf = (C.c_float * (n * width)).from_address(C.addressof(ptr.contents))
+            return np.frombuffer(buf, dtype=np.float32).view(dt).copy()
+
+        return {
+            "signal_id": res.signal_id,
+            "rate": res.rate,
+            "n_iq": res.n_iq,
+            "phase_count": res.phase_count,
+            "history_len": res.history_len,
+            "nco_phase": res.nco_phase,
+            "iq": arr(res.iq, res.n_iq, np.complex64, 2),
+            "audio": arr(res.audio, res.n_audio, np.float32, 1),
+            "audio_channels": res.audio_channels,
+            "rds": arr(res.rds, res.n_rds, np.complex64, 2),
+            "rds_rate": res.rds_rate,
+            "locked": bool(res.flags & 1),
+            "stereo": bool(res.flags & 2),
+            "coherence": res.coherence,
+            "pilot_hz": res.pilot_hz,
+            "err_avg": res.err_avg,
+        }
+
+    def stats(self) -> dict:
+        s = RunnerStats()
+        _check(self._r, lib.gpud_runner_stats_get(self._r, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in RunnerStats._fields_}
+
+    def stream_handle(self) -> int:
+        h = C.c_void_p()
+        _check(self._r, lib.gpud_runner_stream(self._r, C.byref(h)))
+        return h.value or 0
+
+    def snapshot(self, slot: int) -> bytes:
+        n = C.c_uint64()
+        _check(self._r, lib.gpud_runner_snapshot(self._r, int(slot), None, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(self._r, lib.gpud_runner_snapshot(self._r, int(slot), buf, C.byref(n)))
+        return buf.raw[: n.value]
+
+    def restore(self, slot: int, blob: bytes):
+        buf = C.create_string_buffer(blob, len(blob))
+        _check(self._r, lib.gpud_runner_restore(self._r, int(slot), buf, len(blob)))
+
+    # -- BatchRunner.StreamingExtractGPU ----------------------------------
+    def streaming_extract(self, iq, jobs):
+        a = np.ascontiguousarray(iq, dtype=np.complex64)
+        specs = (ChannelSpec * max(1, len(jobs)))()
+        for i, j in enumerate(jobs):
+            specs[i] = _spec(j.SignalID, j.OffsetHz, j.Bandwidth, j.OutRate, j.NumTaps, j.ConfigHash)
+        results = (ChannelResult * max(1, len(jobs)))()
+        cap = sum(a.size // max(1, self.sample_rate // max(1, j.OutRate)) + 2 for j in jobs) + 16
+        out = np.zeros(cap, np.complex64)
+        rc = lib.gpud_runner_streaming_extract(self._r, a.ctypes.data if a.size else None, a.size, specs,
+                                               len(jobs), results, out.ctypes.data, cap)
+        _check(self._r, rc)
+        outs, pos = [], 0
+        for i, j in enumerate(jobs):
+            r = results[i]
+            iqo = out[pos: pos + r.n_iq].copy()
+            pos += r.n_iq
+            outs.append(StreamingExtractResult(j.SignalID, iqo, r.rate, r.n_iq, r.phase_count, r.history_len,
+                                               r.nco_phase))
+        return outs
+
+
+class BatchRunner:
+    """gpudemod.BatchRunner (batch_runner.go:12-98) -- streaming extraction
+    keyed by SignalID with per-signal state on the device."""
+
+    def __init__(self, max_samples: int, sample_rate: int, max_channels: int = 256, max_taps: int = 1024):
+        self._cr = ChannelRunner(sample_rate, max(1, max_samples), max_channels, max_taps)
+        self.sampleRate = sample_rate
+
+    def StreamingExtractGPU(self, iq_new, jobs):
+        """streaming_gpu_stub.go:21-26."""
+        if self._cr is None:
+            raise ErrUnavailable("gpudemod batch runner unavailable")
+        return self._cr.streaming_extract(iq_new, jobs)
+
+    StreamingExtractGPUExec = StreamingExtractGPU
+
+    def ResetSignalState(self, signal_id: int):
+        """stream_state.go:9-16: forget one signal (its next job starts fresh)."""
+        _check(self._cr._r, lib.gpud_runner_reset_signal(self._cr._r, int(signal_id)))
+
+    def ResetAllSignalStates(self):
+        """stream_state.go:18-24."""
+        _check(self._cr._r, lib.gpud_runner_reset_all_signals(self._cr._r))
+
+    def Close(self):
+        if self._cr is not None:
+            self._cr.close()
+            self._cr = None
+
+
+def NewBatchRunner(max_samples: int, sample_rate: int) -> BatchRunner:
+    """batch_runner.go:23-35."""
+    return BatchRunner(max_samples, sample_rate)
+
+
+def kernel_launch_count() -> int:
+    return int(lib.gpud_kernel_launch_count())

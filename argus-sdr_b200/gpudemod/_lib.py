@@ -1,0 +1,140 @@
+"""ctypes binding of libgpudemod_kernels.so (include/gpudemod.h).
+
+The library is the product; this module only declares its C ABI for Python
+callers.  There is no fallback: if the shared library is missing or cannot be
+loaded, importing raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+_PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_ROOT, "libgpudemod_kernels.so")
+HEADER_PATH = os.path.join(os.path.dirname(_PKG_ROOT), "include", "gpudemod.h")
+
+
+class GPUDFloat2(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class ChannelSpec(C.Structure):
+    """gpud_channel_spec: StreamingExtractJob (streaming_types.go:8-15) + mode."""
+    _fields_ = [
+        ("signal_id", C.c_int64),
+        ("offset_hz", C.c_double),
+        ("bandwidth", C.c_double),
+        ("out_rate", C.c_int32),
+        ("num_taps", C.c_int32),
+        ("config_hash", C.c_uint64),
+        ("mode", C.c_int32),
+        ("flags", C.c_int32),
+    ]
+
+
+class ChannelResult(C.Structure):
+    _fields_ = [
+        ("signal_id", C.c_int64),
+        ("rate", C.c_int32),
+        ("n_iq", C.c_int32),
+        ("phase_count", C.c_int32),
+        ("history_len", C.c_int32),
+        ("nco_phase", C.c_double),
+        ("n_audio", C.c_int32),
+        ("audio_channels", C.c_int32),
+        ("n_rds", C.c_int32),
+        ("rds_rate", C.c_int32),
+        ("flags", C.c_int32),
+        ("coherence", C.c_float),
+        ("pilot_hz", C.c_float),
+        ("err_avg", C.c_float),
+        ("iq", C.POINTER(GPUDFloat2)),
+        ("audio", C.POINTER(C.c_float)),
+        ("rds", C.POINTER(GPUDFloat2)),
+    ]
+
+
+class RunnerStats(C.Structure):
+    _fields_ = [
+        ("blocks", C.c_uint64),
+        ("active_channels", C.c_int32),
+        ("max_channels", C.c_int32),
+        ("device_bytes_used", C.c_uint64),
+        ("device_bytes_budget", C.c_uint64),
+        ("last_block_ms", C.c_double),
+        ("p50_block_ms", C.c_double),
+        ("p99_block_ms", C.c_double),
+        ("kernel_launches", C.c_uint64),
+        ("graph_rebuilds", C.c_int32),
+    ]
+
+
+def _declare(lib: C.CDLL) -> C.CDLL:
+    P, i, d = C.c_void_p, C.c_int, C.c_double
+    pi = C.POINTER(C.c_int)
+    pd = C.POINTER(C.c_double)
+    sig = {
+        # legacy (native/exports.cu)
+        "gpud_stream_create": (i, [C.POINTER(P)]),
+        "gpud_stream_destroy": (i, [P]),
+        "gpud_stream_sync": (i, [P]),
+        "gpud_launch_freq_shift_stream_cuda": (i, [P, P, i, d, d, P]),
+        "gpud_launch_freq_shift_cuda": (i, [P, P, i, d, d]),
+        "gpud_launch_fm_discrim_cuda": (i, [P, P, i]),
+        "gpud_upload_fir_taps_cuda": (i, [P, i]),
+        "gpud_launch_fir_cuda": (i, [P, P, i, i]),
+        "gpud_launch_fir_stream_cuda": (i, [P, P, i, i, P]),
+        "gpud_launch_fir_v2_stream_cuda": (i, [P, P, P, i, i, P]),
+        "gpud_launch_decimate_cuda": (i, [P, P, i, i]),
+        "gpud_launch_decimate_stream_cuda": (i, [P, P, i, i, P]),
+        "gpud_launch_am_envelope_cuda": (i, [P, P, i]),
+        "gpud_launch_ssb_product_cuda": (i, [P, P, i, d, d]),
+        "gpud_launch_streaming_polyphase_prepare_cuda": (
+            i, [P, i, P, i, P, i, i, i, i, d, d, P, pi, pi, pd, P]),
+        "gpud_launch_streaming_polyphase_stateful_cuda": (
+            i, [P, i, P, P, i, i, i, P, P, i, pi, pi, pd, d, P, i, pi]),
+        # runner
+        "gpud_runner_create": (i, [i, i, i, i, C.c_uint64, C.POINTER(P)]),
+        "gpud_runner_destroy": (i, [P]),
+        "gpud_runner_admit": (i, [P, C.POINTER(ChannelSpec), pi]),
+        "gpud_runner_retire": (i, [P, i]),
+        "gpud_runner_update": (i, [P, i, d, d]),
+        "gpud_runner_set_schedule": (i, [P, i]),
+        "gpud_runner_channel_footprint": (i, [P, C.POINTER(ChannelSpec), C.POINTER(C.c_uint64)]),
+        "gpud_runner_process_block": (i, [P, P, i, i]),
+        "gpud_runner_submit": (i, [P, P, i, i, C.POINTER(C.c_uint64)]),
+        "gpud_runner_wait": (i, [P, C.c_uint64, i]),
+        "gpud_runner_result": (i, [P, i, C.POINTER(ChannelResult)]),
+        "gpud_runner_stats_get": (i, [P, C.POINTER(RunnerStats)]),
+        "gpud_runner_stream": (i, [P, C.POINTER(P)]),
+        "gpud_runner_last_error": (C.c_char_p, [P]),
+        "gpud_runner_snapshot": (i, [P, i, P, C.POINTER(C.c_uint64)]),
+        "gpud_runner_restore": (i, [P, i, P, C.c_uint64]),
+        "gpud_runner_streaming_extract": (i, [P, P, i, C.POINTER(ChannelSpec), i, C.POINTER(ChannelResult), P, i]),
+        "gpud_runner_reset_signal": (i, [P, C.c_int64]),
+        "gpud_runner_reset_all_signals": (i, [P]),
+        "gpud_streaming_config_hash": (C.c_uint64, [C.c_int64, i, i, i]),
+        "gpud_kernel_launch_count": (C.c_uint64, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def header_symbols(path: str = HEADER_PATH) -> list[str]:
+    """Every function the public header declares."""
+    txt = open(path).read()
+    return sorted(set(re.findall(r"GPUD_CALL\s+(gpud_\w+)\s*\(", txt)))
+
+
+def load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C argus-sdr_b200` "
+                          f"(or __graft_entry__.build()); there is no non-CUDA fallback")
+    return _declare(C.CDLL(LIB_PATH))
+
+
+lib = load()

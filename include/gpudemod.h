@@ -1,0 +1,284 @@
+/*
+ * gpudemod.h -- C ABI of libgpudemod_kernels.so, the B200 (sm_100a)
+ * implementation of Argus SDR's per-signal extraction and demod runner.
+ *
+ * Part 1 is the drop-in for the reference's `gpudemod_kernels` library: the
+ * sixteen `gpud_*` entry points of internal/demod/gpudemod/native/exports.cu
+ * with identical C signatures and return codes (0 ok; n<=0 is a no-op that
+ * returns 0; positive = cudaError_t; negative = argument error).  The Linux
+ * cgo preamble of the reference (internal/demod/gpudemod/gpudemod.go:33-39)
+ * binds seven of them; the Windows loader (windows_bridge.go:56-82) resolves
+ * all sixteen.
+ *
+ * Part 2 is the batched / serving runner that replaces the reference's
+ * per-signal Go loop (BatchRunner.StreamingExtractGPU ->
+ * executeStreamingGPUNativePrepared, streaming_gpu_native_prepare.go:17-108)
+ * with one device-resident channel table, one fused launch sequence per IQ
+ * block captured in a CUDA graph, and the demod chain (FM discriminator,
+ * AM, SSB, CW, WFM stereo with pilot PLL, RDS baseband) on the device.
+ * Its return-code space extends the reference's with new negative codes only
+ * (GPUD_E_*), none reused with another meaning.
+ *
+ * All device pointers are plain CUDA device pointers; host pointers are
+ * marked `host`.  No torch types cross this boundary.
+ */
+#ifndef GPUDEMOD_H
+#define GPUDEMOD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define GPUD_API __declspec(dllexport)
+#define GPUD_CALL __stdcall
+#else
+#define GPUD_API __attribute__((visibility("default")))
+#define GPUD_CALL
+#endif
+
+/* exports.cu:4-12 and gpudemod.go:10 (`gpud_float2`), exports.cu:12
+ * (`gpud_stream_handle`). */
+typedef struct {
+    float x;
+    float y;
+} gpud_float2;
+typedef void *gpud_stream_handle;
+
+/* ======================================================================== */
+/* Part 1: reference entry points (native/exports.cu)                        */
+/* ======================================================================== */
+
+/* exports.cu:18-25 -- create a CUDA stream; -1 on a null out pointer. */
+GPUD_API int GPUD_CALL gpud_stream_create(gpud_stream_handle *out);
+/* exports.cu:27-30 */
+GPUD_API int GPUD_CALL gpud_stream_destroy(gpud_stream_handle stream);
+/* exports.cu:32-35 -- a null stream synchronizes the device. */
+GPUD_API int GPUD_CALL gpud_stream_sync(gpud_stream_handle stream);
+
+/* exports.cu:37-76 -- out[i] = in[i] * exp(j*(phase_start + i*phase_inc)). */
+GPUD_API int GPUD_CALL gpud_launch_freq_shift_stream_cuda(const gpud_float2 *in, gpud_float2 *out, int n,
+                                                          double phase_inc, double phase_start,
+                                                          gpud_stream_handle stream);
+/* exports.cu:78-85 (legacy default stream); also kernels.cu:26-37. */
+GPUD_API int GPUD_CALL gpud_launch_freq_shift_cuda(const gpud_float2 *in, gpud_float2 *out, int n,
+                                                   double phase_inc, double phase_start);
+
+/* exports.cu:87-112 -- out[i] = arg(conj(in[i]) * in[i+1]), n-1 outputs. */
+GPUD_API int GPUD_CALL gpud_launch_fm_discrim_cuda(const gpud_float2 *in, float *out, int n);
+
+/* exports.cu:169-173 -- process-global taps for gpud_launch_fir[_stream]_cuda;
+ * -1 unless 1 <= n <= 256. */
+GPUD_API int GPUD_CALL gpud_upload_fir_taps_cuda(const float *taps, int n);
+/* exports.cu:175-186 -- complex x real FIR, zero history, n outputs. */
+GPUD_API int GPUD_CALL gpud_launch_fir_cuda(const gpud_float2 *in, gpud_float2 *out, int n, int num_taps);
+/* exports.cu:188-196 */
+GPUD_API int GPUD_CALL gpud_launch_fir_stream_cuda(const gpud_float2 *in, gpud_float2 *out, int n, int num_taps,
+                                                   gpud_stream_handle stream);
+/* exports.cu:198-244 -- as gpud_launch_fir_stream_cuda with a device taps
+ * pointer per call. */
+GPUD_API int GPUD_CALL gpud_launch_fir_v2_stream_cuda(const gpud_float2 *in, gpud_float2 *out, const float *taps,
+                                                      int n, int num_taps, gpud_stream_handle stream);
+
+/* exports.cu:246-257 -- out[i] = in[i*factor]. */
+GPUD_API int GPUD_CALL gpud_launch_decimate_cuda(const gpud_float2 *in, gpud_float2 *out, int n_out, int factor);
+/* exports.cu:259-271 */
+GPUD_API int GPUD_CALL gpud_launch_decimate_stream_cuda(const gpud_float2 *in, gpud_float2 *out, int n_out,
+                                                        int factor, gpud_stream_handle stream);
+
+/* exports.cu:273-294 -- |in[i]| (no mean removal, as the reference kernel). */
+GPUD_API int GPUD_CALL gpud_launch_am_envelope_cuda(const gpud_float2 *in, float *out, int n);
+
+/* exports.cu:296-326 -- Re(in[i] * exp(j*(phase_start + i*phase_inc))). */
+GPUD_API int GPUD_CALL gpud_launch_ssb_product_cuda(const gpud_float2 *in, float *out, int n, double phase_inc,
+                                                    double phase_start);
+
+/* exports.cu:356-460 -- transitional one-shot polyphase prepare (shift, FIR,
+ * decimate, history tail).  Codes -1..-5 as the reference.  Unlike the
+ * reference it allocates no device memory: the shifted samples are produced
+ * inside the fused kernel. */
+GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_prepare_cuda(
+    const gpud_float2 *in_new, int n_new, const gpud_float2 *history_in, int history_len, const float *polyphase_taps,
+    int polyphase_len, int decim, int num_taps, int phase_count_in, double phase_start, double phase_inc,
+    gpud_float2 *out, int *n_out /*host*/, int *phase_count_out /*host*/, double *phase_end_out /*host*/,
+    gpud_float2 *history_out);
+
+/* exports.cu:533-631 -- production stateful streaming extractor for one
+ * signal.  history_len_io, phase_count_state, phase_state and n_out are host
+ * pointers read before and written after the launches; everything else is
+ * device memory.  Codes -10..-16 as the reference.  Taps follow the CPU
+ * oracle: the layout stride is polyphase_len/decim and taps with
+ * p + k*decim >= num_taps are not applied (gpudemod/streaming_host_core.go). */
+GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_cuda(
+    const gpud_float2 *in_new, int n_new, gpud_float2 *shifted_new_tmp, const float *polyphase_taps,
+    int polyphase_len, int decim, int num_taps, gpud_float2 *history_state, gpud_float2 *history_scratch,
+    int history_cap, int *history_len_io /*host*/, int *phase_count_state /*host*/, double *phase_state /*host*/,
+    double phase_inc, gpud_float2 *out, int out_cap, int *n_out /*host*/);
+
+/* ======================================================================== */
+/* Part 2: batched / serving runner                                          */
+/* ======================================================================== */
+
+/* New error codes (all below the reference's -16). */
+#define GPUD_E_ARG (-20)           /* null pointer / bad size */
+#define GPUD_E_DECIM (-21)         /* sample_rate % out_rate != 0 (ExactIntegerDecimation) */
+#define GPUD_E_TAPS (-22)          /* tap count or polyphase layout beyond the runner's caps */
+#define GPUD_E_BUDGET (-23)        /* admission refused: device-memory budget exhausted */
+#define GPUD_E_SLOTS (-24)         /* admission refused: channel cap reached */
+#define GPUD_E_SLOT (-25)          /* slot id not active */
+#define GPUD_E_BLOCK (-26)         /* block larger than the runner's max_block */
+#define GPUD_E_TIMEOUT (-27)       /* wait timed out */
+#define GPUD_E_CUDA (-28)          /* CUDA call failed (details via gpud_runner_last_error) */
+#define GPUD_E_MODE (-29)          /* unknown demod mode */
+#define GPUD_E_DEVICE_STATUS (-30) /* a kernel reported a bounds/status failure */
+#define GPUD_E_STATE (-31)         /* snapshot blob does not match the slot geometry */
+
+/* Demod modes: DemodType of gpudemod.go:69-76 plus WFM_STEREO and IQ-only. */
+enum {
+    GPUD_MODE_IQ = 0,
+    GPUD_MODE_NFM = 1,
+    GPUD_MODE_WFM = 2,
+    GPUD_MODE_WFM_STEREO = 3,
+    GPUD_MODE_AM = 4,
+    GPUD_MODE_USB = 5,
+    GPUD_MODE_LSB = 6,
+    GPUD_MODE_CW = 7
+};
+
+/* channel flags */
+#define GPUD_CH_EMIT_IQ 1 /* copy the extracted IQ back every block */
+#define GPUD_CH_RDS 2     /* WFM modes: produce the 57 kHz RDS baseband */
+
+/* Schedules for gpud_runner_set_schedule. */
+#define GPUD_SCHED_BATCHED 0 /* one fused launch sequence for all channels (graph-captured) */
+#define GPUD_SCHED_PLAIN 1   /* per-signal, synchronous: H2D, launches, D2H per channel */
+
+/* StreamingExtractJob (gpudemod/streaming_types.go:8-15) plus the demod mode. */
+typedef struct {
+    int64_t signal_id;
+    double offset_hz;
+    double bandwidth;
+    int32_t out_rate;
+    int32_t num_taps; /* <= 0 selects 101 (stream_state.go:51-53) */
+    uint64_t config_hash;
+    int32_t mode;  /* GPUD_MODE_* */
+    int32_t flags; /* GPUD_CH_* */
+} gpud_channel_spec;
+
+/* Per-channel result of the last processed block.  The pointers reference
+ * the runner's pinned host output arena and stay valid until the next block
+ * is submitted.  Mirrors StreamingExtractResult (streaming_types.go:17-24)
+ * plus the demod outputs. */
+typedef struct {
+    int64_t signal_id;
+    int32_t rate;        /* extraction output rate */
+    int32_t n_iq;        /* NOut */
+    int32_t phase_count; /* PhaseCount after the block */
+    int32_t history_len; /* HistoryLen after the block */
+    double nco_phase;    /* NCO phase after the block, [-pi, pi) */
+    int32_t n_audio;     /* floats in audio (2 per frame for WFM_STEREO) */
+    int32_t audio_channels;
+    int32_t n_rds;    /* complex RDS baseband samples */
+    int32_t rds_rate; /* out_rate / floor(out_rate / 19000) */
+    int32_t flags;    /* bit0 pilot locked this block, bit1 stereo enabled */
+    float coherence;  /* pilot lock margins of this block */
+    float pilot_hz;
+    float err_avg;
+    const gpud_float2 *iq; /* host; NULL unless GPUD_CH_EMIT_IQ */
+    const float *audio;    /* host */
+    const gpud_float2 *rds;
+} gpud_channel_result;
+
+/* Runner statistics. */
+typedef struct {
+    uint64_t blocks;
+    int32_t active_channels;
+    int32_t max_channels;
+    uint64_t device_bytes_used;
+    uint64_t device_bytes_budget;
+    double last_block_ms;   /* device time of the last block (CUDA events) */
+    double p50_block_ms;    /* over the last 4096 blocks */
+    double p99_block_ms;
+    uint64_t kernel_launches; /* kernels launched by the runner since creation */
+    int32_t graph_rebuilds;
+} gpud_runner_stats;
+
+typedef struct gpud_runner gpud_runner;
+
+/* Create a runner for one wideband stream.  max_block: largest IQ block;
+ * max_channels: slot count (<= 4096); max_taps: largest FIR (<= 4096);
+ * device_mem_budget: bytes the runner may allocate for channel state and
+ * buffers (0 = no limit).  Returns 0 or a GPUD_E_* code. */
+GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int max_channels, int max_taps,
+                                          uint64_t device_mem_budget, gpud_runner **out);
+GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r);
+
+/* Admit a channel (slot state resident on the device).  Refused with
+ * GPUD_E_BUDGET when the channel's device footprint would exceed the budget,
+ * GPUD_E_SLOTS at the channel cap.  New channels join at the next block. */
+GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out);
+GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot);
+/* Offset / bandwidth drift: the NCO increment follows the offset with the
+ * phase kept; taps are rebuilt when the cutoff changes, history kept
+ * (stream_state.go:57-77, Q11). */
+GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offset_hz, double bandwidth);
+GPUD_API int GPUD_CALL gpud_runner_set_schedule(gpud_runner *r, int schedule);
+/* Bytes of device memory one more channel of this spec would take. */
+GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_channel_spec *spec,
+                                                     uint64_t *bytes);
+
+/* Process one IQ block through every active channel, synchronously.  iq is a
+ * host pointer (copied through the runner's pinned staging buffer) unless
+ * iq_on_device != 0. */
+GPUD_API int GPUD_CALL gpud_runner_process_block(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device);
+/* Asynchronous form: enqueue the block and return a ticket; wait returns 0
+ * once its outputs are in host memory (GPUD_E_TIMEOUT after timeout_ms). */
+GPUD_API int GPUD_CALL gpud_runner_submit(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device,
+                                          uint64_t *ticket);
+GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int timeout_ms);
+GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel_result *out);
+GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *out);
+/* Device stream the runner launches on (for external event timing). */
+GPUD_API int GPUD_CALL gpud_runner_stream(gpud_runner *r, gpud_stream_handle *out);
+GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r);
+
+/* Slot snapshot / restore (checkpoint across segment rotation; mirrors
+ * recorder/streamer.go:1646-1752 captureDSPState/restoreDSPState).  The blob
+ * holds the complete device state of the slot; size via *bytes with
+ * blob == NULL. */
+GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob /*host*/, uint64_t *bytes);
+GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void *blob /*host*/, uint64_t bytes);
+
+/* BatchRunner.StreamingExtractGPU (streaming_gpu_stub.go:21-26) semantics:
+ * jobs keyed by signal_id; state reset when config_hash changes
+ * (stream_state.go:41-47); signals absent from the call are pruned
+ * (streaming_gpu_prepare.go:38-43).  Extracted IQ is written back to iq_out
+ * (host, capacity iq_out_cap complex samples) job after job; results[i].iq
+ * points into it. */
+GPUD_API int GPUD_CALL gpud_runner_streaming_extract(gpud_runner *r, const gpud_float2 *iq /*host*/, int n,
+                                                     const gpud_channel_spec *jobs, int n_jobs,
+                                                     gpud_channel_result *results, gpud_float2 *iq_out /*host*/,
+                                                     int iq_out_cap);
+
+/* BatchRunner.ResetSignalState / ResetAllSignalStates (stream_state.go:9-24):
+ * forget the streaming state of one signal id (or of all signals admitted
+ * through gpud_runner_streaming_extract); the next job for it starts fresh. */
+GPUD_API int GPUD_CALL gpud_runner_reset_signal(gpud_runner *r, int64_t signal_id);
+GPUD_API int GPUD_CALL gpud_runner_reset_all_signals(gpud_runner *r);
+
+/* gpudemod/streaming_types.go:58-72 StreamingConfigHash. */
+GPUD_API uint64_t GPUD_CALL gpud_streaming_config_hash(int64_t signal_id, int out_rate, int num_taps,
+                                                       int sample_rate);
+
+/* Number of kernels this library has launched in the process (all entry
+ * points). */
+GPUD_API uint64_t GPUD_CALL gpud_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUDEMOD_H */

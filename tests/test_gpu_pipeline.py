@@ -1,0 +1,198 @@
+"""The full per-channel chain on the GPU runner (extract -> demod -> WFM
+multiplex -> RDS baseband) against the CPU oracle chain, block by block."""
+import numpy as np
+import pytest
+
+import gpudemod as G
+from gpudemod import synth
+from oracle import oracle as O
+from signals import max_abs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+AUDIO_TOL = 1e-5   # relative L2 per block
+RDS_TOL = 1e-5
+
+
+def _scene_blocks(n_blocks, block=262_144, seed=synth.CONFIG_SEEDS[0]):
+    scene, st = synth.plain_wfm_scene(block=block, seed=seed)
+    return [scene.next_block().numpy() for _ in range(n_blocks)], st
+
+
+def _compare_block(g, w, ctx):
+    assert g["n_iq"] == w["iq"].size, ctx
+    assert g["audio"].size == w["audio"].size, ctx
+    assert g["rds"].size == w["rds"].size, ctx
+    if w["audio"].size:
+        assert rel_l2(g["audio"], w["audio"]) <= AUDIO_TOL, (ctx, rel_l2(g["audio"], w["audio"]))
+    if w["rds"].size:
+        assert rel_l2(g["rds"], w["rds"]) <= RDS_TOL, (ctx, rel_l2(g["rds"], w["rds"]))
+    assert g["locked"] == w["locked"], ctx
+    assert g["stereo"] == w["stereo"], ctx
+
+
+def test_wfm_stereo_rds_chain_matches_oracle(cuda):
+    blocks, st = _scene_blocks(10)
+    fs, out = 2_400_000, 300_000
+    runner = G.ChannelRunner(fs, 262_144, max_channels=4)
+    slot = runner.admit(1, 300_000.0, 250_000.0, out, 128, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_EMIT_IQ)
+    ref = O.OracleChannel(fs, 300_000.0, 250_000.0, out, 128, O.MODE_WFM_STEREO, rds=True)
+    g_rds, w_rds = [], []
+    try:
+        for b, x in enumerate(blocks):
+            runner.process_block(x)
+            g = runner.result(slot)
+            w = ref.process(x)
+            assert rel_l2(g["iq"], w["iq"]) <= 1e-5
+            _compare_block(g, w, b)
+            c, f, e = ref.margins()
+            assert abs(g["coherence"] - c) <= 1e-4 * max(1, c)
+            assert abs(g["pilot_hz"] - f) <= 1e-2
+            g_rds.append(g["rds"])
+            w_rds.append(w["rds"])
+        # RDS groups decoded from the GPU baseband == from the oracle baseband
+        dg, dw = O.RDSDecoder(), O.RDSDecoder()
+        ng = dg.decode(np.concatenate(g_rds), 20_000)
+        nw = dw.decode(np.concatenate(w_rds), 20_000)
+        assert ng == nw and ng > 0
+        assert dg.result() == dw.result()
+        assert dg.result()[0] == st[0].pi and dg.result()[1] == st[0].ps
+        assert runner.result(slot)["stereo"]
+    finally:
+        runner.close()
+
+
+@pytest.mark.parametrize("mode,out_rate,taps,bw,offset", [
+    (G.MODE_NFM, 25_000, 512, 12_500, -400_000.0),
+    (G.MODE_AM, 25_000, 384, 10_000, 150_000.0),
+    (G.MODE_USB, 12_500, 256, 3_000, 612_345.0),
+    (G.MODE_LSB, 12_500, 256, 3_000, -512_345.0),
+    (G.MODE_CW, 5_000, 128, 500, 1_000_000.0),
+    (G.MODE_WFM, 312_500, 256, 250_000, -2_000_000.0),
+])
+def test_narrow_modes_match_oracle(cuda, mode, out_rate, taps, bw, offset):
+    fs, block = 10_000_000, 200_000
+    rng = np.random.default_rng(mode)
+    runner = G.ChannelRunner(fs, block, max_channels=2)
+    slot = runner.admit(9, offset, bw, out_rate, taps, mode, G.CH_EMIT_IQ)
+    ref = O.OracleChannel(fs, offset, bw, out_rate, taps, mode, rds=False)
+    try:
+        for b in range(4):
+            n = block - 17 * b
+            t = np.arange(b * block, b * block + n)
+            x = (0.3 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+                 + np.exp(2j * np.pi * (offset + 1234.5) * t / fs)).astype(np.complex64)
+            runner.process_block(x)
+            g = runner.result(slot)
+            w = ref.process(x)
+            assert rel_l2(g["iq"], w["iq"]) <= 1e-5
+            assert g["audio"].size == w["audio"].size
+            assert rel_l2(g["audio"], w["audio"]) <= AUDIO_TOL, rel_l2(g["audio"], w["audio"])
+            assert g["phase_count"] == ref.state()[1] and g["history_len"] == ref.state()[2]
+    finally:
+        runner.close()
+
+
+def _mixed_runner(fs, block, schedule=G.SCHED_BATCHED):
+    r = G.ChannelRunner(fs, block, max_channels=16)
+    r.set_schedule(schedule)
+    specs = [
+        (1, 300_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_EMIT_IQ),
+        (2, -450_000.0, 12_500.0, 25_000, 512, G.MODE_NFM, 0),
+        (3, 700_000.0, 10_000.0, 25_000, 384, G.MODE_AM, 0),
+        (4, -900_000.0, 3_000.0, 12_500, 256, G.MODE_USB, 0),
+        (5, 100_000.0, 500.0, 5_000, 128, G.MODE_CW, 0),
+    ]
+    slots = [r.admit(*s) for s in specs]
+    return r, slots, specs
+
+
+def test_batched_equals_plain_schedule(cuda):
+    blocks, _ = _scene_blocks(3)
+    fs = 2_400_000
+    rb, sb, _ = _mixed_runner(fs, 262_144)
+    rp, sp, _ = _mixed_runner(fs, 262_144, G.SCHED_PLAIN)
+    try:
+        for x in blocks:
+            rb.process_block(x)
+            rp.process_block(x)
+            for a, b in zip(sb, sp):
+                ga, gb = rb.result(a), rp.result(b)
+                assert np.array_equal(ga["audio"], gb["audio"])
+                assert np.array_equal(ga["rds"], gb["rds"])
+                assert np.array_equal(ga["iq"], gb["iq"])
+                assert ga["stereo"] == gb["stereo"]
+    finally:
+        rb.close()
+        rp.close()
+
+
+def test_channel_alone_equals_in_mix(cuda):
+    """Serving invariant: a channel's output is identical alone and in a mix."""
+    blocks, _ = _scene_blocks(3)
+    fs = 2_400_000
+    mix, slots, specs = _mixed_runner(fs, 262_144)
+    try:
+        for k, spec in enumerate(specs):
+            alone = G.ChannelRunner(fs, 262_144, max_channels=2)
+            s = alone.admit(*spec)
+            outs_alone = []
+            for x in blocks:
+                alone.process_block(x)
+                outs_alone.append(alone.result(s))
+            alone.close()
+            if k == 0:
+                outs_mix = [[] for _ in specs]
+                for x in blocks:
+                    mix.process_block(x)
+                    for j, sl in enumerate(slots):
+                        outs_mix[j].append(mix.result(sl))
+            for a, m in zip(outs_alone, outs_mix[k]):
+                assert np.array_equal(a["audio"], m["audio"])
+                assert np.array_equal(a["rds"], m["rds"])
+                assert a["stereo"] == m["stereo"]
+    finally:
+        mix.close()
+
+
+def test_snapshot_restore_continues_exactly(cuda):
+    blocks, _ = _scene_blocks(4)
+    fs = 2_400_000
+    spec = (1, 300_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS)
+    ra = G.ChannelRunner(fs, 262_144, max_channels=2)
+    rb = G.ChannelRunner(fs, 262_144, max_channels=2)
+    sa = ra.admit(*spec)
+    try:
+        for x in blocks[:2]:
+            ra.process_block(x)
+        blob = ra.snapshot(sa)
+        sb = rb.admit(*spec)
+        rb.restore(sb, blob)
+        for x in blocks[2:]:
+            ra.process_block(x)
+            rb.process_block(x)
+            a, b = ra.result(sa), rb.result(sb)
+            assert np.array_equal(a["audio"], b["audio"])
+            assert np.array_equal(a["rds"], b["rds"])
+    finally:
+        ra.close()
+        rb.close()
+
+
+def test_admission_by_device_memory_budget(cuda):
+    fs, block = 10_000_000, 262_144
+    probe = G.ChannelRunner(fs, block, max_channels=8)
+    fp = probe.footprint(312_500, G.MODE_WFM_STEREO, G.CH_RDS, 256)
+    base = probe.stats()["device_bytes_used"]
+    probe.close()
+    r = G.ChannelRunner(fs, block, max_channels=8, device_mem_budget=base + 3 * fp + fp // 2)
+    try:
+        for i in range(3):
+            r.admit(i, 100_000.0 * i, 250_000.0, 312_500, 256, G.MODE_WFM_STEREO, G.CH_RDS)
+        with pytest.raises(G.GPUDError) as ei:
+            r.admit(9, 0.0, 250_000.0, 312_500, 256, G.MODE_WFM_STEREO, G.CH_RDS)
+        assert ei.value.code == G.E_BUDGET
+        r.retire(0)
+        r.admit(9, 0.0, 250_000.0, 312_500, 256, G.MODE_WFM_STEREO, G.CH_RDS)
+    finally:
+        r.close()

@@ -1,0 +1,243 @@
+"""The CPU oracle pinned against the reference's own known-answer tests for
+this path (each test names the reference test it restates).  CPU only."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from signals import (chunks_of, make_deterministic_iq, make_lowpass_taps, max_abs)
+
+
+def _state(decim=20, taps=65, phase=0.0):
+    t = make_lowpass_taps(taps)
+    return O.CPUOracleState(SignalID=1, ConfigHash=123, NCOPhase=phase, Decim=decim, PhaseCount=0,
+                            NumTaps=taps, BaseTaps=t,
+                            PolyphaseTaps=O.build_polyphase_taps_phase_major(t, decim))
+
+
+def test_polyphase_layout_kat():
+    # polyphase_test.go:5-22
+    got = O.build_polyphase_taps_phase_major(np.arange(1, 8, dtype=np.float32), 3)
+    assert got.tolist() == [1, 4, 7, 2, 5, 0, 3, 6, 0]
+
+
+def test_exact_integer_decimation():
+    # cpu_oracle_test.go:60-67
+    assert O.exact_integer_decimation(4_000_000, 200_000) == 20
+    with pytest.raises(ValueError):
+        O.exact_integer_decimation(4_000_000, 192_000)
+
+
+def _chunked(iq, sizes, phase_inc, polyphase):
+    st = _state()
+    return np.concatenate([O.cpu_oracle_extract(c, st, phase_inc, polyphase) for c in chunks_of(iq, sizes)])
+
+
+def test_monolithic_vs_chunked_direct():
+    # cpu_oracle_test.go:39-58
+    iq = make_deterministic_iq(200_000)
+    mono = O.cpu_oracle_extract(iq, _state(), 0.017)
+    chunked = _chunked(iq, [4096, 5000, 8192, 27307], 0.017, False)
+    assert mono.size == chunked.size == 200_000 // 20
+    assert max_abs(mono, chunked) <= 1e-5
+
+
+def test_direct_vs_polyphase():
+    # cpu_oracle_test.go:69-89
+    iq = make_deterministic_iq(50_000)
+    direct = O.cpu_oracle_extract(iq, _state(), 0.017, polyphase=False)
+    poly = O.cpu_oracle_extract(iq, _state(), 0.017, polyphase=True)
+    assert max_abs(direct, poly) <= 1e-5
+
+
+@pytest.mark.parametrize("n,inc,sizes", [
+    (120_000, 0.013, [4096, 3000, 8192, 7777, 12000]),   # oracle_validation_test.go:5-45
+    (150_000, 0.017, [4096, 5000, 8192, 27307]),          # test_harness_test.go:18-32
+])
+def test_monolithic_vs_chunked_polyphase(n, inc, sizes):
+    iq = make_deterministic_iq(n)
+    mono = O.cpu_oracle_extract(iq, _state(), inc, polyphase=True)
+    chunked = _chunked(iq, sizes, inc, True)
+    assert max_abs(mono, chunked) <= 1e-5
+
+
+def test_host_core_matches_oracle_polyphase():
+    # streaming_host_core_test.go:5-40
+    iq = make_deterministic_iq(12_000)
+    st = _state()
+    want = O.cpu_oracle_extract(iq, st, 0.017, polyphase=True)
+    s2 = _state()
+    out, phase, pc, hist = O.run_host_core(iq, 4_000_000, -0.017 * 4_000_000 / (2 * 3.141592653589793), 0.0, 0,
+                                           65, 20, np.zeros(0, np.complex64), s2.PolyphaseTaps)
+    assert max_abs(out, want) <= 1e-5
+    assert phase != 0 and 0 <= pc < 20 and hist.size > 0
+
+
+def test_even_taps_apply_first_T_of_odd_design():
+    # LowpassFIR bumps an even T to T+1 (dsp/fir.go:7-9) while the stream keeps
+    # T-1 history (stream_state.go:78-82): the T+1-th tap never applies.
+    fs, out_rate, T = 2_400_000, 300_000, 128
+    base = O.base_taps_f32(250_000, fs, T)
+    assert base.size == 129
+    iq = make_deterministic_iq(4096)
+    poly = O.build_polyphase_taps_phase_major(base, 8)
+    got, *_ = O.run_host_core(iq, fs, 10_000.0, 0.0, 0, T, 8, np.zeros(0, np.complex64), poly)
+    st = O.CPUOracleState(SignalID=1, Decim=8, NumTaps=T, BaseTaps=base[:T].copy())
+    want = O.cpu_oracle_extract(iq, st, -2 * math.pi * 10_000.0 / fs)
+    assert max_abs(got, want) <= 1e-6
+
+
+def test_runner_prunes_and_resets():
+    # state_reset_test.go / oracle_runner_test.go: hash change zeroes state,
+    # vanished signals are pruned
+    r = O.CPUOracleRunner(4_000_000)
+    a = O.StreamingExtractJob(11, 12_500.0, 20_000.0, 200_000, 65, 1001)
+    b = O.StreamingExtractJob(22, -18_750.0, 16_000.0, 100_000, 33, 2002)
+    r.StreamingExtract(make_deterministic_iq(512), [a, b])
+    assert set(r.States) == {11, 22}
+    assert r.States[11].PhaseCount == 512 % 20 and r.States[11].ShiftedHistory.size == 64
+    a2 = O.StreamingExtractJob(11, 12_500.0, 20_000.0, 200_000, 65, 1002)
+    r.StreamingExtract(np.zeros(0, np.complex64), [a2])
+    assert set(r.States) == {11}
+    assert r.States[11].NCOPhase == 0.0 and r.States[11].PhaseCount == 0
+    assert r.States[11].ShiftedHistory.size == 0
+
+
+def test_config_hash_ignores_offset_and_bandwidth():
+    from gpudemod import StreamingConfigHash
+    h = O.streaming_config_hash(7, 200_000, 65, 4_000_000)
+    assert h == StreamingConfigHash(7, 123.0, 9999.0, 200_000, 65, 4_000_000)
+    assert h != O.streaming_config_hash(7, 200_000, 66, 4_000_000)
+
+
+# ---------------------------------------------------------------------------
+# RDS baseband: streaming == one plain call (fm_rds_test.go:10-35, byte exact)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("sr", [200_000, 250_000, 240_000])
+def test_rds_baseband_stream_equals_plain(sr):
+    rng = np.random.default_rng(1)
+    for n in [0, 1, 2, 17, 999, 4096]:
+        iq = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+        want, rate = O.rds_baseband_complex(iq, sr)
+        assert rate == (sr // (sr // 19000) if n >= 2 else 0)
+        disc = O.fm_discrim(iq)
+        st = O.RDSStream(sr)
+        got = np.concatenate([st.process(c) for c in chunks_of(disc, [1, 16, 333, 0, 1000])]) \
+            if disc.size else np.zeros(0, np.complex64)
+        assert got.size == want.size
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_rds_syndrome_and_group_kat():
+    from gpudemod import synth
+    for off in (synth.OFF_A, synth.OFF_B, synth.OFF_C, synth.OFF_CP, synth.OFF_D):
+        for data in (0, 1, 0xABCD, 0xFFFF, 0x1234):
+            blk = synth.rds_block(data, off)
+            assert O.rds_syndrome(blk) == off == synth.rds_syndrome(blk)
+            assert blk >> 10 == data
+
+
+def test_rds_encoder_decoder_kat():
+    """Encoder -> BPSK baseband -> decoder: PI/PS/RT recovered bit-exactly."""
+    from gpudemod import synth
+    pi, ps, rt = 0xC0DE, "ARGUSB2K", "RADIOTEXT ON A B200 - SEEDED GROUP KAT 0123456789"
+    bits = synth.rds_bits(synth.rds_groups(pi, ps, rt), 3000)
+    sym = synth.rds_symbols(bits)
+    fs = 20000.0
+    t = np.arange(int(len(sym) / synth.RDS_BAUD * fs) - 40) / fs
+    pos = t * synth.RDS_BAUD
+    k = np.floor(pos).astype(int)
+    c = 0.5 * (1 + np.cos(np.pi * (pos - k)))
+    level = sym[k] * c + sym[k + 1] * (1 - c)
+    x = (0.3 * level * np.exp(1j * 0.7)).astype(np.complex64)
+    d = O.RDSDecoder()
+    groups = d.decode(x, 20000)
+    got_pi, got_ps, got_rt = d.result()
+    assert groups >= 20
+    assert (got_pi, got_ps, got_rt) == (pi, ps, rt.rstrip())
+
+
+# ---------------------------------------------------------------------------
+# stereo decoder properties (recorder/streamer_test.go, stereo_lock_test.go)
+# ---------------------------------------------------------------------------
+def _tone_mag(x, f, sr):
+    n = np.arange(len(x))
+    return abs(np.sum(x * np.exp(-2j * np.pi * f * n / sr))) * 2 / len(x)
+
+
+def test_stereo_pilot_lock_and_separation():
+    # streamer_test.go:8-67 (same composite: L-R on cos 38 kHz, pilot sin 19 kHz)
+    sr, blk = 192_000, 4096
+    dec = O.StereoDecoder()
+    for b in range(10):
+        t = (b * blk + np.arange(blk)) / sr
+        l, r = np.sin(2 * np.pi * 440 * t), np.sin(2 * np.pi * 880 * t)
+        comp = 0.5 * (l + r) + 0.5 * (l - r) * np.cos(2 * np.pi * 38000 * t) + 0.1 * np.sin(2 * np.pi * 19000 * t)
+        out, locked = dec.decode(comp.astype(np.float32), sr)
+    assert locked and out.size == 2 * blk
+    L, R = out[0::2], out[1::2]
+    l440, l880, r440, r880 = (_tone_mag(L, 440, sr), _tone_mag(L, 880, sr), _tone_mag(R, 440, sr),
+                              _tone_mag(R, 880, sr))
+    assert l440 >= 0.05 or l880 >= 0.05
+    left_is_l = l440 >= l880 * 1.3 and r880 >= r440 * 1.3
+    right_is_l = l880 >= l440 * 1.3 and r440 >= r880 * 1.3
+    assert left_is_l or right_is_l
+
+
+def _gen_mpx(n, sr, audio_amp, pilot_amp, t0):
+    t = t0 + np.arange(n) / sr
+    audio = audio_amp * np.sin(2 * np.pi * 1000 * t)
+    pilot = pilot_amp * np.sin(2 * np.pi * 19000 * t)
+    lr = 0.3 * audio_amp * np.sin(2 * np.pi * 2000 * t) * np.sin(2 * np.pi * 38000 * t)
+    return (audio + pilot + lr).astype(np.float32), t0 + n / sr
+
+
+def test_stereo_lock_holds_through_loud_audio():
+    # stereo_lock_test.go:31-63
+    sr, blk = 256_000, 4096
+    dec = O.StereoDecoder()
+    amps = [0.1] * 6 + [0.9, 0.15, 0.95, 0.1, 0.9, 0.95, 0.12, 0.9, 0.95, 0.9, 0.1, 0.95]
+    t0, loud, loud_locked = 0.0, 0, 0
+    for b, amp in enumerate(amps):
+        mpx, t0 = _gen_mpx(blk, sr, amp, 0.08, t0)
+        _, locked = dec.decode(mpx, sr)
+        if b >= 6 and amp >= 0.8:
+            loud += 1
+            loud_locked += int(locked)
+    assert loud > 0 and loud_locked == loud
+
+
+def test_stereo_no_false_lock_on_noise():
+    # stereo_lock_test.go:67-84 (seeded numpy noise stands in for Go math/rand)
+    sr, blk = 256_000, 4096
+    dec = O.StereoDecoder()
+    rng = np.random.default_rng(1)
+    for _ in range(15):
+        _, locked = dec.decode((rng.standard_normal(blk) * 0.3).astype(np.float32), sr)
+        assert not locked
+
+
+def test_pll_coefficients():
+    a, b = O.pll_coefficients(50, 0.707, 300_000)
+    bl = 50 / 300_000
+    th = bl / (0.707 + 0.25 / 0.707)
+    d = 1 + 2 * 0.707 * th + th * th
+    assert a == pytest.approx(4 * 0.707 * th / d, rel=1e-15)
+    assert b == pytest.approx(4 * th * th / d, rel=1e-15)
+
+
+def test_demod_semantics():
+    iq = make_deterministic_iq(1000)
+    am = O.am_demod(iq)
+    mag = np.abs(iq.astype(np.complex128))
+    assert np.allclose(am, (mag.astype(np.float32) - np.float32(mag.mean())), atol=1e-6)
+    usb = O.ssb_demod(iq, 48000, True)
+    ph = 2 * np.pi * 700 / 48000 * np.arange(1, 1001)
+    assert np.allclose(usb, iq.real * np.cos(ph) - iq.imag * np.sin(ph), atol=1e-6)
+    cw = O.cw_demod(iq, 48000)
+    assert np.allclose(cw, iq.real * np.cos(ph), atol=1e-6)
+    d = O.fm_discrim(iq)
+    assert d.size == 999
+    assert np.allclose(d, np.angle(iq[1:].astype(np.complex128) * np.conj(iq[:-1].astype(np.complex128))),
+                       atol=1e-6)
