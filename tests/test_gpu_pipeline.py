@@ -32,7 +32,8 @@ def _compare_block(g, w, ctx):
 
 
 def test_wfm_stereo_rds_chain_matches_oracle(cuda):
-    blocks, st = _scene_blocks(10)
+    # 20 blocks = 2.2 s: more than one full RDS group cycle (20 groups, 1.75 s)
+    blocks, st = _scene_blocks(20)
     fs, out = 2_400_000, 300_000
     runner = G.ChannelRunner(fs, 262_144, max_channels=4)
     slot = runner.admit(1, 300_000.0, 250_000.0, out, 128, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_EMIT_IQ)
@@ -80,8 +81,11 @@ def test_narrow_modes_match_oracle(cuda, mode, out_rate, taps, bw, offset):
         for b in range(4):
             n = block - 17 * b
             t = np.arange(b * block, b * block + n)
+            # a tone carrier; for AM a 1 kHz tone at 50 % modulation, so the
+            # demodulated audio is not a vanishing difference of two envelopes
+            env = 1.0 + (0.5 * np.sin(2 * np.pi * 1000 * t / fs) if mode == G.MODE_AM else 0.0)
             x = (0.3 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
-                 + np.exp(2j * np.pi * (offset + 1234.5) * t / fs)).astype(np.complex64)
+                 + env * np.exp(2j * np.pi * (offset + 1234.5) * t / fs)).astype(np.complex64)
             runner.process_block(x)
             g = runner.result(slot)
             w = ref.process(x)
