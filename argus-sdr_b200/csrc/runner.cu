@@ -224,7 +224,41 @@ struct gpud_runner {
     cudaEvent_t ev_done = nullptr;
     // StreamingExtractGPU bookkeeping
     std::map<int64_t, int> by_signal;
+    bool host_outputs = true;
+    uint64_t last_h2d = 0, last_d2h = 0;
+    // per-stage profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<std::string> prof_names;
+    int prof_n = 0;
+    std::vector<gpud_stage_time> stage_times;
 };
+
+static void prof_mark(gpud_runner *r, const char *name) {
+    if (!r->profiling) return;
+    if ((int)r->prof_ev.size() <= r->prof_n) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        r->prof_ev.push_back(e);
+        r->prof_names.emplace_back();
+    }
+    cudaEventRecord(r->prof_ev[(size_t)r->prof_n], r->stream);
+    r->prof_names[(size_t)r->prof_n] = name;
+    r->prof_n++;
+}
+
+static void prof_collect(gpud_runner *r) {
+    if (!r->profiling || r->prof_n < 2) return;
+    r->stage_times.clear();
+    for (int i = 0; i + 1 < r->prof_n; ++i) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r->prof_ev[(size_t)i], r->prof_ev[(size_t)i + 1]);
+        gpud_stage_time t{};
+        std::snprintf(t.name, sizeof t.name, "%s", r->prof_names[(size_t)i].c_str());
+        t.ms = ms;
+        r->stage_times.push_back(t);
+    }
+}
 
 static int set_err(gpud_runner *r, int code, const char *what, cudaError_t e = cudaSuccess) {
     char buf[256];
@@ -449,6 +483,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
     if (r->ev_done) cudaEventDestroy(r->ev_done);
+    for (auto e : r->prof_ev) cudaEventDestroy(e);
     if (r->stream) cudaStreamDestroy(r->stream);
     delete r;
     return 0;
@@ -800,51 +835,70 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
     int nl = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) {
         if (pl.w_dense[L].empty()) continue;
+        prof_mark(r, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str() : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
         CK(launch_extract_dense(L, (int)pl.w_dense[L].size(), pl.dense_smem[L], r->stream, d_w + w_dense_off[L],
                                 d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_wide.empty()) {
+        prof_mark(r, "extract_wide");
         CK(launch_extract_wide((int)pl.w_wide.size(), pl.wide_smem, r->stream, d_w + o_wide, d_sb, r->d_prm, r->d_st,
                                x_dev, n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_demod.empty()) {
+        prof_mark(r, "demod");
         CK(launch_demod((int)pl.w_demod.size(), r->stream, d_w + o_dem, d_sb, r->d_prm, r->d_st, d_ext, r->d_wk,
                         d_audio));
         nl++;
     }
     if (!pl.w_am.empty()) {
+        prof_mark(r, "am");
         CK(launch_am((int)pl.w_am.size(), r->stream, d_w + o_am, d_sb, d_ext, d_audio));
         nl++;
     }
     if (!pl.w_fir.empty()) {
+        prof_mark(r, "wfm_fir");
         CK(launch_wfm_fir((int)pl.w_fir.size(), r->stream, d_w + o_fir, d_sb, r->d_prm, wt, r->d_wk, W, r->d_comp_dl));
         nl++;
     }
     if (!pl.pll_list.empty()) {
+        prof_mark(r, "pll");
         CK(launch_pll((int)pl.pll_list.size(), r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W));
         nl++;
     }
     if (!pl.w_out.empty()) {
+        prof_mark(r, "wfm_out");
         CK(launch_wfm_out((int)pl.w_out.size(), r->stream, d_w + o_out, d_sb, r->d_prm, r->d_st, wt, r->d_wk, W,
                           r->d_lr_dl, r->d_audio_dl, d_audio));
         nl++;
     }
     if (!pl.w_rds.empty()) {
+        prof_mark(r, "rds");
         CK(launch_rds((int)pl.w_rds.size(), pl.rds_smem, r->stream, d_w + o_rds, d_sb, r->d_prm, r->d_st, wt,
                       r->d_tabs, r->d_wk, r->d_rds_dl, d_rds));
         nl++;
     }
     if (!pl.sbs.empty()) {
+        prof_mark(r, "post");
         CK(launch_post((int)pl.sbs.size(), r->stream, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_ext, r->d_wk, W,
                        r->d_comp_dl, r->d_lr_dl, r->d_audio_dl, r->d_rds_dl, r->d_tabs, d_res));
         nl++;
     }
+    prof_mark(r, "d2h");
     r->launches += (uint64_t)nl;
     gpud_count_launch(nl);
     r->out_bytes = r->off_ext + (size_t)pl.tot_emit_ext * 8;
-    CK(cudaMemcpyAsync(r->h_out, r->d_out, r->out_bytes, cudaMemcpyDeviceToHost, r->stream));
+    if (r->host_outputs) {
+        CK(cudaMemcpyAsync(r->h_out, r->d_out, r->out_bytes, cudaMemcpyDeviceToHost, r->stream));
+        r->last_d2h += r->out_bytes;
+    } else {
+        // keep the results table on the host (small); payload stays on the device
+        CK(cudaMemcpyAsync(r->h_out, r->d_out, r->off_audio, cudaMemcpyDeviceToHost, r->stream));
+        r->last_d2h += r->off_audio;
+    }
+    r->last_h2d += dbytes;
+    prof_mark(r, "end");
     return 0;
 }
 
@@ -867,6 +921,7 @@ static int stage_input(gpud_runner *r, const gpud_float2 *iq, int n, int on_devi
         src = r->h_in;
     }
     CK(cudaMemcpyAsync(r->d_block, src, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, r->stream));
+    r->last_h2d += (uint64_t)n * sizeof(float2);
     *x_dev = r->d_block;
     return 0;
 }
@@ -885,7 +940,10 @@ static int run_block(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
         CK(cudaEventSynchronize(r->ev_done));
         r->done_ticket = r->pending_ticket;
     }
+    r->prof_n = 0;
+    r->last_h2d = r->last_d2h = 0;
     CK(cudaEventRecord(r->ev0, r->stream));
+    prof_mark(r, "h2d");
     const float2 *x = nullptr;
     int rc = stage_input(r, iq, n, on_device, &x);
     if (rc) return rc;
@@ -969,6 +1027,7 @@ static int run_block(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
         CK(cudaEventSynchronize(r->ev_done));
         r->done_ticket = r->pending_ticket;
         record_latency(r);
+        prof_collect(r);
     }
     return 0;
 }
@@ -1008,6 +1067,27 @@ GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int tim
     }
     r->done_ticket = r->pending_ticket;
     record_latency(r);
+    prof_collect(r);
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on) {
+    if (!r) return GPUD_E_ARG;
+    r->host_outputs = on != 0;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_set_profiling(gpud_runner *r, int on) {
+    if (!r) return GPUD_E_ARG;
+    r->profiling = on != 0;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_stage_times(gpud_runner *r, gpud_stage_time *out, int cap, int *count) {
+    if (!r || !count) return GPUD_E_ARG;
+    int n = (int)r->stage_times.size();
+    *count = n;
+    for (int i = 0; i < n && i < cap && out; ++i) out[i] = r->stage_times[(size_t)i];
     return 0;
 }
 
@@ -1037,9 +1117,10 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->coherence = res->coherence;
     out->pilot_hz = res->pilot_hz;
     out->err_avg = res->err_avg;
-    out->audio = (const float *)(r->h_out + r->off_audio) + sb.audio_off;
-    out->rds = (const gpud_float2 *)(r->h_out + r->off_rds) + sb.rds_off;
-    out->iq = (s.spec.flags & GPUD_CH_EMIT_IQ) ? (const gpud_float2 *)(r->h_out + r->off_ext) + sb.ext_off : nullptr;
+    const char *base = r->host_outputs ? r->h_out : r->d_out;
+    out->audio = (const float *)(base + r->off_audio) + sb.audio_off;
+    out->rds = (const gpud_float2 *)(base + r->off_rds) + sb.rds_off;
+    out->iq = (s.spec.flags & GPUD_CH_EMIT_IQ) ? (const gpud_float2 *)(base + r->off_ext) + sb.ext_off : nullptr;
     return 0;
 }
 
@@ -1064,6 +1145,8 @@ GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *
     }
     out->kernel_launches = r->launches;
     out->graph_rebuilds = r->graph_rebuilds;
+    out->last_h2d_bytes = r->last_h2d;
+    out->last_d2h_bytes = r->last_d2h;
     return 0;
 }
 

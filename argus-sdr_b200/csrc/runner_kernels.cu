@@ -350,15 +350,23 @@ k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
     }
 }
 
-// Pilot PLL, serial per channel (one lane per WFM_STEREO slot).  Phase,
+// Pilot PLL, serial per channel (recorder/streamer.go:1560-1619).  Phase,
 // frequency and the I/Q lowpass states are float64 (the frequency integrator
 // moves by ~1e-10 rad/sample, below float32 resolution); the loop's sin/cos and
-// atan2 are float32.  Writes lr = bpf * float32(2 sin(2 phase)) and the
-// per-call lock decision with its hysteresis (streamer.go:1363-1380,1615-1635).
-__global__ void __launch_bounds__(32)
+// atan2 are float32.  One CTA per channel: lane 0 of warp 0 runs the recurrence
+// from shared memory; warp 1 prefetches the next chunk of the pilot band and
+// finishes the previous chunk off the critical path (lr = bpf * float32(2 sin
+// 2phase), pilot power).  Per-call lock decision and hysteresis at the end
+// (streamer.go:1363-1380, 1615-1635).
+constexpr int kPllChunk = 2048;
+
+__global__ void __launch_bounds__(64)
 k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
       const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W) {
-    const int idx = blockIdx.x * 32 + threadIdx.x;
+    __shared__ float s_pil[2][kPllChunk];
+    __shared__ float s_th[2][kPllChunk];
+    __shared__ double s_red[32];
+    const int idx = blockIdx.x;
     if (idx >= count) return;
     const SlotBlock sb = sbt[list[idx]];
     const int n = sb.n_disc;
@@ -368,31 +376,72 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
     const float *pil = wk + 3 * W + sb.comp_off;
     const float *bpf = wk + 2 * W + sb.comp_off;
     float *lr = wk + 4 * W + sb.comp_off;
-    double ph = s.pll_phase, fr = s.pll_freq, I = s.pll_i, Q = s.pll_q;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nc = (n + kPllChunk - 1) / kPllChunk;
+    const double twopi = 2.0 * GPUD_PI;
+    double pp = 0.0;  // pilot power, accumulated by warp 1
+    // prologue: chunk 0 into buffer 0
+    if (warp == 1) {
+        for (int q = lane; q < min(n, kPllChunk); q += 32) s_pil[0][q] = pil[q];
+    }
+    __syncthreads();
+    double ph = s.pll_phase, fr = s.pll_freq, I = s.pll_i, Q = s.pll_q, es = 0.0;
     const double alpha = cp.pll_alpha, beta = cp.pll_beta, lpa = cp.pll_lpa;
     const double fmin = cp.pll_fmin, fmax = cp.pll_fmax;
-    const double twopi = 2.0 * GPUD_PI;
-    double pp = 0.0, es = 0.0;
-    for (int q = 0; q < n; ++q) {
-        const double p = (double)pil[q];
-        const float bq = bpf[q];
-        float sf, cf;
-        __sincosf((float)(ph - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sin/-cos(ph - pi)
-        const double cp_ = -(double)cf, sp_ = -(double)sf;
-        I += lpa * (p * cp_ - I);
-        Q += lpa * (p * -sp_ - Q);
-        const double err = (double)atan2f((float)Q, (float)I);
-        fr += beta * err;
-        fr = fr < fmin ? fmin : (fr > fmax ? fmax : fr);
-        ph += fr + alpha * err;
-        if (ph > twopi) ph -= twopi;
-        else if (ph < 0.0) ph += twopi;
-        pp += p * p;
-        es += fabs(err);
-        double t2 = 2.0 * ph;  // [0, 4pi]
-        t2 -= twopi * rint(t2 * (1.0 / twopi));
-        lr[q] = bq * (2.0f * sinf((float)t2));
+    for (int c = 0; c <= nc; ++c) {
+        if (warp == 0) {
+            if (lane == 0 && c < nc) {
+                const float *sp = s_pil[c & 1];
+                float *th = s_th[c & 1];
+                const int len = min(kPllChunk, n - c * kPllChunk);
+                for (int q = 0; q < len; ++q) {
+                    const double p = (double)sp[q];
+                    float sf, cf;
+                    __sincosf((float)(ph - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sin/-cos(ph - pi)
+                    I += lpa * (p * -(double)cf - I);
+                    Q += lpa * (p * (double)sf - Q);
+                    const double err = (double)atan2f((float)Q, (float)I);
+                    fr += beta * err;
+                    fr = fr < fmin ? fmin : (fr > fmax ? fmax : fr);
+                    ph += fr + alpha * err;
+                    if (ph > twopi) ph -= twopi;
+                    else if (ph < 0.0) ph += twopi;
+                    es += fabs(err);
+                    double t2 = 2.0 * ph;  // [0, 4pi] -> [-pi, pi]
+                    t2 -= twopi * rint(t2 * (1.0 / twopi));
+                    th[q] = (float)t2;
+                }
+            }
+        } else {
+            // finish chunk c-1, then prefetch chunk c+1 into the buffer it frees
+            if (c >= 1) {
+                const int base = (c - 1) * kPllChunk;
+                const int len = min(kPllChunk, n - base);
+                const float *th = s_th[(c - 1) & 1];
+                const float *sp = s_pil[(c - 1) & 1];
+                for (int q = lane; q < len; q += 32) {
+                    const double p = (double)sp[q];
+                    pp += p * p;
+                    lr[base + q] = bpf[base + q] * (2.0f * sinf(th[q]));
+                }
+            }
+            __syncwarp();
+            if (c + 1 < nc) {
+                const int base = (c + 1) * kPllChunk;
+                const int len = min(kPllChunk, n - base);
+                float *dst = s_pil[(c + 1) & 1];
+                for (int q = lane; q < len; q += 32) dst[q] = pil[base + q];
+            }
+        }
+        __syncthreads();
     }
+    if (warp == 1) {
+        for (int off = 16; off > 0; off >>= 1) pp += __shfl_xor_sync(0xffffffffu, pp, off);
+        if (lane == 0) s_red[0] = pp;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    pp = s_red[0];
     s.pll_phase = ph;
     s.pll_freq = fr;
     s.pll_i = I;
@@ -707,7 +756,7 @@ cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const Sl
 
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
                        ChanState *st, float *wk, int W) {
-    k_pll<<<(count + 31) / 32, 32, 0, sm>>>(list, count, sbt, prm, st, wk, W);
+    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W);
     return cudaGetLastError();
 }
 

@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import ChannelResult, ChannelSpec, RunnerStats, lib
+from ._lib import ChannelResult, ChannelSpec, RunnerStats, StageTime, lib
 
 # DemodType (gpudemod.go:69-76) -> runner modes
 DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
@@ -226,6 +226,18 @@ class ChannelRunner:
         s = RunnerStats()
         _check(self._r, lib.gpud_runner_stats_get(self._r, C.byref(s)))
         return {f: getattr(s, f) for f, _ in RunnerStats._fields_}
+
+    def set_host_outputs(self, on: bool):
+        _check(self._r, lib.gpud_runner_set_host_outputs(self._r, 1 if on else 0))
+
+    def set_profiling(self, on: bool):
+        _check(self._r, lib.gpud_runner_set_profiling(self._r, 1 if on else 0))
+
+    def stage_times(self) -> list:
+        arr = (StageTime * 64)()
+        cnt = C.c_int()
+        _check(self._r, lib.gpud_runner_stage_times(self._r, arr, 64, C.byref(cnt)))
+        return [(arr[i].name.decode(), arr[i].ms) for i in range(min(cnt.value, 64))]
 
     def stream_handle(self) -> int:
         h = C.c_void_p()

@@ -55,6 +55,10 @@ class ChannelResult(C.Structure):
     ]
 
 
+class StageTime(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("ms", C.c_double)]
+
+
 class RunnerStats(C.Structure):
     _fields_ = [
         ("blocks", C.c_uint64),
@@ -67,6 +71,9 @@ class RunnerStats(C.Structure):
         ("p99_block_ms", C.c_double),
         ("kernel_launches", C.c_uint64),
         ("graph_rebuilds", C.c_int32),
+        ("pad", C.c_int32),
+        ("last_h2d_bytes", C.c_uint64),
+        ("last_d2h_bytes", C.c_uint64),
     ]
 
 
@@ -113,6 +120,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_restore": (i, [P, i, P, C.c_uint64]),
         "gpud_runner_streaming_extract": (i, [P, P, i, C.POINTER(ChannelSpec), i, C.POINTER(ChannelResult), P, i]),
         "gpud_runner_reset_signal": (i, [P, C.c_int64]),
+        "gpud_runner_set_host_outputs": (i, [P, i]),
+        "gpud_runner_set_profiling": (i, [P, i]),
+        "gpud_runner_stage_times": (i, [P, C.POINTER(StageTime), i, pi]),
         "gpud_runner_reset_all_signals": (i, [P]),
         "gpud_streaming_config_hash": (C.c_uint64, [C.c_int64, i, i, i]),
         "gpud_kernel_launch_count": (C.c_uint64, []),

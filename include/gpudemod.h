@@ -204,6 +204,9 @@ typedef struct {
     double p99_block_ms;
     uint64_t kernel_launches; /* kernels launched by the runner since creation */
     int32_t graph_rebuilds;
+    int32_t pad;
+    uint64_t last_h2d_bytes;  /* host->device bytes of the last block */
+    uint64_t last_d2h_bytes;  /* device->host bytes of the last block */
 } gpud_runner_stats;
 
 typedef struct gpud_runner gpud_runner;
@@ -244,6 +247,20 @@ GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *
 /* Device stream the runner launches on (for external event timing). */
 GPUD_API int GPUD_CALL gpud_runner_stream(gpud_runner *r, gpud_stream_handle *out);
 GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r);
+
+/* Output placement: with on == 0 the per-block outputs stay in the runner's
+ * device arena (no D2H; for consumers that read them on the GPU) and the
+ * pointers of gpud_channel_result are device pointers.  Default on. */
+GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on);
+
+/* Per-kernel device time of the last block (CUDA events between the
+ * launches on the runner stream); enable with gpud_runner_set_profiling. */
+typedef struct {
+    char name[24];
+    double ms;
+} gpud_stage_time;
+GPUD_API int GPUD_CALL gpud_runner_set_profiling(gpud_runner *r, int on);
+GPUD_API int GPUD_CALL gpud_runner_stage_times(gpud_runner *r, gpud_stage_time *out, int cap, int *count);
 
 /* Slot snapshot / restore (checkpoint across segment rotation; mirrors
  * recorder/streamer.go:1646-1752 captureDSPState/restoreDSPState).  The blob
