@@ -92,7 +92,7 @@ struct ChanState {
     uint64_t nco_q;      // NCO phase at the start of the next block
     float2 last_iq;      // discriminator bridge sample
     int32_t has_last;
-    int32_t pad0;
+    int32_t pll_path;    // last block: 1 parallel-in-time solver, 2 serial loop
     // stereo pilot PLL (recorder/streamer.go:1560-1619)
     double pll_phase, pll_freq, pll_i, pll_q, err_avg;
     int32_t on_count, off_count, enabled, locked;

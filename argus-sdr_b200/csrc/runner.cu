@@ -42,7 +42,11 @@ cudaError_t launch_am(int grid, cudaStream_t sm, const int2 *work, const SlotBlo
 cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const WfmTaps *taps, float *wk, int W, const float *comp_dl);
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W);
+                       ChanState *st, float *wk, int W, const int *done);
+cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
+                              const ChanParams *prm, ChanState *st, float *wk, int W, double *traj,
+                              const int64_t *traj_off, int *done);
+int pll_newton_threads();
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
                            const float *audio_dl, float *audio);
@@ -173,6 +177,8 @@ struct BlockPlan {
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
+    std::vector<int64_t> pll_traj_off;  // doubles, per pll_list entry
+    int64_t tot_traj = 0;
     int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_rds = 0;
 };
 
@@ -206,6 +212,12 @@ struct gpud_runner {
     float2 *d_block = nullptr;
     float *d_wk = nullptr;
     int64_t wk_cap = 0;  // W (floats per work array)
+    double *d_traj = nullptr;  // PLL trajectories (parallel-in-time solver)
+    int64_t traj_cap = 0;
+    int *d_done = nullptr;
+    int64_t done_cap = 0;
+    bool pll_parallel = true;
+    int num_sms = 148;
     char *d_out = nullptr, *h_out = nullptr;
     size_t out_cap = 0;
     char *d_desc = nullptr, *h_desc = nullptr;
@@ -437,6 +449,12 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
         }                                     \
     } while (0)
     CKC(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+            r->num_sms = sms;
+    }
     CKC(cudaEventCreate(&r->ev0));
     CKC(cudaEventCreate(&r->ev1));
     CKC(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
@@ -475,6 +493,8 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     cudaFree(r->d_tabs);
     cudaFree(r->d_block);
     cudaFree(r->d_wk);
+    cudaFree(r->d_traj);
+    cudaFree(r->d_done);
     cudaFree(r->d_out);
     cudaFree(r->d_desc);
     if (r->h_out) cudaFreeHost(r->h_out);
@@ -700,6 +720,8 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.w_out.clear();
     pl.w_rds.clear();
     pl.pll_list.clear();
+    pl.pll_traj_off.clear();
+    pl.tot_traj = 0;
     pl.rds_smem = 0;
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
@@ -721,6 +743,8 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         if (mode == GPUD_MODE_WFM_STEREO && sb.n_disc > 0) {
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_fir.push_back(make_int2(i, t));
             pl.pll_list.push_back(i);
+            pl.pll_traj_off.push_back(pl.tot_traj);
+            pl.tot_traj += 8 * ((int64_t)sb.n_disc + 1);
         }
         if ((mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO) && sb.n_disc > 0)
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_out.push_back(make_int2(i, t));
@@ -743,6 +767,20 @@ static int ensure_buffers(gpud_runner *r, const BlockPlan &pl) {
         r->wk_cap = cap;
         r->graph_rebuilds++;
     }
+    if (pl.tot_traj > r->traj_cap) {
+        cudaFree(r->d_traj);
+        r->d_traj = nullptr;
+        int64_t cap = std::max<int64_t>(pl.tot_traj * 5 / 4, 1 << 16);
+        CK(dalloc(&r->d_traj, (size_t)cap));
+        r->traj_cap = cap;
+    }
+    if ((int64_t)pl.pll_list.size() > r->done_cap) {
+        cudaFree(r->d_done);
+        r->d_done = nullptr;
+        int64_t cap = std::max<int64_t>((int64_t)pl.pll_list.size() * 2, 64);
+        CK(dalloc(&r->d_done, (size_t)cap));
+        r->done_cap = cap;
+    }
     size_t res = align256(pl.sbs.size() * sizeof(DevResult));
     size_t need = res + align256((size_t)pl.tot_audio * 4) + align256((size_t)pl.tot_rds * 8) +
                   align256((size_t)pl.tot_ext * 8);
@@ -762,7 +800,7 @@ static int ensure_buffers(gpud_runner *r, const BlockPlan &pl) {
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
-                   align256(pl.pll_list.size() * 4) + 4096;
+                   align256(pl.pll_list.size() * 4) + align256(pl.pll_list.size() * 8) + 4096;
     if (dneed > r->desc_cap) {
         cudaFree(r->d_desc);
         if (r->h_desc) cudaFreeHost(r->h_desc);
@@ -816,11 +854,14 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
            o_out = put(pl.w_out), o_rds = put(pl.w_rds);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
-    size_t dbytes = o_pll + pl.pll_list.size() * 4;
+    size_t o_traj = o_pll + align256(pl.pll_list.size() * 4);
+    std::memcpy(hd + o_traj, pl.pll_traj_off.data(), pl.pll_traj_off.size() * 8);
+    size_t dbytes = o_traj + pl.pll_traj_off.size() * 8;
     CK(cudaMemcpyAsync(r->d_desc, hd, dbytes, cudaMemcpyHostToDevice, r->stream));
     const SlotBlock *d_sb = (const SlotBlock *)(r->d_desc + o_sb);
     const int2 *d_w = (const int2 *)(r->d_desc + o_w);
     const int *d_pll = (const int *)(r->d_desc + o_pll);
+    const int64_t *d_traj_off = (const int64_t *)(r->d_desc + o_traj);
 
     r->off_res = 0;
     r->off_audio = align256(pl.sbs.size() * sizeof(DevResult));
@@ -863,8 +904,25 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
         nl++;
     }
     if (!pl.pll_list.empty()) {
-        prof_mark(r, "pll");
-        CK(launch_pll((int)pl.pll_list.size(), r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W));
+        const int *done = nullptr;
+        if (r->pll_parallel) {
+            // cluster size: enough CTAs to cover the SMs, no more than 8 per
+            // channel, at least 8 steps per thread
+            int nch = (int)pl.pll_list.size();
+            int max_n = 0;
+            for (int i : pl.pll_list) max_n = std::max(max_n, pl.sbs[(size_t)i].n_disc);
+            int cluster = 1;
+            while (cluster < 8 && nch * cluster * 2 <= 2 * r->num_sms &&
+                   max_n / (cluster * 2 * pll_newton_threads()) >= 8)
+                cluster *= 2;
+            prof_mark(r, "pll_newton");
+            CK(launch_pll_newton(nch, cluster, r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W, r->d_traj,
+                                 d_traj_off, r->d_done));
+            nl++;
+            done = r->d_done;
+        }
+        prof_mark(r, "pll_serial");
+        CK(launch_pll((int)pl.pll_list.size(), r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W, done));
         nl++;
     }
     if (!pl.w_out.empty()) {
@@ -1077,6 +1135,12 @@ GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on) {
     return 0;
 }
 
+GPUD_API int GPUD_CALL gpud_runner_set_pll_solver(gpud_runner *r, int parallel) {
+    if (!r) return GPUD_E_ARG;
+    r->pll_parallel = parallel != 0;
+    return 0;
+}
+
 GPUD_API int GPUD_CALL gpud_runner_set_profiling(gpud_runner *r, int on) {
     if (!r) return GPUD_E_ARG;
     r->profiling = on != 0;
@@ -1117,6 +1181,7 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->coherence = res->coherence;
     out->pilot_hz = res->pilot_hz;
     out->err_avg = res->err_avg;
+    out->pll_path = res->status;
     const char *base = r->host_outputs ? r->h_out : r->d_out;
     out->audio = (const float *)(base + r->off_audio) + sb.audio_off;
     out->rds = (const gpud_float2 *)(base + r->off_rds) + sb.rds_off;

@@ -10,6 +10,7 @@
 //   k_post                                per-slot state carry (histories, phases)
 // Every kernel takes a work list of (slot-block index, tile) pairs so channels
 // with uneven taps / decimation run in the same launch.
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -350,6 +351,38 @@ k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
     }
 }
 
+// End of one stereoDecodeStateful call: store the loop state, update errAvg
+// (EMA per call), the coherence / frequency / errAvg lock test and the
+// hysteresis counters (streamer.go:1614-1635, 1363-1380).
+__device__ void pll_finish(ChanState &s, const ChanParams &cp, int n, double ph, double fr, double I, double Q,
+                           double es, double pp) {
+    const double twopi = 2.0 * GPUD_PI;
+    s.pll_phase = ph;
+    s.pll_freq = fr;
+    s.pll_i = I;
+    s.pll_q = Q;
+    const double block_err = es / (double)n;
+    const double ea = 0.9 * s.err_avg + 0.1 * block_err;
+    s.err_avg = ea;
+    double coherence = 0.0;
+    if (pp > 1e-12) coherence = (I * I + Q * Q) * (double)n / pp;
+    const double fhz = fr * (double)cp.out_rate / twopi;
+    const int locked = coherence > 0.15 && fabs(fhz - 19000.0) < 250.0 && ea < 0.35;
+    s.locked = locked;
+    s.coherence = (float)coherence;
+    s.pilot_hz = (float)fhz;
+    s.last_err_avg = (float)ea;
+    if (locked) {
+        s.on_count += 1;
+        s.off_count = 0;
+        if (s.on_count >= 4) s.enabled = 1;
+    } else {
+        s.on_count = 0;
+        s.off_count += 1;
+        if (s.off_count >= 10) s.enabled = 0;
+    }
+}
+
 // Pilot PLL, serial per channel (recorder/streamer.go:1560-1619).  Phase,
 // frequency and the I/Q lowpass states are float64 (the frequency integrator
 // moves by ~1e-10 rad/sample, below float32 resolution); the loop's sin/cos and
@@ -362,12 +395,14 @@ constexpr int kPllChunk = 2048;
 
 __global__ void __launch_bounds__(64)
 k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
-      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W) {
+      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
+      const int *__restrict__ done) {
     __shared__ float s_pil[2][kPllChunk];
     __shared__ float s_th[2][kPllChunk];
     __shared__ double s_red[32];
     const int idx = blockIdx.x;
     if (idx >= count) return;
+    if (done && done[idx]) return;  // solved by the parallel-in-time kernel
     const SlotBlock sb = sbt[list[idx]];
     const int n = sb.n_disc;
     if (n <= 0) return;
@@ -441,31 +476,426 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    pp = s_red[0];
-    s.pll_phase = ph;
-    s.pll_freq = fr;
-    s.pll_i = I;
-    s.pll_q = Q;
-    const double block_err = es / (double)n;
-    const double ea = 0.9 * s.err_avg + 0.1 * block_err;
-    s.err_avg = ea;
-    double coherence = 0.0;
-    if (pp > 1e-12) coherence = (I * I + Q * Q) * (double)n / pp;
-    const double fhz = fr * (double)cp.out_rate / twopi;
-    const int locked = coherence > 0.15 && fabs(fhz - 19000.0) < 250.0 && ea < 0.35;
-    s.locked = locked;
-    s.coherence = (float)coherence;
-    s.pilot_hz = (float)fhz;
-    s.last_err_avg = (float)ea;
-    if (locked) {
-        s.on_count += 1;
-        s.off_count = 0;
-        if (s.on_count >= 4) s.enabled = 1;
-    } else {
-        s.on_count = 0;
-        s.off_count += 1;
-        if (s.off_count >= 10) s.enabled = 0;
+    pll_finish(s, cp, n, ph, fr, I, Q, es, s_red[0]);
+    s.pll_path = 2;
+}
+
+
+// ===========================================================================
+// Pilot PLL, parallel in time.
+// ===========================================================================
+// The block's loop trajectory x_t = (phase, freq, I, Q), t = 0..n, obeys
+// x_{t+1} = F(x_t, p_t) with the serial kernel's exact step F.  Newton's method
+// on the whole trajectory: with the current iterate X and J_t = dF/dx at X_t,
+//     delta_{t+1} = J_t delta_t + (F(X_t) - X_{t+1}),   delta_0 = 0,
+//     X_{t+1} <- X_{t+1} + delta_{t+1},
+// a linear recurrence solved by an associative scan over affine maps (4x4 matrix
+// + vector, float32; the residual and the iterate are float64).  The fixed point
+// is the serial trajectory; a locked loop converges quadratically from the
+// free-running guess phase_0 + t*freq_0 in 3-4 iterations.  A block that has
+// not converged after kMaxNewton iterations (acquisition, no pilot) is left to
+// the serial kernel (done[idx] = 0).
+constexpr int kNewtonThreads = 256;
+constexpr int kMaxNewton = 8;
+constexpr int kNW = kNewtonThreads / 32;
+
+struct PllK {
+    double alpha, beta, lpa, fmin, fmax;
+};
+
+struct Aff {
+    float a[16];  // row-major, state order (phase, freq, I, Q)
+    float b[4];
+};
+
+// One loop step at (ph, f, I, Q) with pilot p: new state and the Jacobian's
+// nonzero entries.  Mirrors k_pll's arithmetic exactly.
+struct PllEval {
+    double ph1, f1, I1, Q1;
+    float e;
+    float ja, jb, jc, jd;   // phase row: d/dphase, d/dfreq, d/dI, d/dQ
+    float ka, kb, kc, kd;   // freq row
+    float iphi, qphi;       // I/Q rows' d/dphase (diagonals are 1 - lpa)
+};
+
+__device__ __forceinline__ void pll_step(double ph, double f, double I, double Q, double p, const PllK &k,
+                                         PllEval &o) {
+    const double twopi = 2.0 * GPUD_PI;
+    const double r = ph - twopi * floor(ph * (1.0 / twopi));  // [0, 2pi): the serial loop's wrapped phase
+    float sf, cf;
+    __sincosf((float)(r - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sf, -cf
+    o.I1 = I + k.lpa * (p * -(double)cf - I);
+    o.Q1 = Q + k.lpa * (p * (double)sf - Q);
+    const float If = (float)o.I1, Qf = (float)o.Q1;
+    const float e = atan2f(Qf, If);
+    o.e = e;
+    double fn = f + k.beta * (double)e;
+    bool clamped = false;
+    if (fn < k.fmin) {
+        fn = k.fmin;
+        clamped = true;
+    } else if (fn > k.fmax) {
+        fn = k.fmax;
+        clamped = true;
     }
+    o.f1 = fn;
+    o.ph1 = ph + fn + k.alpha * (double)e;
+    // Jacobian
+    const float lpa = (float)k.lpa;
+    const float pf = (float)p;
+    const float r2 = fmaf(If, If, Qf * Qf);
+    const float inv = r2 > 0.f ? 1.0f / r2 : 0.f;
+    const float gI = -Qf * inv, gQ = If * inv;
+    const float dIphi = lpa * pf * sf;  // d/dphase of lpa*p*cos(phase)
+    const float dQphi = lpa * pf * cf;  // d/dphase of -lpa*p*sin(phase)
+    const float ePhi = fmaf(gI, dIphi, gQ * dQphi);
+    const float eI = gI * (1.f - lpa), eQ = gQ * (1.f - lpa);
+    const float g = clamped ? 0.f : (float)k.beta, h = clamped ? 0.f : 1.f;
+    const float ga = g + (float)k.alpha;
+    o.ka = g * ePhi;
+    o.kb = h;
+    o.kc = g * eI;
+    o.kd = g * eQ;
+    o.ja = 1.f + ga * ePhi;
+    o.jb = h;
+    o.jc = ga * eI;
+    o.jd = ga * eQ;
+    o.iphi = dIphi;
+    o.qphi = dQphi;
+}
+
+// (J, R) o (A, b): A <- J A, b <- J b + R, with J's sparsity.
+__device__ __forceinline__ void aff_push(Aff &m, const PllEval &o, float om, const float R[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float p0 = m.a[j], f0 = m.a[4 + j], i0 = m.a[8 + j], q0 = m.a[12 + j];
+        m.a[j] = fmaf(o.ja, p0, fmaf(o.jb, f0, fmaf(o.jc, i0, o.jd * q0)));
+        m.a[4 + j] = fmaf(o.ka, p0, fmaf(o.kb, f0, fmaf(o.kc, i0, o.kd * q0)));
+        m.a[8 + j] = fmaf(o.iphi, p0, om * i0);
+        m.a[12 + j] = fmaf(o.qphi, p0, om * q0);
+    }
+    const float p0 = m.b[0], f0 = m.b[1], i0 = m.b[2], q0 = m.b[3];
+    m.b[0] = fmaf(o.ja, p0, fmaf(o.jb, f0, fmaf(o.jc, i0, fmaf(o.jd, q0, R[0]))));
+    m.b[1] = fmaf(o.ka, p0, fmaf(o.kb, f0, fmaf(o.kc, i0, fmaf(o.kd, q0, R[1]))));
+    m.b[2] = fmaf(o.iphi, p0, fmaf(om, i0, R[2]));
+    m.b[3] = fmaf(o.qphi, p0, fmaf(om, q0, R[3]));
+}
+
+// hi o lo (lo applied first)
+__device__ __forceinline__ void aff_compose(Aff &out, const Aff &hi, const Aff &lo) {
+    Aff r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            r.a[4 * i + j] = fmaf(hi.a[4 * i], lo.a[j],
+                                  fmaf(hi.a[4 * i + 1], lo.a[4 + j],
+                                       fmaf(hi.a[4 * i + 2], lo.a[8 + j], hi.a[4 * i + 3] * lo.a[12 + j])));
+        }
+        r.b[i] = fmaf(hi.a[4 * i], lo.b[0],
+                      fmaf(hi.a[4 * i + 1], lo.b[1], fmaf(hi.a[4 * i + 2], lo.b[2], fmaf(hi.a[4 * i + 3], lo.b[3], hi.b[i]))));
+    }
+    out = r;
+}
+
+__device__ __forceinline__ void aff_shfl_up(Aff &dst, const Aff &src, int d) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) dst.a[i] = __shfl_up_sync(0xffffffffu, src.a[i], d);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst.b[i] = __shfl_up_sync(0xffffffffu, src.b[i], d);
+}
+
+struct TrajView {
+    double *ph, *f, *I, *Q;  // n+1 each
+};
+
+__device__ __forceinline__ void traj_load(const TrajView &v, bool guess, int t, double ph0, double f0, double I0,
+                                          double Q0, double &ph, double &f, double &I, double &Q) {
+    if (guess) {
+        ph = ph0 + (double)t * f0;
+        f = f0;
+        I = I0;
+        Q = Q0;
+    } else {
+        ph = v.ph[t];
+        f = v.f[t];
+        I = v.I[t];
+        Q = v.Q[t];
+    }
+}
+
+
+__device__ __forceinline__ void aff_identity(Aff &m) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) m.a[i] = (i % 5 == 0) ? 1.f : 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) m.b[i] = 0.f;
+}
+
+__device__ __forceinline__ void aff_load(Aff &m, const float *src) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) m.a[i] = src[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) m.b[i] = src[16 + i];
+}
+
+__device__ __forceinline__ void aff_store(float *dst, const Aff &m) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) dst[i] = m.a[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[16 + i] = m.b[i];
+}
+
+__device__ __forceinline__ void aff_apply(float out[4], const Aff &m, const float x[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        out[i] = fmaf(m.a[4 * i], x[0], fmaf(m.a[4 * i + 1], x[1], fmaf(m.a[4 * i + 2], x[2], fmaf(m.a[4 * i + 3], x[3], m.b[i]))));
+}
+
+// One channel-block per cluster of `gridDim.x / count` CTAs; the block's steps
+// are split evenly over all threads of the cluster.  Segment maps are scanned
+// within each warp (shuffles), across warps (shared memory) and across the
+// cluster's CTAs (distributed shared memory).
+__global__ void __launch_bounds__(kNewtonThreads, 2)
+k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
+             const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
+             double *__restrict__ traj, const int64_t *__restrict__ traj_off, int *__restrict__ done) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ float s_tot[kNW][20];     // warp totals
+    __shared__ float s_wex[kNW][20];     // exclusive warp prefix (A, b) within the CTA
+    __shared__ float s_cta[2][20];       // CTA total, double-buffered across iterations
+    __shared__ float s_max[kNW][4];
+    __shared__ float s_cmax[2][4];       // CTA max |delta|, double-buffered
+    __shared__ double s_sum[kNW][2];
+    __shared__ double s_csum[2];
+    const int csize = (int)cl.num_blocks();
+    const int crank = (int)cl.block_rank();
+    const int idx = blockIdx.x / csize;
+    if (idx >= count) return;  // uniform per cluster
+    const SlotBlock sb = sbt[list[idx]];
+    const int n = sb.n_disc;
+    if (n <= 0) {
+        if (threadIdx.x == 0 && crank == 0) done[idx] = 0;
+        return;  // uniform per cluster
+    }
+    const ChanParams &cp = prm[sb.slot];
+    ChanState &s = st[sb.slot];
+    const float *pil = wk + 3 * W + sb.comp_off;
+    const float *bpf = wk + 2 * W + sb.comp_off;
+    float *lr = wk + 4 * W + sb.comp_off;
+    const PllK k{cp.pll_alpha, cp.pll_beta, cp.pll_lpa, cp.pll_fmin, cp.pll_fmax};
+    const float om = (float)(1.0 - cp.pll_lpa);
+    const double ph0 = s.pll_phase, f0 = s.pll_freq, I0 = s.pll_i, Q0 = s.pll_q;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gthreads = csize * kNewtonThreads;
+    const int S = (n + gthreads - 1) / gthreads;
+    const int g = crank * kNewtonThreads + threadIdx.x;
+    const int t0 = min(n, g * S), t1 = min(n, t0 + S);
+    double *base = traj + traj_off[idx];
+    TrajView buf[2] = {{base, base + (n + 1), base + 2 * (n + 1), base + 3 * (n + 1)},
+                       {base + 4 * (n + 1), base + 5 * (n + 1), base + 6 * (n + 1), base + 7 * (n + 1)}};
+    int cur = -1;  // -1: the free-running guess
+    bool converged = false;
+    for (int it = 0; it < kMaxNewton && !converged; ++it) {
+        const int pb = it & 1;
+        const bool guess = cur < 0;
+        const TrajView &X = buf[guess ? 0 : cur];
+        const TrajView &Z = buf[guess ? 0 : 1 - cur];
+        // ---- phase A: this thread's segment map ---------------------------
+        Aff m;
+        aff_identity(m);
+        {
+            double ph, f, I, Q;
+            if (t0 < t1) traj_load(X, guess, t0, ph0, f0, I0, Q0, ph, f, I, Q);
+            for (int t = t0; t < t1; ++t) {
+                double nph, nf, nI, nQ;
+                traj_load(X, guess, t + 1, ph0, f0, I0, Q0, nph, nf, nI, nQ);
+                PllEval o;
+                pll_step(ph, f, I, Q, (double)__ldg(pil + t), k, o);
+                const float R[4] = {(float)(o.ph1 - nph), (float)(o.f1 - nf), (float)(o.I1 - nI),
+                                    (float)(o.Q1 - nQ)};
+                aff_push(m, o, om, R);
+                ph = nph;
+                f = nf;
+                I = nI;
+                Q = nQ;
+            }
+        }
+        // ---- phase B: scan ------------------------------------------------
+        Aff inc = m;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            Aff o;
+            aff_shfl_up(o, inc, d);
+            if (lane >= d) aff_compose(inc, inc, o);
+        }
+        Aff exl;  // lanes before this one
+        aff_shfl_up(exl, inc, 1);
+        if (lane == 0) aff_identity(exl);
+        if (lane == 31) aff_store(s_tot[warp], inc);
+        __syncthreads();
+        if (warp == 0) {
+            Aff wv;
+            if (lane < kNW) aff_load(wv, s_tot[lane]);
+            else aff_identity(wv);
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                Aff o;
+                aff_shfl_up(o, wv, d);
+                if (lane >= d) aff_compose(wv, wv, o);
+            }
+            Aff ex;
+            aff_shfl_up(ex, wv, 1);
+            if (lane == 0) aff_identity(ex);
+            if (lane < kNW) aff_store(s_wex[lane], ex);
+            if (lane == kNW - 1) aff_store(s_cta[pb], wv);
+        }
+        cl.sync();  // CTA totals of the whole cluster are visible
+        float dcta[4] = {0.f, 0.f, 0.f, 0.f};  // delta at this CTA's first step
+        for (int r = 0; r < crank; ++r) {
+            Aff rm;
+            aff_load(rm, cl.map_shared_rank(&s_cta[pb][0], r));
+            float tmp[4];
+            aff_apply(tmp, rm, dcta);
+            dcta[0] = tmp[0];
+            dcta[1] = tmp[1];
+            dcta[2] = tmp[2];
+            dcta[3] = tmp[3];
+        }
+        float dl[4];
+        {
+            Aff wx;
+            aff_load(wx, s_wex[warp]);
+            float dw[4];
+            aff_apply(dw, wx, dcta);
+            aff_apply(dl, exl, dw);
+        }
+        // ---- phase C: apply, write the next iterate ----------------------
+        float mx[4] = {0.f, 0.f, 0.f, 0.f};
+        {
+            double ph, f, I, Q;
+            if (t0 < t1) {
+                traj_load(X, guess, t0, ph0, f0, I0, Q0, ph, f, I, Q);
+                if (t0 == 0) {
+                    Z.ph[0] = ph0;
+                    Z.f[0] = f0;
+                    Z.I[0] = I0;
+                    Z.Q[0] = Q0;
+                }
+            }
+            for (int t = t0; t < t1; ++t) {
+                double nph, nf, nI, nQ;
+                traj_load(X, guess, t + 1, ph0, f0, I0, Q0, nph, nf, nI, nQ);
+                PllEval o;
+                pll_step(ph, f, I, Q, (double)__ldg(pil + t), k, o);
+                const float R[4] = {(float)(o.ph1 - nph), (float)(o.f1 - nf), (float)(o.I1 - nI),
+                                    (float)(o.Q1 - nQ)};
+                const float d0 = fmaf(o.ja, dl[0], fmaf(o.jb, dl[1], fmaf(o.jc, dl[2], fmaf(o.jd, dl[3], R[0]))));
+                const float d1 = fmaf(o.ka, dl[0], fmaf(o.kb, dl[1], fmaf(o.kc, dl[2], fmaf(o.kd, dl[3], R[1]))));
+                const float d2 = fmaf(o.iphi, dl[0], fmaf(om, dl[2], R[2]));
+                const float d3 = fmaf(o.qphi, dl[0], fmaf(om, dl[3], R[3]));
+                dl[0] = d0;
+                dl[1] = d1;
+                dl[2] = d2;
+                dl[3] = d3;
+                Z.ph[t + 1] = nph + (double)d0;
+                Z.f[t + 1] = nf + (double)d1;
+                Z.I[t + 1] = nI + (double)d2;
+                Z.Q[t + 1] = nQ + (double)d3;
+                mx[0] = fmaxf(mx[0], fabsf(d0));
+                mx[1] = fmaxf(mx[1], fabsf(d1));
+                mx[2] = fmaxf(mx[2], fabsf(d2));
+                mx[3] = fmaxf(mx[3], fabsf(d3));
+                ph = nph;
+                f = nf;
+                I = nI;
+                Q = nQ;
+            }
+        }
+        cur = guess ? 0 : 1 - cur;
+        // ---- convergence, agreed by every CTA of the cluster ---------------
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) mx[i] = fmaxf(mx[i], __shfl_xor_sync(0xffffffffu, mx[i], off));
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) s_max[warp][i] = mx[i];
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            float v = 0.f;
+            for (int w2 = 0; w2 < kNW; ++w2) v = fmaxf(v, s_max[w2][threadIdx.x]);
+            s_cmax[pb][threadIdx.x] = v;
+        }
+        cl.sync();  // also orders this iteration's trajectory writes before the next reads
+        float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+        for (int r = 0; r < csize; ++r) {
+            const float *rm = cl.map_shared_rank(&s_cmax[pb][0], r);
+            m0 = fmaxf(m0, rm[0]);
+            m1 = fmaxf(m1, rm[1]);
+            m2 = fmaxf(m2, rm[2]);
+            m3 = fmaxf(m3, rm[3]);
+        }
+        // Converged once the last correction is below what the outputs resolve:
+        // the float32 sin/cos/atan2 inside the loop leave a ~1e-10 floor.
+        converged = (m0 <= 1e-8f && m1 <= 1e-12f && m2 <= 1e-8f && m3 <= 1e-8f);
+    }
+    if (!converged) {
+        if (threadIdx.x == 0 && crank == 0) done[idx] = 0;
+        // No CTA may leave while a peer can still be reading its shared memory
+        // (the s_cmax reads just above).
+        cl.sync();
+        return;  // uniform per cluster: the serial kernel takes this block
+    }
+    // ---- outputs from the converged trajectory --------------------------
+    const TrajView &X = buf[cur];
+    const double twopi = 2.0 * GPUD_PI;
+    double es = 0.0, pp = 0.0;
+    for (int t = t0; t < t1; ++t) {
+        const float e = atan2f((float)X.Q[t + 1], (float)X.I[t + 1]);
+        es += fabs((double)e);
+        const double p = (double)pil[t];
+        pp += p * p;
+        double u = 2.0 * X.ph[t + 1];
+        u -= twopi * rint(u * (1.0 / twopi));
+        lr[t] = bpf[t] * (2.0f * sinf((float)u));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        es += __shfl_xor_sync(0xffffffffu, es, off);
+        pp += __shfl_xor_sync(0xffffffffu, pp, off);
+    }
+    if (lane == 0) {
+        s_sum[warp][0] = es;
+        s_sum[warp][1] = pp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w2 = 0; w2 < kNW; ++w2) {
+            a += s_sum[w2][0];
+            b += s_sum[w2][1];
+        }
+        s_csum[0] = a;
+        s_csum[1] = b;
+    }
+    cl.sync();
+    if (threadIdx.x == 0 && crank == 0) {
+        es = 0;
+        pp = 0;
+        for (int r = 0; r < csize; ++r) {
+            const double *rs = cl.map_shared_rank(&s_csum[0], r);
+            es += rs[0];
+            pp += rs[1];
+        }
+        double ph = X.ph[n];
+        ph -= twopi * floor(ph * (1.0 / twopi));
+        pll_finish(s, cp, n, ph, X.f[n], X.I[n], X.Q[n], es, pp);
+        s.pll_path = 1;
+        done[idx] = 1;
+    }
+    cl.sync();  // keep shared memory alive until rank 0 has read it
 }
 
 // L-R lowpass and L/R matrix when stereo is enabled; otherwise the 15 kHz mono
@@ -690,7 +1120,7 @@ k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, Ch
         o.coherence = s.coherence;
         o.pilot_hz = s.pilot_hz;
         o.err_avg = s.last_err_avg;
-        o.status = 0;
+        o.status = (cp.mode == 3 && sb.n_disc > 0) ? s.pll_path : 0;
     }
 }
 
@@ -755,10 +1185,30 @@ cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const Sl
 }
 
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W) {
-    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W);
+                       ChanState *st, float *wk, int W, const int *done) {
+    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W, done);
     return cudaGetLastError();
 }
+
+cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
+                              const ChanParams *prm, ChanState *st, float *wk, int W, double *traj,
+                              const int64_t *traj_off, int *done) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(count * cluster), 1, 1);
+    cfg.blockDim = dim3(kNewtonThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = sm;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_pll_newton, list, count, sbt, prm, st, wk, W, traj, traj_off, done);
+}
+
+int pll_newton_threads() { return kNewtonThreads; }
 
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,

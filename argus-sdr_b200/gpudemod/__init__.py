@@ -220,6 +220,7 @@ class ChannelRunner:
             "coherence": res.coherence,
             "pilot_hz": res.pilot_hz,
             "err_avg": res.err_avg,
+            "pll_path": res.pll_path,
         }
 
     def stats(self) -> dict:
@@ -229,6 +230,9 @@ class ChannelRunner:
 
     def set_host_outputs(self, on: bool):
         _check(self._r, lib.gpud_runner_set_host_outputs(self._r, 1 if on else 0))
+
+    def set_pll_solver(self, parallel: bool):
+        _check(self._r, lib.gpud_runner_set_pll_solver(self._r, 1 if parallel else 0))
 
     def set_profiling(self, on: bool):
         _check(self._r, lib.gpud_runner_set_profiling(self._r, 1 if on else 0))

@@ -52,6 +52,8 @@ class ChannelResult(C.Structure):
         ("iq", C.POINTER(GPUDFloat2)),
         ("audio", C.POINTER(C.c_float)),
         ("rds", C.POINTER(GPUDFloat2)),
+        ("pll_path", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -122,6 +124,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_reset_signal": (i, [P, C.c_int64]),
         "gpud_runner_set_host_outputs": (i, [P, i]),
         "gpud_runner_set_profiling": (i, [P, i]),
+        "gpud_runner_set_pll_solver": (i, [P, i]),
         "gpud_runner_stage_times": (i, [P, C.POINTER(StageTime), i, pi]),
         "gpud_runner_reset_all_signals": (i, [P]),
         "gpud_streaming_config_hash": (C.c_uint64, [C.c_int64, i, i, i]),

@@ -190,6 +190,8 @@ typedef struct {
     const gpud_float2 *iq; /* host; NULL unless GPUD_CH_EMIT_IQ */
     const float *audio;    /* host */
     const gpud_float2 *rds;
+    int32_t pll_path;      /* WFM_STEREO: 1 parallel-in-time PLL solver, 2 serial loop */
+    int32_t pad;
 } gpud_channel_result;
 
 /* Runner statistics. */
@@ -252,6 +254,13 @@ GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r);
  * device arena (no D2H; for consumers that read them on the GPU) and the
  * pointers of gpud_channel_result are device pointers.  Default on. */
 GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on);
+
+/* Stereo pilot PLL solver: 1 (default) solves each block's loop trajectory in
+ * parallel (Newton iteration over the block with an associative scan) and
+ * falls back per channel to the serial loop when it has not converged; 0 runs
+ * the serial loop only.  Both compute the same recurrence
+ * (recorder/streamer.go:1588-1613). */
+GPUD_API int GPUD_CALL gpud_runner_set_pll_solver(gpud_runner *r, int parallel);
 
 /* Per-kernel device time of the last block (CUDA events between the
  * launches on the runner stream); enable with gpud_runner_set_profiling. */

@@ -200,3 +200,60 @@ def test_admission_by_device_memory_budget(cuda):
         r.admit(9, 0.0, 250_000.0, 312_500, 256, G.MODE_WFM_STEREO, G.CH_RDS)
     finally:
         r.close()
+
+
+def test_parallel_pll_equals_serial_pll(cuda):
+    """The Newton/scan PLL solver reproduces the serial loop (same recurrence)
+    and takes over once the loop is locked."""
+    blocks, _ = _scene_blocks(8)
+    fs = 2_400_000
+    spec = (1, 300_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS)
+    rp = G.ChannelRunner(fs, 262_144, max_channels=2)
+    rs = G.ChannelRunner(fs, 262_144, max_channels=2)
+    rs.set_pll_solver(False)
+    sp, ss = rp.admit(*spec), rs.admit(*spec)
+    paths = []
+    try:
+        for x in blocks:
+            rp.process_block(x)
+            rs.process_block(x)
+            a, b = rp.result(sp), rs.result(ss)
+            paths.append(a["pll_path"])
+            assert b["pll_path"] == 2
+            assert rel_l2(a["audio"], b["audio"]) <= 1e-6, rel_l2(a["audio"], b["audio"])
+            assert a["locked"] == b["locked"] and a["stereo"] == b["stereo"]
+            assert abs(a["coherence"] - b["coherence"]) <= 1e-5
+        assert all(p == 1 for p in paths[2:]), paths
+    finally:
+        rp.close()
+        rs.close()
+
+
+def test_parallel_pll_fallback_and_clusters(cuda):
+    """Several stereo channels (split over thread-block clusters), some without
+    a pilot: blocks that do not converge fall back to the serial loop; every
+    block matches the serial-only solver."""
+    blocks, _ = _scene_blocks(6)
+    fs = 2_400_000
+    specs = [(1, 300_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS),
+             (2, -500_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS),
+             (3, 800_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, 0)]
+    rp = G.ChannelRunner(fs, 262_144, max_channels=4)
+    rs = G.ChannelRunner(fs, 262_144, max_channels=4)
+    rs.set_pll_solver(False)
+    sp = [rp.admit(*s) for s in specs]
+    ss = [rs.admit(*s) for s in specs]
+    paths = set()
+    try:
+        for x in blocks:
+            rp.process_block(x)
+            rs.process_block(x)
+            for a_slot, b_slot in zip(sp, ss):
+                a, b = rp.result(a_slot), rs.result(b_slot)
+                paths.add(a["pll_path"])
+                assert rel_l2(a["audio"], b["audio"]) <= 1e-6, rel_l2(a["audio"], b["audio"])
+                assert a["locked"] == b["locked"] and a["stereo"] == b["stereo"]
+        assert 1 in paths
+    finally:
+        rp.close()
+        rs.close()
