@@ -100,7 +100,7 @@ struct ChanState {
     // RDS baseband stream
     int64_t rds_count;   // composite samples consumed
     int32_t rds_hist_len;
-    int32_t pad2;
+    int32_t pll_iters;   // Newton iterations of the last parallel solve
 };
 
 // Per-block per-slot descriptor (host-built; all integer bookkeeping is
@@ -130,7 +130,8 @@ struct DevResult {
     int32_t flags;
     float coherence, pilot_hz, err_avg;
     int32_t status;
-    int32_t pad[3];
+    int32_t pll_iters;
+    int32_t pad[2];
 };
 
 // Exact sequential float64 accumulation x_k = fl(x_{k-1} + inc), x_0 = 0

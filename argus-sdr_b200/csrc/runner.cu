@@ -633,7 +633,7 @@ GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offse
 // ---------------------------------------------------------------------------
 int gpud::dense_smem_bytes_host(int P, int L) {
     int M = 256 + L - 1;
-    int Mp = M + (M >> 3) + 1;
+    int Mp = (M + (M >> 3) + 1) | 1;
     int z = P * Mp * 8;
     int red = 8 * (256 + 32) * 8;
     return std::max(z, red) + P * L * 4 + 16;
@@ -912,7 +912,7 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
             int max_n = 0;
             for (int i : pl.pll_list) max_n = std::max(max_n, pl.sbs[(size_t)i].n_disc);
             int cluster = 1;
-            while (cluster < 8 && nch * cluster * 2 <= 2 * r->num_sms &&
+            while (cluster < 8 && nch * cluster * 2 <= 3 * r->num_sms &&
                    max_n / (cluster * 2 * pll_newton_threads()) >= 8)
                 cluster *= 2;
             prof_mark(r, "pll_newton");
@@ -1182,6 +1182,7 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->pilot_hz = res->pilot_hz;
     out->err_avg = res->err_avg;
     out->pll_path = res->status;
+    out->pll_iters = res->pll_iters;
     const char *base = r->host_outputs ? r->h_out : r->d_out;
     out->audio = (const float *)(base + r->off_audio) + sb.audio_off;
     out->rds = (const gpud_float2 *)(base + r->off_rds) + sb.rds_off;

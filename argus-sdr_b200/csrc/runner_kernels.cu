@@ -40,9 +40,12 @@ constexpr int kDenseR = 8;
 constexpr int kDenseOT = 32 * kDenseR;  // outputs per tile
 constexpr int kDenseThreads = 256;
 
+// Row stride in float2: one pad slot per 8 (lane-strided window reads stay
+// conflict-free) and odd (the staging stores, which walk down a column with
+// consecutive threads on consecutive phases, spread over all banks).
 __host__ __device__ inline int dense_row_stride(int L) {
     int M = kDenseOT + L - 1;
-    return M + (M >> 3) + 1;
+    return (M + (M >> 3) + 1) | 1;
 }
 
 __host__ __device__ inline int dense_smem_bytes(int P, int L) {
@@ -92,13 +95,49 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     const uint64_t inc = cp.inc_q;
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
     const int H = sb.hist_len;
-    const float invP = 1.0f / (float)P;
-    const int total = P * M;
-    for (int f = threadIdx.x; f < total; f += kDenseThreads) {
-        int mr = (int)(((float)f + 0.5f) * invP);
-        int p = f - mr * P;
-        int i = s0 + (m_base + mr) * D - p;
-        Z[p * Mp + mr + (mr >> 3)] = shifted_sample(i, n, x, u0, inc, hist, H);
+    // Staging.  Tile sample i' = 0..M*D-1 is block sample i = ibase + i' and
+    // lands in Z[p][m] with m = i'/D, p = D-1 - i'%D.  Thread t takes
+    // i' = t + 256*k: consecutive threads hit consecutive phases (odd row
+    // stride: no bank conflicts) and its rotator advances by w = exp(j*256*inc)
+    // per k, re-anchored from the exact Q0.64 phase every 8 steps.
+    const int total = P * M;  // P == D in the dense form
+    const int ibase = s0 + m_base * D - (D - 1);
+    const float invD = 1.0f / (float)D;
+    const float2 w256 = q64_phasor((uint64_t)kDenseThreads * inc);
+    float2 rot = make_float2(1.f, 0.f);
+    constexpr int U = 4;
+    for (int k0 = 0; k0 * kDenseThreads < total; k0 += U) {
+        float2 xv[U];
+        int zi[U], ii[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int ip = (int)threadIdx.x + (k0 + u) * kDenseThreads;
+            const int i = ibase + ip;
+            const int mr = (int)(((float)ip + 0.5f) * invD);
+            const int p = D - 1 - (ip - mr * D);
+            zi[u] = ip < total ? p * Mp + mr + (mr >> 3) : -1;
+            ii[u] = i;
+            xv[u] = (ip < total && i >= 0 && i < n) ? __ldg(x + i) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if ((k & 7) == 0) {
+                rot = q64_phasor(u0 + (uint64_t)(int64_t)(ibase + (int)threadIdx.x + k * kDenseThreads) * inc);
+            } else {
+                rot = cmulf(rot, w256);
+            }
+            if (zi[u] < 0) continue;
+            const int i = ii[u];
+            float2 v;
+            if (i >= 0) {
+                v = i < n ? cmulf(xv[u], rot) : make_float2(0.f, 0.f);
+            } else {
+                const int hi = H + i;
+                v = hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
+            }
+            Z[zi[u]] = v;
+        }
     }
     __syncthreads();
 
@@ -351,6 +390,104 @@ k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
     }
 }
 
+struct PllK {
+    double alpha, beta;
+    float lpa;
+    double dfmin, dfmax;  // frequency clamp as deviations from the block-start frequency
+    uint64_t q0, qf;      // block-start phase and frequency in Q0.64 turns
+};
+
+// One loop step (recorder/streamer.go:1588-1613) in deviation form: the phase
+// is phase0 + t*freq0 + dphi, the frequency freq0 + df (dphi, df float64); the
+// ramp phase0 + t*freq0 is exact in Q0.64 turns, so the sin/cos argument needs
+// no float64 range reduction.  The I/Q lowpass states are float32.  The serial
+// loop and the Newton solver both use this step, so they iterate the same map.
+struct PllEval {
+    double dphi1, df1;
+    float I1, Q1;
+    float e;
+    float ja, jb, jc, jd;   // phase row: d/dphase, d/dfreq, d/dI, d/dQ
+    float ka, kb, kc, kd;   // freq row
+    float iphi, qphi;       // I/Q rows' d/dphase (diagonals are 1 - lpa)
+};
+
+__device__ __forceinline__ void pll_angle(const PllK &k, int t, double dphi, float &s, float &c) {
+    const uint64_t q = k.q0 + (uint64_t)t * k.qf;
+    const float h = (float)(int32_t)(q >> 32) * 4.656612873077393e-10f + (float)(dphi * (1.0 / GPUD_PI));
+    __sincosf(h * 3.14159265358979f, &s, &c);  // |angle| <= pi + |dphi|
+}
+
+template <bool kJac>
+__device__ __forceinline__ void pll_step(int t, double dphi, double df, float I, float Q, float p, const PllK &k,
+                                         PllEval &o) {
+    float sn, cs;
+    pll_angle(k, t, dphi, sn, cs);
+    o.I1 = fmaf(k.lpa, fmaf(p, cs, -I), I);
+    o.Q1 = fmaf(k.lpa, fmaf(p, -sn, -Q), Q);
+    const float e = atan2f(o.Q1, o.I1);
+    o.e = e;
+    double d = df + k.beta * (double)e;
+    bool clamped = false;
+    if (d < k.dfmin) {
+        d = k.dfmin;
+        clamped = true;
+    } else if (d > k.dfmax) {
+        d = k.dfmax;
+        clamped = true;
+    }
+    o.df1 = d;
+    o.dphi1 = dphi + d + k.alpha * (double)e;
+    if (kJac) {
+        const float r2 = fmaf(o.I1, o.I1, o.Q1 * o.Q1);
+        const float inv = r2 > 0.f ? __frcp_rn(r2) : 0.f;
+        const float gI = -o.Q1 * inv, gQ = o.I1 * inv;
+        const float dIphi = -k.lpa * p * sn;  // d/dphase of lpa*p*cos(phase)
+        const float dQphi = -k.lpa * p * cs;  // d/dphase of -lpa*p*sin(phase)
+        const float ePhi = fmaf(gI, dIphi, gQ * dQphi);
+        const float om = 1.f - k.lpa;
+        const float eI = gI * om, eQ = gQ * om;
+        const float g = clamped ? 0.f : (float)k.beta, h = clamped ? 0.f : 1.f;
+        const float ga = g + (float)k.alpha;
+        o.ka = g * ePhi;
+        o.kb = h;
+        o.kc = g * eI;
+        o.kd = g * eQ;
+        o.ja = 1.f + ga * ePhi;
+        o.jb = h;
+        o.jc = ga * eI;
+        o.jd = ga * eQ;
+        o.iphi = dIphi;
+        o.qphi = dQphi;
+    }
+}
+
+__device__ __forceinline__ PllK pll_consts(const ChanParams &cp, const ChanState &s) {
+    PllK k;
+    k.alpha = cp.pll_alpha;
+    k.beta = cp.pll_beta;
+    k.lpa = (float)cp.pll_lpa;
+    k.dfmin = cp.pll_fmin - s.pll_freq;
+    k.dfmax = cp.pll_fmax - s.pll_freq;
+    k.q0 = rad_to_q64(s.pll_phase);
+    k.qf = rad_to_q64(s.pll_freq);
+    return k;
+}
+
+// Loop phase after t steps, wrapped to [0, 2pi) (the serial loop's range).
+__device__ __forceinline__ double pll_phase_at(const PllK &k, int t, double dphi) {
+    const uint64_t q = k.q0 + (uint64_t)t * k.qf;
+    double ph = (double)q * (2.0 * GPUD_PI / 18446744073709551616.0) + dphi;
+    ph -= (2.0 * GPUD_PI) * floor(ph * (1.0 / (2.0 * GPUD_PI)));
+    return ph;
+}
+
+// 2*sin(2*phase) of the loop phase after t steps, float32 (lr = bpf * that).
+__device__ __forceinline__ float pll_two_sin2(const PllK &k, int t, double dphi) {
+    const uint64_t q2 = 2 * (k.q0 + (uint64_t)t * k.qf);
+    const float h = (float)(int32_t)(q2 >> 32) * 4.656612873077393e-10f + (float)(dphi * (2.0 / GPUD_PI));
+    return 2.0f * sinpif(h);
+}
+
 // End of one stereoDecodeStateful call: store the loop state, update errAvg
 // (EMA per call), the coherence / frequency / errAvg lock test and the
 // hysteresis counters (streamer.go:1614-1635, 1363-1380).
@@ -413,38 +550,31 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
     float *lr = wk + 4 * W + sb.comp_off;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nc = (n + kPllChunk - 1) / kPllChunk;
-    const double twopi = 2.0 * GPUD_PI;
     double pp = 0.0;  // pilot power, accumulated by warp 1
     // prologue: chunk 0 into buffer 0
     if (warp == 1) {
         for (int q = lane; q < min(n, kPllChunk); q += 32) s_pil[0][q] = pil[q];
     }
     __syncthreads();
-    double ph = s.pll_phase, fr = s.pll_freq, I = s.pll_i, Q = s.pll_q, es = 0.0;
-    const double alpha = cp.pll_alpha, beta = cp.pll_beta, lpa = cp.pll_lpa;
-    const double fmin = cp.pll_fmin, fmax = cp.pll_fmax;
+    const PllK k = pll_consts(cp, s);
+    double dphi = 0.0, df = 0.0, es = 0.0;
+    float I = (float)s.pll_i, Q = (float)s.pll_q;
     for (int c = 0; c <= nc; ++c) {
         if (warp == 0) {
             if (lane == 0 && c < nc) {
                 const float *sp = s_pil[c & 1];
                 float *th = s_th[c & 1];
-                const int len = min(kPllChunk, n - c * kPllChunk);
+                const int base = c * kPllChunk;
+                const int len = min(kPllChunk, n - base);
                 for (int q = 0; q < len; ++q) {
-                    const double p = (double)sp[q];
-                    float sf, cf;
-                    __sincosf((float)(ph - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sin/-cos(ph - pi)
-                    I += lpa * (p * -(double)cf - I);
-                    Q += lpa * (p * (double)sf - Q);
-                    const double err = (double)atan2f((float)Q, (float)I);
-                    fr += beta * err;
-                    fr = fr < fmin ? fmin : (fr > fmax ? fmax : fr);
-                    ph += fr + alpha * err;
-                    if (ph > twopi) ph -= twopi;
-                    else if (ph < 0.0) ph += twopi;
-                    es += fabs(err);
-                    double t2 = 2.0 * ph;  // [0, 4pi] -> [-pi, pi]
-                    t2 -= twopi * rint(t2 * (1.0 / twopi));
-                    th[q] = (float)t2;
+                    PllEval o;
+                    pll_step<false>(base + q, dphi, df, I, Q, sp[q], k, o);
+                    dphi = o.dphi1;
+                    df = o.df1;
+                    I = o.I1;
+                    Q = o.Q1;
+                    es += fabs((double)o.e);
+                    th[q] = pll_two_sin2(k, base + q + 1, dphi);
                 }
             }
         } else {
@@ -457,7 +587,7 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
                 for (int q = lane; q < len; q += 32) {
                     const double p = (double)sp[q];
                     pp += p * p;
-                    lr[base + q] = bpf[base + q] * (2.0f * sinf(th[q]));
+                    lr[base + q] = bpf[base + q] * th[q];
                 }
             }
             __syncwarp();
@@ -476,7 +606,7 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    pll_finish(s, cp, n, ph, fr, I, Q, es, s_red[0]);
+    pll_finish(s, cp, n, pll_phase_at(k, n, dphi), s.pll_freq + df, (double)I, (double)Q, es, s_red[0]);
     s.pll_path = 2;
 }
 
@@ -499,70 +629,10 @@ constexpr int kNewtonThreads = 256;
 constexpr int kMaxNewton = 8;
 constexpr int kNW = kNewtonThreads / 32;
 
-struct PllK {
-    double alpha, beta, lpa, fmin, fmax;
-};
-
 struct Aff {
     float a[16];  // row-major, state order (phase, freq, I, Q)
     float b[4];
 };
-
-// One loop step at (ph, f, I, Q) with pilot p: new state and the Jacobian's
-// nonzero entries.  Mirrors k_pll's arithmetic exactly.
-struct PllEval {
-    double ph1, f1, I1, Q1;
-    float e;
-    float ja, jb, jc, jd;   // phase row: d/dphase, d/dfreq, d/dI, d/dQ
-    float ka, kb, kc, kd;   // freq row
-    float iphi, qphi;       // I/Q rows' d/dphase (diagonals are 1 - lpa)
-};
-
-__device__ __forceinline__ void pll_step(double ph, double f, double I, double Q, double p, const PllK &k,
-                                         PllEval &o) {
-    const double twopi = 2.0 * GPUD_PI;
-    const double r = ph - twopi * floor(ph * (1.0 / twopi));  // [0, 2pi): the serial loop's wrapped phase
-    float sf, cf;
-    __sincosf((float)(r - GPUD_PI), &sf, &cf);  // sin/cos(ph) = -sf, -cf
-    o.I1 = I + k.lpa * (p * -(double)cf - I);
-    o.Q1 = Q + k.lpa * (p * (double)sf - Q);
-    const float If = (float)o.I1, Qf = (float)o.Q1;
-    const float e = atan2f(Qf, If);
-    o.e = e;
-    double fn = f + k.beta * (double)e;
-    bool clamped = false;
-    if (fn < k.fmin) {
-        fn = k.fmin;
-        clamped = true;
-    } else if (fn > k.fmax) {
-        fn = k.fmax;
-        clamped = true;
-    }
-    o.f1 = fn;
-    o.ph1 = ph + fn + k.alpha * (double)e;
-    // Jacobian
-    const float lpa = (float)k.lpa;
-    const float pf = (float)p;
-    const float r2 = fmaf(If, If, Qf * Qf);
-    const float inv = r2 > 0.f ? 1.0f / r2 : 0.f;
-    const float gI = -Qf * inv, gQ = If * inv;
-    const float dIphi = lpa * pf * sf;  // d/dphase of lpa*p*cos(phase)
-    const float dQphi = lpa * pf * cf;  // d/dphase of -lpa*p*sin(phase)
-    const float ePhi = fmaf(gI, dIphi, gQ * dQphi);
-    const float eI = gI * (1.f - lpa), eQ = gQ * (1.f - lpa);
-    const float g = clamped ? 0.f : (float)k.beta, h = clamped ? 0.f : 1.f;
-    const float ga = g + (float)k.alpha;
-    o.ka = g * ePhi;
-    o.kb = h;
-    o.kc = g * eI;
-    o.kd = g * eQ;
-    o.ja = 1.f + ga * ePhi;
-    o.jb = h;
-    o.jc = ga * eI;
-    o.jd = ga * eQ;
-    o.iphi = dIphi;
-    o.qphi = dQphi;
-}
 
 // (J, R) o (A, b): A <- J A, b <- J b + R, with J's sparsity.
 __device__ __forceinline__ void aff_push(Aff &m, const PllEval &o, float om, const float R[4]) {
@@ -605,25 +675,16 @@ __device__ __forceinline__ void aff_shfl_up(Aff &dst, const Aff &src, int d) {
     for (int i = 0; i < 4; ++i) dst.b[i] = __shfl_up_sync(0xffffffffu, src.b[i], d);
 }
 
-struct TrajView {
-    double *ph, *f, *I, *Q;  // n+1 each
+// One trajectory entry (state after t steps), deviation form.
+struct TStep {
+    double dphi, df;
+    float I, Q;
 };
 
-__device__ __forceinline__ void traj_load(const TrajView &v, bool guess, int t, double ph0, double f0, double I0,
-                                          double Q0, double &ph, double &f, double &I, double &Q) {
-    if (guess) {
-        ph = ph0 + (double)t * f0;
-        f = f0;
-        I = I0;
-        Q = Q0;
-    } else {
-        ph = v.ph[t];
-        f = v.f[t];
-        I = v.I[t];
-        Q = v.Q[t];
-    }
+__device__ __forceinline__ TStep tstep_load(const TStep *X, bool guess, int t, float I0, float Q0) {
+    if (guess) return TStep{0.0, 0.0, I0, Q0};  // free-running ramp, constant lowpass states
+    return X[t];
 }
-
 
 __device__ __forceinline__ void aff_identity(Aff &m) {
 #pragma unroll
@@ -656,7 +717,7 @@ __device__ __forceinline__ void aff_apply(float out[4], const Aff &m, const floa
 // are split evenly over all threads of the cluster.  Segment maps are scanned
 // within each warp (shuffles), across warps (shared memory) and across the
 // cluster's CTAs (distributed shared memory).
-__global__ void __launch_bounds__(kNewtonThreads, 2)
+__global__ void __launch_bounds__(kNewtonThreads, 3)
 k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
              const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
              double *__restrict__ traj, const int64_t *__restrict__ traj_off, int *__restrict__ done) {
@@ -684,42 +745,44 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     const float *pil = wk + 3 * W + sb.comp_off;
     const float *bpf = wk + 2 * W + sb.comp_off;
     float *lr = wk + 4 * W + sb.comp_off;
-    const PllK k{cp.pll_alpha, cp.pll_beta, cp.pll_lpa, cp.pll_fmin, cp.pll_fmax};
-    const float om = (float)(1.0 - cp.pll_lpa);
-    const double ph0 = s.pll_phase, f0 = s.pll_freq, I0 = s.pll_i, Q0 = s.pll_q;
+    const PllK k = pll_consts(cp, s);
+    const float om = 1.f - k.lpa;
+    const float I0 = (float)s.pll_i, Q0 = (float)s.pll_q;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gthreads = csize * kNewtonThreads;
     const int S = (n + gthreads - 1) / gthreads;
-    const int g = crank * kNewtonThreads + threadIdx.x;
+    const int g = crank * kNewtonThreads + (int)threadIdx.x;
     const int t0 = min(n, g * S), t1 = min(n, t0 + S);
-    double *base = traj + traj_off[idx];
-    TrajView buf[2] = {{base, base + (n + 1), base + 2 * (n + 1), base + 3 * (n + 1)},
-                       {base + 4 * (n + 1), base + 5 * (n + 1), base + 6 * (n + 1), base + 7 * (n + 1)}};
+    TStep *B0 = reinterpret_cast<TStep *>(traj + traj_off[idx]);
+    TStep *B1 = B0 + (n + 1);
     int cur = -1;  // -1: the free-running guess
     bool converged = false;
+    int iters = 0;
     for (int it = 0; it < kMaxNewton && !converged; ++it) {
+        iters = it + 1;
         const int pb = it & 1;
         const bool guess = cur < 0;
-        const TrajView &X = buf[guess ? 0 : cur];
-        const TrajView &Z = buf[guess ? 0 : 1 - cur];
+        const TStep *X = (guess || cur == 0) ? B0 : B1;
+        TStep *Z = (guess || cur == 1) ? B0 : B1;
         // ---- phase A: this thread's segment map ---------------------------
         Aff m;
         aff_identity(m);
-        {
-            double ph, f, I, Q;
-            if (t0 < t1) traj_load(X, guess, t0, ph0, f0, I0, Q0, ph, f, I, Q);
+        if (t0 < t1) {
+            TStep a = tstep_load(X, guess, t0, I0, Q0);
+            TStep b = tstep_load(X, guess, t0 + 1, I0, Q0);
+            float pt = __ldg(pil + t0);
             for (int t = t0; t < t1; ++t) {
-                double nph, nf, nI, nQ;
-                traj_load(X, guess, t + 1, ph0, f0, I0, Q0, nph, nf, nI, nQ);
+                TStep c = b;
+                float pn = pt;
+                if (t + 2 <= t1) c = tstep_load(X, guess, t + 2, I0, Q0);
+                if (t + 1 < t1) pn = __ldg(pil + t + 1);
                 PllEval o;
-                pll_step(ph, f, I, Q, (double)__ldg(pil + t), k, o);
-                const float R[4] = {(float)(o.ph1 - nph), (float)(o.f1 - nf), (float)(o.I1 - nI),
-                                    (float)(o.Q1 - nQ)};
+                pll_step<true>(t, a.dphi, a.df, a.I, a.Q, pt, k, o);
+                const float R[4] = {(float)(o.dphi1 - b.dphi), (float)(o.df1 - b.df), o.I1 - b.I, o.Q1 - b.Q};
                 aff_push(m, o, om, R);
-                ph = nph;
-                f = nf;
-                I = nI;
-                Q = nQ;
+                a = b;
+                b = c;
+                pt = pn;
             }
         }
         // ---- phase B: scan ------------------------------------------------
@@ -773,24 +836,19 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
         }
         // ---- phase C: apply, write the next iterate ----------------------
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
-        {
-            double ph, f, I, Q;
-            if (t0 < t1) {
-                traj_load(X, guess, t0, ph0, f0, I0, Q0, ph, f, I, Q);
-                if (t0 == 0) {
-                    Z.ph[0] = ph0;
-                    Z.f[0] = f0;
-                    Z.I[0] = I0;
-                    Z.Q[0] = Q0;
-                }
-            }
+        if (t0 < t1) {
+            if (t0 == 0) Z[0] = TStep{0.0, 0.0, I0, Q0};
+            TStep a = tstep_load(X, guess, t0, I0, Q0);
+            TStep b = tstep_load(X, guess, t0 + 1, I0, Q0);
+            float pt = __ldg(pil + t0);
             for (int t = t0; t < t1; ++t) {
-                double nph, nf, nI, nQ;
-                traj_load(X, guess, t + 1, ph0, f0, I0, Q0, nph, nf, nI, nQ);
+                TStep c = b;
+                float pn = pt;
+                if (t + 2 <= t1) c = tstep_load(X, guess, t + 2, I0, Q0);
+                if (t + 1 < t1) pn = __ldg(pil + t + 1);
                 PllEval o;
-                pll_step(ph, f, I, Q, (double)__ldg(pil + t), k, o);
-                const float R[4] = {(float)(o.ph1 - nph), (float)(o.f1 - nf), (float)(o.I1 - nI),
-                                    (float)(o.Q1 - nQ)};
+                pll_step<true>(t, a.dphi, a.df, a.I, a.Q, pt, k, o);
+                const float R[4] = {(float)(o.dphi1 - b.dphi), (float)(o.df1 - b.df), o.I1 - b.I, o.Q1 - b.Q};
                 const float d0 = fmaf(o.ja, dl[0], fmaf(o.jb, dl[1], fmaf(o.jc, dl[2], fmaf(o.jd, dl[3], R[0]))));
                 const float d1 = fmaf(o.ka, dl[0], fmaf(o.kb, dl[1], fmaf(o.kc, dl[2], fmaf(o.kd, dl[3], R[1]))));
                 const float d2 = fmaf(o.iphi, dl[0], fmaf(om, dl[2], R[2]));
@@ -799,18 +857,14 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
                 dl[1] = d1;
                 dl[2] = d2;
                 dl[3] = d3;
-                Z.ph[t + 1] = nph + (double)d0;
-                Z.f[t + 1] = nf + (double)d1;
-                Z.I[t + 1] = nI + (double)d2;
-                Z.Q[t + 1] = nQ + (double)d3;
+                Z[t + 1] = TStep{b.dphi + (double)d0, b.df + (double)d1, b.I + d2, b.Q + d3};
                 mx[0] = fmaxf(mx[0], fabsf(d0));
                 mx[1] = fmaxf(mx[1], fabsf(d1));
                 mx[2] = fmaxf(mx[2], fabsf(d2));
                 mx[3] = fmaxf(mx[3], fabsf(d3));
-                ph = nph;
-                f = nf;
-                I = nI;
-                Q = nQ;
+                a = b;
+                b = c;
+                pt = pn;
             }
         }
         cur = guess ? 0 : 1 - cur;
@@ -837,29 +891,30 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             m2 = fmaxf(m2, rm[2]);
             m3 = fmaxf(m3, rm[3]);
         }
-        // Converged once the last correction is below what the outputs resolve:
-        // the float32 sin/cos/atan2 inside the loop leave a ~1e-10 floor.
-        converged = (m0 <= 1e-8f && m1 <= 1e-12f && m2 <= 1e-8f && m3 <= 1e-8f);
+        // Converged once the last correction is below what the outputs resolve
+        // (the float32 sin/cos/atan2 and lowpass states leave a floor near
+        // 1e-10 rad and 1e-9 in I/Q).
+        converged = (m0 <= 1e-8f && m1 <= 1e-12f && m2 <= 1e-7f && m3 <= 1e-7f);
     }
     if (!converged) {
-        if (threadIdx.x == 0 && crank == 0) done[idx] = 0;
+        if (threadIdx.x == 0 && crank == 0) {
+            done[idx] = 0;
+            s.pll_iters = iters;
+        }
         // No CTA may leave while a peer can still be reading its shared memory
         // (the s_cmax reads just above).
         cl.sync();
         return;  // uniform per cluster: the serial kernel takes this block
     }
     // ---- outputs from the converged trajectory --------------------------
-    const TrajView &X = buf[cur];
-    const double twopi = 2.0 * GPUD_PI;
+    const TStep *X = cur == 0 ? B0 : B1;
     double es = 0.0, pp = 0.0;
     for (int t = t0; t < t1; ++t) {
-        const float e = atan2f((float)X.Q[t + 1], (float)X.I[t + 1]);
-        es += fabs((double)e);
+        const TStep x1 = X[t + 1];
+        es += fabs((double)atan2f(x1.Q, x1.I));
         const double p = (double)pil[t];
         pp += p * p;
-        double u = 2.0 * X.ph[t + 1];
-        u -= twopi * rint(u * (1.0 / twopi));
-        lr[t] = bpf[t] * (2.0f * sinf((float)u));
+        lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x1.dphi);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -889,10 +944,10 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             es += rs[0];
             pp += rs[1];
         }
-        double ph = X.ph[n];
-        ph -= twopi * floor(ph * (1.0 / twopi));
-        pll_finish(s, cp, n, ph, X.f[n], X.I[n], X.Q[n], es, pp);
+        const TStep xn = X[n];
+        pll_finish(s, cp, n, pll_phase_at(k, n, xn.dphi), s.pll_freq + xn.df, (double)xn.I, (double)xn.Q, es, pp);
         s.pll_path = 1;
+        s.pll_iters = iters;
         done[idx] = 1;
     }
     cl.sync();  // keep shared memory alive until rank 0 has read it
@@ -1121,6 +1176,7 @@ k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, Ch
         o.pilot_hz = s.pilot_hz;
         o.err_avg = s.last_err_avg;
         o.status = (cp.mode == 3 && sb.n_disc > 0) ? s.pll_path : 0;
+        o.pll_iters = s.pll_iters;
     }
 }
 

@@ -193,12 +193,15 @@ class ChannelRunner:
     def wait(self, ticket: int, timeout_ms: int = 10000):
         _check(self._r, lib.gpud_runner_wait(self._r, int(ticket), int(timeout_ms)))
 
-    def result(self, slot: int) -> dict:
+    def result(self, slot: int, payload: bool = True) -> dict:
+        """Results of the last block.  With payload=False (required while host
+        outputs are off: the payload pointers are then device pointers) only
+        counts, flags and margins are returned."""
         res = ChannelResult()
         _check(self._r, lib.gpud_runner_result(self._r, int(slot), C.byref(res)))
 
         def arr(ptr, n, dt, width):
-            if not ptr or n <= 0:
+            if not payload or not ptr or n <= 0:
                 return np.zeros(0, dt)
             buf = (C.c_float * (n * width)).from_address(C.addressof(ptr.contents))
             return np.frombuffer(buf, dtype=np.float32).view(dt).copy()
@@ -221,6 +224,7 @@ class ChannelRunner:
             "pilot_hz": res.pilot_hz,
             "err_avg": res.err_avg,
             "pll_path": res.pll_path,
+            "pll_iters": res.pll_iters,
         }
 
     def stats(self) -> dict:

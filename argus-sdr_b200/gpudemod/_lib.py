@@ -53,7 +53,7 @@ class ChannelResult(C.Structure):
         ("audio", C.POINTER(C.c_float)),
         ("rds", C.POINTER(GPUDFloat2)),
         ("pll_path", C.c_int32),
-        ("pad", C.c_int32),
+        ("pll_iters", C.c_int32),
     ]
 
 

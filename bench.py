@@ -339,6 +339,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     launches = G.kernel_launch_count() - l0
+    pll_paths = [runner.result(sl, payload=False) for sl in range(N_CH)]
+    pll_info = {"parallel_blocks": sum(1 for r in pll_paths if r["pll_path"] == 1), "channels": N_CH,
+                "newton_iters": sorted({r["pll_iters"] for r in pll_paths})}
     t_ms = max_over_ranks(world, e0.elapsed_time(e1))
     barrier(world)
     value = world * N_CH * BLOCK * args.steps / (t_ms * 1e-3) / 1e6
@@ -387,7 +390,7 @@ def main():
         fp32 = fp32_peak_tflops() if not args.profile_only else None
         kern = {k: statistics.mean(v) for k, v in stage_acc.items() if k not in ("h2d", "d2h")}
         dom = max(kern, key=kern.get)
-        dom_key = "extract" if dom.startswith("extract") else dom
+        dom_key = "extract" if dom.startswith("extract") else ("pll" if dom.startswith("pll") else dom)
         w = work.get(dom_key, {"flop": 0, "bytes": 0})
         dom_ms = kern[dom]
         ach_tf = w["flop"] / (dom_ms * 1e-3) / 1e12
@@ -436,6 +439,7 @@ def main():
             "block_tflops": total_flop / (block_ms_sum * 1e-3) / 1e12,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
+            "pll": pll_info,
             "clocks": clocks,
         }
     runner.close()

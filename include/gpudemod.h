@@ -191,7 +191,7 @@ typedef struct {
     const float *audio;    /* host */
     const gpud_float2 *rds;
     int32_t pll_path;      /* WFM_STEREO: 1 parallel-in-time PLL solver, 2 serial loop */
-    int32_t pad;
+    int32_t pll_iters;     /* Newton iterations of the last parallel solve */
 } gpud_channel_result;
 
 /* Runner statistics. */
