@@ -65,40 +65,22 @@ def parse():
 
 
 # ---------------------------------------------------------------------------
-# distributed plumbing (one process per GPU; ranks shard channels: no collective
-# on the data path, only a barrier and a max-reduction of the timings)
+# distributed plumbing: gpudemod.dist (one process per GPU, channels sharded,
+# no data-path collective; a barrier and a max-reduction of timings only)
 # ---------------------------------------------------------------------------
 def dist_setup(n_gpus):
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return world, rank, local
+    from gpudemod import dist as D
+    return D.init("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from gpudemod import dist as D
+    D.barrier(world)
 
 
 def max_over_ranks(world, v: float) -> float:
-    if world <= 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from gpudemod import dist as D
+    return D.max_over_ranks(world, v, device="cuda")
 
 
 # ---------------------------------------------------------------------------
