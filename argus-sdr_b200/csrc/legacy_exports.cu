@@ -396,3 +396,64 @@ extern "C" GPUD_API uint64_t GPUD_CALL gpud_streaming_config_hash(int64_t signal
     }
     return h;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the stateful streaming extractor.
+//
+// Some callers cannot allocate device memory around this call: the real-time
+// DSP loop of the reference must not stall on cudaMalloc/cudaFree (both can
+// synchronize the whole device, holding up every other signal's work), its
+// per-frame allocation churn was removed on purpose (allocation-free frames),
+// and a host process whose device memory is committed to a fixed budget has no
+// room to hand out per-call temporaries.  This entry point needs no caller
+// scratch: the shifted samples and the history staging live in one file-scope
+// device array, so the caller passes only inputs, state and outputs.
+//
+// Limits: n_new <= GPUD_NOALLOC_MAX_NEW and history_cap <= GPUD_NOALLOC_MAX_HISTORY
+// (larger requests return GPUD_E_SCRATCH before anything is launched).  The
+// array (GPUD_NOALLOC_MAX_NEW + GPUD_NOALLOC_MAX_HISTORY complex samples,
+// about 2.1 MB) is held by every GPU that loads this library until the process
+// exits.  Every call shares it and it keeps the last call's contents; nothing
+// in it has to start at zero (each call writes every element it reads before
+// reading it).  Calls that overlap on the GPU (other host threads, other
+// streams) race on the array: serialize them.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) float2 g_noalloc_scratch[GPUD_NOALLOC_MAX_NEW + GPUD_NOALLOC_MAX_HISTORY];
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, never a device address: it is
+// resolved with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on that device (make that first call before
+// any stream capture).
+static float2 *noalloc_scratch(cudaError_t *err) {
+    static std::atomic<float2 *> cache[64];
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= 64) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    float2 *p = cache[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    void *addr = nullptr;
+    *err = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (*err != cudaSuccess) return nullptr;
+    p = static_cast<float2 *>(addr);
+    cache[dev].store(p, std::memory_order_release);
+    return p;
+}
+
+extern "C" GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
+    const gpud_float2 *in_new, int n_new, const float *polyphase_taps, int polyphase_len, int decim, int num_taps,
+    gpud_float2 *history_state, int history_cap, int *history_len_io, int *phase_count_state, double *phase_state,
+    double phase_inc, gpud_float2 *out, int out_cap, int *n_out) {
+    if (n_new > GPUD_NOALLOC_MAX_NEW || history_cap > GPUD_NOALLOC_MAX_HISTORY) return GPUD_E_SCRATCH;
+    cudaError_t err = cudaSuccess;
+    float2 *scratch = noalloc_scratch(&err);
+    if (!scratch) return (int)err;
+    return gpud_launch_streaming_polyphase_stateful_cuda(
+        in_new, n_new, (gpud_float2 *)scratch, polyphase_taps, polyphase_len, decim, num_taps, history_state,
+        (gpud_float2 *)(scratch + GPUD_NOALLOC_MAX_NEW), history_cap, history_len_io, phase_count_state, phase_state,
+        phase_inc, out, out_cap, n_out);
+}

@@ -103,6 +103,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
             i, [P, i, P, i, P, i, i, i, i, d, d, P, pi, pi, pd, P]),
         "gpud_launch_streaming_polyphase_stateful_cuda": (
             i, [P, i, P, P, i, i, i, P, P, i, pi, pi, pd, d, P, i, pi]),
+        "gpud_launch_streaming_polyphase_stateful_noalloc_cuda": (
+            i, [P, i, P, i, i, i, P, i, pi, pi, pd, d, P, i, pi]),
         # runner
         "gpud_runner_create": (i, [i, i, i, i, C.c_uint64, C.POINTER(P)]),
         "gpud_runner_destroy": (i, [P]),

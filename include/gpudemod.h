@@ -118,6 +118,25 @@ GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_cuda(
     int history_cap, int *history_len_io /*host*/, int *phase_count_state /*host*/, double *phase_state /*host*/,
     double phase_inc, gpud_float2 *out, int out_cap, int *n_out /*host*/);
 
+/* No counterpart in the reference: an allocation-free variant of
+ * gpud_launch_streaming_polyphase_stateful_cuda for callers that cannot
+ * allocate device memory around the call (a real-time loop that must not stall
+ * on cudaMalloc/cudaFree, which can synchronize the device; a process whose
+ * device memory is committed to a fixed budget).  Same arguments minus the two
+ * caller scratch buffers, same results and codes, plus GPUD_E_SCRATCH (-32)
+ * when n_new > GPUD_NOALLOC_MAX_NEW or history_cap > GPUD_NOALLOC_MAX_HISTORY.
+ * The scratch is one file-scope device array (about 2.1 MB) that every GPU
+ * loading the library holds until exit; its device address is resolved on the
+ * first call made on each device (make that call before any stream capture).
+ * All calls share that array: calls that overlap on the GPU race. */
+#define GPUD_NOALLOC_MAX_NEW 262144
+#define GPUD_NOALLOC_MAX_HISTORY 4096
+#define GPUD_E_SCRATCH (-32)
+GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
+    const gpud_float2 *in_new, int n_new, const float *polyphase_taps, int polyphase_len, int decim, int num_taps,
+    gpud_float2 *history_state, int history_cap, int *history_len_io /*host*/, int *phase_count_state /*host*/,
+    double *phase_state /*host*/, double phase_inc, gpud_float2 *out, int out_cap, int *n_out /*host*/);
+
 /* ======================================================================== */
 /* Part 2: batched / serving runner                                          */
 /* ======================================================================== */
