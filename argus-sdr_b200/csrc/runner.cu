@@ -10,7 +10,10 @@
 //     offsets are known before launch,
 //   - one launch sequence per block for all channels, with per-kernel work
 //     lists of (slot, tile) pairs for uneven taps / decimation,
-//   - one H2D of the block, one H2D of the descriptors, one D2H of all outputs.
+//   - one H2D of the block, one H2D of the descriptors, one D2H of all outputs,
+//   - two frames in flight: block k+1's front half (extraction, demod, stereo
+//     FIR bank, RDS) overlaps block k's back half (pilot PLL, stereo output),
+//     ordered by events, with the copies overlapping compute.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -18,6 +21,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <time.h>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -53,10 +57,11 @@ cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const Sl
 cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                        const ChanParams *prm, const ChanState *st, const WfmTaps *taps, const BinadeTable *tabs,
                        const float *wk, const float2 *rds_dl, float2 *rds_out);
-cudaError_t launch_post(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
-                        const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, int W,
-                        float *comp_dl, float *lr_dl, float *audio_dl, float2 *rds_dl, const BinadeTable *tabs,
-                        DevResult *res);
+cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                              const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
+                              float2 *rds_dl, const BinadeTable *tabs, DevResult *res);
+cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                             const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res);
 int rds_smem_bytes(int dr);
 int dense_smem_bytes_host(int P, int L);
 
@@ -150,25 +155,22 @@ static int build_binade_table(double inc, BinadeTable *t) {
 // ---------------------------------------------------------------------------
 struct Slot {
     bool active = false;
+    uint64_t reusable_after = 0;  // a retired slot is reused once this ticket completed
     gpud_channel_spec spec{};
     int D = 1, T = 1, P = 1, L = 1, hcap = 0;
     int ext_kind = 0;  // 0 dense, 1 wide
     int taps_off = 0, dtaps_off = 0, hist_off = 0, wfm_idx = -1, rate_class = -1;
     double cutoff = 0;
-    // host mirrors of device integer state
+    // host mirrors of device integer state (as of the last submitted block)
     int pc = 0, hist_len = 0, hist_sel = 0, comp_hist_len = 0;
     bool has_last = false;
     int64_t rds_count = 0;
     uint64_t footprint = 0;
-    // last block bookkeeping
-    SlotBlock sb{};
-    int res_row = -1;
 };
 
 struct BlockPlan {
     int n = 0;
     std::vector<SlotBlock> sbs;
-    std::vector<int> sb_slot;  // slot of each sb entry
     // work lists
     std::vector<int2> w_dense[kDenseMaxL + 1];
     int dense_smem[kDenseMaxL + 1] = {};
@@ -182,6 +184,48 @@ struct BlockPlan {
     int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_rds = 0;
 };
 
+struct SlotAfter {
+    int pc, hist_len;
+};
+
+// One stream-ordered host->device write, applied before the next block's front half.
+struct PendingOp {
+    int slot;
+    void *dst;
+    std::vector<char> data;
+};
+
+// Everything one block in flight owns.
+struct Frame {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev_front = nullptr, ev_back = nullptr, ev_done = nullptr, ev0 = nullptr, ev1 = nullptr;
+    char *d_desc = nullptr, *h_desc = nullptr;
+    size_t desc_cap = 0;
+    char *d_out = nullptr, *h_out = nullptr;
+    size_t out_cap = 0;
+    char *h_stage = nullptr;
+    size_t stage_cap = 0;
+    float *d_wk = nullptr;
+    int64_t wk_cap = 0;
+    double *d_traj = nullptr;
+    int64_t traj_cap = 0;
+    int *d_done = nullptr;
+    int64_t done_cap = 0;
+    float2 *d_block = nullptr;
+    float2 *h_in = nullptr;
+    BlockPlan plan;
+    std::vector<SlotAfter> after;
+    std::vector<int> row_of_slot;
+    size_t off_res = 0, off_audio = 0, off_rds = 0, off_ext = 0, out_bytes = 0;
+    bool host_outputs = true;
+    uint64_t ticket = 0;
+    bool inflight = false;
+    uint64_t h2d = 0, d2h = 0;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<std::string> prof_names;
+    int prof_n = 0;
+};
+
 }  // namespace gpud
 
 using namespace gpud;
@@ -190,10 +234,10 @@ struct gpud_runner {
     int fs = 0, max_block = 0, max_ch = 0, max_taps = 0;
     uint64_t budget = 0, used = 0;
     int schedule = GPUD_SCHED_BATCHED;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream = nullptr;  // joins every block: work recorded here follows all submitted blocks
+    cudaStream_t admin = nullptr;   // admission copies into slots no block in flight uses
     std::string err;
-    std::mutex mu;
+    std::recursive_mutex mu;
 
     std::vector<Slot> slots;
     int tapcap = 0;  // floats per slot in each taps region
@@ -206,71 +250,28 @@ struct gpud_runner {
     float2 *d_rds_dl = nullptr;
     WfmTapsHost *d_wtaps = nullptr;
     BinadeTable *d_tabs = nullptr;
-    std::vector<int> wfm_free;
     std::vector<int> class_rate;  // rate of each WFM rate class
-    // per-block buffers (grown on demand)
-    float2 *d_block = nullptr;
-    float *d_wk = nullptr;
-    int64_t wk_cap = 0;  // W (floats per work array)
-    double *d_traj = nullptr;  // PLL trajectories (parallel-in-time solver)
-    int64_t traj_cap = 0;
-    int *d_done = nullptr;
-    int64_t done_cap = 0;
     bool pll_parallel = true;
     int num_sms = 148;
-    char *d_out = nullptr, *h_out = nullptr;
-    size_t out_cap = 0;
-    char *d_desc = nullptr, *h_desc = nullptr;
-    size_t desc_cap = 0;
-    float2 *h_in = nullptr;
-    // last block layout
-    BlockPlan plan;
-    size_t off_res = 0, off_audio = 0, off_rds = 0, off_ext = 0, out_bytes = 0;
+    // frames
+    Frame fr[2];
+    int nxt = 0;        // frame the next block uses
+    int last = -1;      // frame of the last submitted block
+    int done_frame = -1;  // frame whose results gpud_runner_result reads
+    uint64_t submitted = 0, completed = 0;
+    std::vector<PendingOp> pending;
     // stats
     uint64_t blocks = 0, launches = 0;
     int graph_rebuilds = 0;
     std::vector<float> lat_ms;
     size_t lat_pos = 0;
     double last_ms = 0;
-    uint64_t pending_ticket = 0, done_ticket = 0;
-    cudaEvent_t ev_done = nullptr;
+    bool host_outputs = true;
+    bool profiling = false;
+    std::vector<gpud_stage_time> stage_times;
     // StreamingExtractGPU bookkeeping
     std::map<int64_t, int> by_signal;
-    bool host_outputs = true;
-    uint64_t last_h2d = 0, last_d2h = 0;
-    // per-stage profiling
-    bool profiling = false;
-    std::vector<cudaEvent_t> prof_ev;
-    std::vector<std::string> prof_names;
-    int prof_n = 0;
-    std::vector<gpud_stage_time> stage_times;
 };
-
-static void prof_mark(gpud_runner *r, const char *name) {
-    if (!r->profiling) return;
-    if ((int)r->prof_ev.size() <= r->prof_n) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        r->prof_ev.push_back(e);
-        r->prof_names.emplace_back();
-    }
-    cudaEventRecord(r->prof_ev[(size_t)r->prof_n], r->stream);
-    r->prof_names[(size_t)r->prof_n] = name;
-    r->prof_n++;
-}
-
-static void prof_collect(gpud_runner *r) {
-    if (!r->profiling || r->prof_n < 2) return;
-    r->stage_times.clear();
-    for (int i = 0; i + 1 < r->prof_n; ++i) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, r->prof_ev[(size_t)i], r->prof_ev[(size_t)i + 1]);
-        gpud_stage_time t{};
-        std::snprintf(t.name, sizeof t.name, "%s", r->prof_names[(size_t)i].c_str());
-        t.ms = ms;
-        r->stage_times.push_back(t);
-    }
-}
 
 static int set_err(gpud_runner *r, int code, const char *what, cudaError_t e = cudaSuccess) {
     char buf[256];
@@ -282,9 +283,9 @@ static int set_err(gpud_runner *r, int code, const char *what, cudaError_t e = c
     return code;
 }
 
-#define CK(call)                                                     \
-    do {                                                             \
-        cudaError_t e_ = (call);                                     \
+#define CK(call)                                                          \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
         if (e_ != cudaSuccess) return set_err(r, GPUD_E_CUDA, #call, e_); \
     } while (0)
 
@@ -293,15 +294,44 @@ static cudaError_t dalloc(T **p, size_t count) {
     return cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
 }
 
-// Bytes of per-block buffers one slot needs at max_block.
+static void prof_mark(gpud_runner *r, Frame &f, const char *name) {
+    if (!r->profiling) return;
+    if ((int)f.prof_ev.size() <= f.prof_n) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        f.prof_ev.push_back(e);
+        f.prof_names.emplace_back();
+    }
+    cudaEventRecord(f.prof_ev[(size_t)f.prof_n], f.s);
+    f.prof_names[(size_t)f.prof_n] = name;
+    f.prof_n++;
+}
+
+// Per-kernel times of a completed frame.  Intervals that only cover a wait on
+// the other frame ("wait_*" marks) are reported under their own names.
+static void prof_collect(gpud_runner *r, Frame &f) {
+    if (!r->profiling || f.prof_n < 2) return;
+    r->stage_times.clear();
+    for (int i = 0; i + 1 < f.prof_n; ++i) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, f.prof_ev[(size_t)i], f.prof_ev[(size_t)i + 1]);
+        gpud_stage_time t{};
+        std::snprintf(t.name, sizeof t.name, "%s", f.prof_names[(size_t)i].c_str());
+        t.ms = ms;
+        r->stage_times.push_back(t);
+    }
+}
+
+// Bytes of per-block buffers one slot needs at max_block (both frames).
 static uint64_t slot_block_bytes(const gpud_runner *r, int D, int mode, int flags) {
     uint64_t nout = (uint64_t)r->max_block / (uint64_t)D + 2;
     uint64_t b = nout * 8;  // extracted IQ (in the output arena)
     bool wfm = mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO;
     if (wfm) b += 5 * (nout + 8) * 4;  // composite work arrays
+    if (mode == GPUD_MODE_WFM_STEREO) b += 8 * (nout + 1) * 8;  // PLL trajectories
     if (mode != GPUD_MODE_IQ) b += nout * 4 * (mode == GPUD_MODE_WFM_STEREO ? 2 : 1);
     if (wfm && (flags & GPUD_CH_RDS)) b += (nout / 16 + 4) * 8;
-    return b;
+    return 2 * b;
 }
 
 static uint64_t slot_state_bytes(const gpud_runner *r) {
@@ -314,7 +344,6 @@ static int rate_class_for(gpud_runner *r, int rate) {
         if (r->class_rate[i] == rate) return (int)i;
     if ((int)r->class_rate.size() >= kMaxWfmClasses) return -1;
     int id = (int)r->class_rate.size();
-    r->class_rate.push_back(rate);
     WfmTapsHost h{};
     auto t15 = lowpass_fir(15000, rate, 101), t53 = lowpass_fir(53000, rate, 101), t23 = lowpass_fir(23000, rate, 101),
          t21 = lowpass_fir(21000, rate, 101), t17 = lowpass_fir(17000, rate, 101), t75 = lowpass_fir(7500, rate, 101);
@@ -331,32 +360,32 @@ static int rate_class_for(gpud_runner *r, int rate) {
     }
     BinadeTable tab;
     build_binade_table(-2 * GPUD_PI * (-57000.0) / (double)rate, &tab);
-    if (cudaMemcpy(r->d_wtaps + id, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
-    if (cudaMemcpy(r->d_tabs + id, &tab, sizeof tab, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+    // a new class id is not referenced by any block in flight
+    if (cudaMemcpyAsync(r->d_wtaps + id, &h, sizeof h, cudaMemcpyHostToDevice, r->admin) != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(r->d_tabs + id, &tab, sizeof tab, cudaMemcpyHostToDevice, r->admin) != cudaSuccess)
+        return -1;
+    if (cudaStreamSynchronize(r->admin) != cudaSuccess) return -1;
+    r->class_rate.push_back(rate);
     return id;
 }
 
 // Tap design of gpudemod/stream_state.go:57-77 (cutoff = max(BW/2, 200),
 // LowpassFIR in float64, cast to float32, the first T taps applied), laid out
 // phase-major (p*L + u -> h[p + u*D]) and direct.
-static int upload_taps(gpud_runner *r, int slot, double bandwidth) {
-    Slot &s = r->slots[(size_t)slot];
+static void design_taps(gpud_runner *r, const Slot &s, double bandwidth, std::vector<float> &pm,
+                        std::vector<float> &h, double *cutoff_out) {
     double cutoff = bandwidth / 2;
     if (cutoff < 200) cutoff = 200;
     auto base = lowpass_fir(cutoff, r->fs, s.T);
-    std::vector<float> h((size_t)s.T);
+    h.assign((size_t)s.T, 0.f);
     for (int k = 0; k < s.T; ++k) h[(size_t)k] = (float)base[(size_t)k];
-    std::vector<float> pm((size_t)s.P * s.L, 0.f);
+    pm.assign((size_t)s.P * s.L, 0.f);
     for (int p = 0; p < s.P; ++p)
         for (int u = 0; u < s.L; ++u) {
             int k = p + u * s.D;
             pm[(size_t)p * s.L + u] = k < s.T ? h[(size_t)k] : 0.f;
         }
-    CK(cudaMemcpyAsync(r->d_taps + s.taps_off, pm.data(), pm.size() * 4, cudaMemcpyHostToDevice, r->stream));
-    CK(cudaMemcpyAsync(r->d_taps + s.dtaps_off, h.data(), h.size() * 4, cudaMemcpyHostToDevice, r->stream));
-    CK(cudaStreamSynchronize(r->stream));
-    s.cutoff = cutoff;
-    return 0;
+    *cutoff_out = cutoff;
 }
 
 static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
@@ -389,27 +418,18 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     p->rds_tab = s.rate_class < 0 ? 0 : s.rate_class;
 }
 
-// Fresh device state: NCO phase 0, empty histories, PLL as built by
-// stereoDecodeStateful's first call (streamer.go:1546-1555).
-static int reset_slot_state(gpud_runner *r, int slot) {
-    Slot &s = r->slots[(size_t)slot];
-    ChanState st{};
-    st.pll_freq = 2 * GPUD_PI * 19000 / (double)s.spec.out_rate;
-    CK(cudaMemcpyAsync(r->d_st + slot, &st, sizeof st, cudaMemcpyHostToDevice, r->stream));
-    if (s.wfm_idx >= 0) {
-        CK(cudaMemsetAsync(r->d_comp_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->stream));
-        CK(cudaMemsetAsync(r->d_lr_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->stream));
-        CK(cudaMemsetAsync(r->d_audio_dl + (size_t)s.wfm_idx * kAudioDlStrideH, 0, kAudioDlStrideH * 4, r->stream));
-        CK(cudaMemsetAsync(r->d_rds_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 8, r->stream));
-    }
-    s.pc = 0;
-    s.hist_len = 0;
-    s.hist_sel = 0;
-    s.has_last = false;
-    s.comp_hist_len = 0;
-    s.rds_count = 0;
-    CK(cudaStreamSynchronize(r->stream));
-    return 0;
+static void queue_write(gpud_runner *r, int slot, void *dst, const void *src, size_t bytes) {
+    PendingOp op;
+    op.slot = slot;
+    op.dst = dst;
+    op.data.assign((const char *)src, (const char *)src + bytes);
+    r->pending.push_back(std::move(op));
+}
+
+static void drop_pending(gpud_runner *r, int slot) {
+    r->pending.erase(std::remove_if(r->pending.begin(), r->pending.end(),
+                                    [slot](const PendingOp &op) { return op.slot == slot; }),
+                     r->pending.end());
 }
 
 static int validate_spec(gpud_runner *r, const gpud_channel_spec *spec, int *D, int *T) {
@@ -425,208 +445,54 @@ static int validate_spec(gpud_runner *r, const gpud_channel_spec *spec, int *D, 
     return 0;
 }
 
-extern "C" {
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int max_channels, int max_taps,
-                                          uint64_t device_mem_budget, gpud_runner **out) {
-    if (!out || sample_rate <= 0 || max_block <= 0 || max_channels <= 0 || max_channels > 4096 || max_taps <= 0 ||
-        max_taps > 4096)
-        return GPUD_E_ARG;
-    auto *r = new gpud_runner();
-    r->fs = sample_rate;
-    r->max_block = max_block;
-    r->max_ch = max_channels;
-    r->max_taps = max_taps;
-    r->budget = device_mem_budget;
-    r->tapcap = 2 * max_taps + 64;
-    r->slots.resize((size_t)max_channels);
-    r->lat_ms.assign(4096, 0.f);
-#define CKC(call)                             \
-    do {                                      \
-        if ((call) != cudaSuccess) {          \
-            gpud_runner_destroy(r);           \
-            return GPUD_E_CUDA;               \
-        }                                     \
-    } while (0)
-    CKC(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
-    {
-        int dev = 0, sms = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
-            r->num_sms = sms;
-    }
-    CKC(cudaEventCreate(&r->ev0));
-    CKC(cudaEventCreate(&r->ev1));
-    CKC(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
-    size_t M = (size_t)max_channels;
-    CKC(dalloc(&r->d_prm, M));
-    CKC(dalloc(&r->d_st, M));
-    CKC(dalloc(&r->d_taps, M * 2 * (size_t)r->tapcap));
-    CKC(dalloc(&r->d_hist, M * 2 * (size_t)max_taps));
-    CKC(dalloc(&r->d_comp_dl, M * kWfmHist));
-    CKC(dalloc(&r->d_lr_dl, M * kWfmHist));
-    CKC(dalloc(&r->d_audio_dl, M * kAudioDlStrideH));
-    CKC(dalloc(&r->d_rds_dl, M * kWfmHist));
-    CKC(dalloc(&r->d_wtaps, (size_t)kMaxWfmClasses));
-    CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses));
-    CKC(dalloc(&r->d_block, (size_t)max_block));
-    CKC(cudaMallocHost((void **)&r->h_in, (size_t)max_block * sizeof(float2)));
-#undef CKC
-    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 8;
-    for (int i = max_channels - 1; i >= 0; --i) r->wfm_free.push_back(i);
-    *out = r;
-    return 0;
+// ---------------------------------------------------------------------------
+// block completion
+// ---------------------------------------------------------------------------
+static void record_latency(gpud_runner *r, Frame &f) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, f.ev0, f.ev1);
+    r->last_ms = ms;
+    r->lat_ms[r->lat_pos % r->lat_ms.size()] = ms;
+    r->lat_pos++;
 }
 
-GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
-    if (!r) return 0;
-    if (r->stream) cudaStreamSynchronize(r->stream);
-    cudaFree(r->d_prm);
-    cudaFree(r->d_st);
-    cudaFree(r->d_taps);
-    cudaFree(r->d_hist);
-    cudaFree(r->d_comp_dl);
-    cudaFree(r->d_lr_dl);
-    cudaFree(r->d_audio_dl);
-    cudaFree(r->d_rds_dl);
-    cudaFree(r->d_wtaps);
-    cudaFree(r->d_tabs);
-    cudaFree(r->d_block);
-    cudaFree(r->d_wk);
-    cudaFree(r->d_traj);
-    cudaFree(r->d_done);
-    cudaFree(r->d_out);
-    cudaFree(r->d_desc);
-    if (r->h_out) cudaFreeHost(r->h_out);
-    if (r->h_desc) cudaFreeHost(r->h_desc);
-    if (r->h_in) cudaFreeHost(r->h_in);
-    if (r->ev0) cudaEventDestroy(r->ev0);
-    if (r->ev1) cudaEventDestroy(r->ev1);
-    if (r->ev_done) cudaEventDestroy(r->ev_done);
-    for (auto e : r->prof_ev) cudaEventDestroy(e);
-    if (r->stream) cudaStreamDestroy(r->stream);
-    delete r;
-    return 0;
-}
-
-GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r) { return r ? r->err.c_str() : "null runner"; }
-
-GPUD_API int GPUD_CALL gpud_runner_stream(gpud_runner *r, gpud_stream_handle *out) {
-    if (!r || !out) return GPUD_E_ARG;
-    *out = (gpud_stream_handle)r->stream;
-    return 0;
-}
-
-GPUD_API int GPUD_CALL gpud_runner_set_schedule(gpud_runner *r, int schedule) {
-    if (!r || (schedule != GPUD_SCHED_BATCHED && schedule != GPUD_SCHED_PLAIN)) return GPUD_E_ARG;
-    r->schedule = schedule;
-    return 0;
-}
-
-GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_channel_spec *spec, uint64_t *bytes) {
-    if (!r || !bytes) return GPUD_E_ARG;
-    int D, T;
-    int rc = validate_spec(r, spec, &D, &T);
-    if (rc) return rc;
-    *bytes = slot_block_bytes(r, D, spec->mode, spec->flags);
-    return 0;
-}
-
-GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out) {
-    if (!r || !slot_out) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    int D, T;
-    int rc = validate_spec(r, spec, &D, &T);
-    if (rc) return rc;
-    int slot = -1;
-    for (int i = 0; i < r->max_ch; ++i)
-        if (!r->slots[(size_t)i].active) {
-            slot = i;
-            break;
+static int finish_frame(gpud_runner *r, int fi, int timeout_ms) {
+    Frame &f = r->fr[fi];
+    if (!f.inflight) return 0;
+    if (timeout_ms < 0) {
+        CK(cudaEventSynchronize(f.ev_done));
+    } else {
+        double waited = 0;
+        while (true) {
+            cudaError_t q = cudaEventQuery(f.ev_done);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return set_err(r, GPUD_E_CUDA, "event query", q);
+            if (waited >= timeout_ms) return set_err(r, GPUD_E_TIMEOUT, "wait timed out");
+            struct timespec ts{0, 50000};
+            nanosleep(&ts, nullptr);
+            waited += 0.05;
         }
-    if (slot < 0) return set_err(r, GPUD_E_SLOTS, "channel cap reached");
-    uint64_t fp = slot_block_bytes(r, D, spec->mode, spec->flags);
-    if (r->budget && r->used + fp > r->budget) return set_err(r, GPUD_E_BUDGET, "device-memory budget exhausted");
-    bool wfm = spec->mode == GPUD_MODE_WFM || spec->mode == GPUD_MODE_WFM_STEREO;
-    int rclass = -1;
-    if (wfm) {
-        rclass = rate_class_for(r, spec->out_rate);
-        if (rclass < 0) return set_err(r, GPUD_E_CUDA, "WFM rate classes exhausted");
     }
-    Slot &s = r->slots[(size_t)slot];
-    s = Slot{};
-    s.active = true;
-    s.spec = *spec;
-    s.spec.num_taps = T;
-    s.D = D;
-    s.T = T;
-    s.P = std::min(D, T);
-    s.L = (T + D - 1) / D;
-    s.hcap = r->max_taps;
-    s.taps_off = slot * 2 * r->tapcap;
-    s.dtaps_off = s.taps_off + r->tapcap;
-    s.hist_off = slot * 2 * r->max_taps;
-    s.wfm_idx = wfm ? slot : -1;
-    s.rate_class = rclass;
-    int smem = dense_smem_bytes_host(s.P, s.L);
-    s.ext_kind = (s.L >= 2 && s.L <= kDenseMaxL && smem <= kDenseSmemLimit) ? 0 : 1;
-    s.footprint = fp;
-    rc = upload_taps(r, slot, spec->bandwidth);
-    if (rc) {
-        s.active = false;
-        return rc;
-    }
-    ChanParams p;
-    fill_params(r, slot, &p);
-    CK(cudaMemcpyAsync(r->d_prm + slot, &p, sizeof p, cudaMemcpyHostToDevice, r->stream));
-    rc = reset_slot_state(r, slot);
-    if (rc) {
-        s.active = false;
-        return rc;
-    }
-    r->used += fp;
-    *slot_out = slot;
+    f.inflight = false;
+    if (f.ticket > r->completed) r->completed = f.ticket;
+    r->done_frame = fi;
+    record_latency(r, f);
+    prof_collect(r, f);
     return 0;
 }
 
-GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot) {
-    if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
-    Slot &s = r->slots[(size_t)slot];
-    r->used -= s.footprint;
-    s.active = false;
-    for (auto it = r->by_signal.begin(); it != r->by_signal.end(); ++it)
-        if (it->second == slot) {
-            r->by_signal.erase(it);
-            break;
-        }
-    return 0;
-}
-
-GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offset_hz, double bandwidth) {
-    if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
-    Slot &s = r->slots[(size_t)slot];
-    double cutoff = bandwidth / 2;
-    if (cutoff < 200) cutoff = 200;
-    if (cutoff != s.cutoff) {
-        int rc = upload_taps(r, slot, bandwidth);
+// Wait for every block in flight (oldest first).
+static int drain(gpud_runner *r) {
+    for (int k = 0; k < 2; ++k) {
+        int a = r->fr[0].inflight && (!r->fr[1].inflight || r->fr[0].ticket < r->fr[1].ticket) ? 0 : 1;
+        if (!r->fr[a].inflight) continue;
+        int rc = finish_frame(r, a, -1);
         if (rc) return rc;
     }
-    s.spec.bandwidth = bandwidth;
-    if (offset_hz != s.spec.offset_hz) {
-        s.spec.offset_hz = offset_hz;
-        ChanParams p;
-        fill_params(r, slot, &p);
-        CK(cudaMemcpyAsync(r->d_prm + slot, &p, sizeof p, cudaMemcpyHostToDevice, r->stream));
-        CK(cudaStreamSynchronize(r->stream));
-    }
     return 0;
 }
-
-}  // extern "C"
 
 // ---------------------------------------------------------------------------
 // block planning
@@ -680,12 +546,12 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
     }
     sb.res_idx = (int)pl.sbs.size();
     pl.sbs.push_back(sb);
-    pl.sb_slot.push_back(slot);
 }
 
 // Offsets (emitting slots' IQ first so one D2H covers it) and work lists.
 static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     int64_t ext = 0;
+    pl.tot_emit_ext = 0;
     for (int pass = 0; pass < 2; ++pass)
         for (auto &sb : pl.sbs) {
             bool emit = (r->slots[(size_t)sb.slot].spec.flags & GPUD_CH_EMIT_IQ) != 0;
@@ -755,44 +621,42 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     }
 }
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
-
-static int ensure_buffers(gpud_runner *r, const BlockPlan &pl) {
+static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     int64_t W = std::max<int64_t>(pl.tot_comp, 8);
-    if (W > r->wk_cap) {
-        cudaFree(r->d_wk);
-        r->d_wk = nullptr;
+    if (W > f.wk_cap) {
+        cudaFree(f.d_wk);
+        f.d_wk = nullptr;
         int64_t cap = std::max<int64_t>(W * 5 / 4, 1 << 16);
-        CK(dalloc(&r->d_wk, (size_t)cap * 5));
-        r->wk_cap = cap;
+        CK(dalloc(&f.d_wk, (size_t)cap * 5));
+        f.wk_cap = cap;
         r->graph_rebuilds++;
     }
-    if (pl.tot_traj > r->traj_cap) {
-        cudaFree(r->d_traj);
-        r->d_traj = nullptr;
+    if (pl.tot_traj > f.traj_cap) {
+        cudaFree(f.d_traj);
+        f.d_traj = nullptr;
         int64_t cap = std::max<int64_t>(pl.tot_traj * 5 / 4, 1 << 16);
-        CK(dalloc(&r->d_traj, (size_t)cap));
-        r->traj_cap = cap;
+        CK(dalloc(&f.d_traj, (size_t)cap));
+        f.traj_cap = cap;
     }
-    if ((int64_t)pl.pll_list.size() > r->done_cap) {
-        cudaFree(r->d_done);
-        r->d_done = nullptr;
+    if ((int64_t)pl.pll_list.size() > f.done_cap) {
+        cudaFree(f.d_done);
+        f.d_done = nullptr;
         int64_t cap = std::max<int64_t>((int64_t)pl.pll_list.size() * 2, 64);
-        CK(dalloc(&r->d_done, (size_t)cap));
-        r->done_cap = cap;
+        CK(dalloc(&f.d_done, (size_t)cap));
+        f.done_cap = cap;
     }
     size_t res = align256(pl.sbs.size() * sizeof(DevResult));
     size_t need = res + align256((size_t)pl.tot_audio * 4) + align256((size_t)pl.tot_rds * 8) +
                   align256((size_t)pl.tot_ext * 8);
-    if (need > r->out_cap) {
-        cudaFree(r->d_out);
-        if (r->h_out) cudaFreeHost(r->h_out);
-        r->d_out = nullptr;
-        r->h_out = nullptr;
+    if (need > f.out_cap) {
+        cudaFree(f.d_out);
+        if (f.h_out) cudaFreeHost(f.h_out);
+        f.d_out = nullptr;
+        f.h_out = nullptr;
         size_t cap = need * 5 / 4 + 4096;
-        CK(cudaMalloc((void **)&r->d_out, cap));
-        CK(cudaMallocHost((void **)&r->h_out, cap));
-        r->out_cap = cap;
+        CK(cudaMalloc((void **)&f.d_out, cap));
+        CK(cudaMallocHost((void **)&f.h_out, cap));
+        f.out_cap = cap;
         r->graph_rebuilds++;
     }
     size_t nw = 0;
@@ -801,21 +665,31 @@ static int ensure_buffers(gpud_runner *r, const BlockPlan &pl) {
           pl.w_rds.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.pll_list.size() * 8) + 4096;
-    if (dneed > r->desc_cap) {
-        cudaFree(r->d_desc);
-        if (r->h_desc) cudaFreeHost(r->h_desc);
-        r->d_desc = nullptr;
-        r->h_desc = nullptr;
+    if (dneed > f.desc_cap) {
+        cudaFree(f.d_desc);
+        if (f.h_desc) cudaFreeHost(f.h_desc);
+        f.d_desc = nullptr;
+        f.h_desc = nullptr;
         size_t cap = dneed * 5 / 4 + 4096;
-        CK(cudaMalloc((void **)&r->d_desc, cap));
-        CK(cudaMallocHost((void **)&r->h_desc, cap));
-        r->desc_cap = cap;
+        CK(cudaMalloc((void **)&f.d_desc, cap));
+        CK(cudaMallocHost((void **)&f.h_desc, cap));
+        f.desc_cap = cap;
+    }
+    size_t sneed = 0;
+    for (auto &op : r->pending) sneed += align256(op.data.size());
+    if (sneed > f.stage_cap) {
+        if (f.h_stage) cudaFreeHost(f.h_stage);
+        f.h_stage = nullptr;
+        size_t cap = sneed * 5 / 4 + 4096;
+        CK(cudaMallocHost((void **)&f.h_stage, cap));
+        f.stage_cap = cap;
     }
     return 0;
 }
 
 // Host mirrors advance exactly as the device state does.
-static void advance_mirrors(gpud_runner *r, const BlockPlan &pl, int n) {
+static void advance_mirrors(gpud_runner *r, const BlockPlan &pl, int n, std::vector<SlotAfter> *after) {
+    if (after) after->clear();
     for (const SlotBlock &sb : pl.sbs) {
         Slot &s = r->slots[(size_t)sb.slot];
         s.pc = (s.pc + n) % s.D;
@@ -826,14 +700,40 @@ static void advance_mirrors(gpud_runner *r, const BlockPlan &pl, int n) {
             s.comp_hist_len = std::min(kWfmHist, s.comp_hist_len + sb.n_disc);
             s.rds_count += sb.n_disc;
         }
-        s.sb = sb;
+        if (after) after->push_back(SlotAfter{s.pc, s.hist_len});
     }
 }
 
-// Enqueue descriptor upload, kernels and the output D2H for the slots in pl.
-static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int n) {
+static int stage_input(gpud_runner *r, Frame &f, const gpud_float2 *iq, int n, int on_device,
+                       const float2 **x_dev) {
+    if (n == 0) {
+        *x_dev = f.d_block;
+        return 0;
+    }
+    if (!iq) return set_err(r, GPUD_E_ARG, "null IQ block");
+    if (on_device) {
+        *x_dev = (const float2 *)iq;
+        return 0;
+    }
+    cudaPointerAttributes at{};
+    bool pinned = cudaPointerGetAttributes(&at, iq) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    const void *src = iq;
+    if (!pinned) {
+        std::memcpy(f.h_in, iq, (size_t)n * sizeof(float2));
+        src = f.h_in;
+    }
+    CK(cudaMemcpyAsync(f.d_block, src, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, f.s));
+    f.h2d += (uint64_t)n * sizeof(float2);
+    *x_dev = f.d_block;
+    return 0;
+}
+
+// Enqueue one block on frame f: descriptors, front half, [wait prev back],
+// back half, output D2H.  `prev` is the frame of the block before, or null.
+static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan &pl, const float2 *x_dev, int n) {
     // descriptor staging
-    char *hd = r->h_desc;
+    char *hd = f.h_desc;
     size_t o_sb = 0, o_w = align256(pl.sbs.size() * sizeof(SlotBlock));
     std::memcpy(hd + o_sb, pl.sbs.data(), pl.sbs.size() * sizeof(SlotBlock));
     int2 *hw = (int2 *)(hd + o_w);
@@ -857,51 +757,71 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
     size_t o_traj = o_pll + align256(pl.pll_list.size() * 4);
     std::memcpy(hd + o_traj, pl.pll_traj_off.data(), pl.pll_traj_off.size() * 8);
     size_t dbytes = o_traj + pl.pll_traj_off.size() * 8;
-    CK(cudaMemcpyAsync(r->d_desc, hd, dbytes, cudaMemcpyHostToDevice, r->stream));
-    const SlotBlock *d_sb = (const SlotBlock *)(r->d_desc + o_sb);
-    const int2 *d_w = (const int2 *)(r->d_desc + o_w);
-    const int *d_pll = (const int *)(r->d_desc + o_pll);
-    const int64_t *d_traj_off = (const int64_t *)(r->d_desc + o_traj);
+    CK(cudaMemcpyAsync(f.d_desc, hd, dbytes, cudaMemcpyHostToDevice, f.s));
+    f.h2d += dbytes;
+    const SlotBlock *d_sb = (const SlotBlock *)(f.d_desc + o_sb);
+    const int2 *d_w = (const int2 *)(f.d_desc + o_w);
+    const int *d_pll = (const int *)(f.d_desc + o_pll);
+    const int64_t *d_traj_off = (const int64_t *)(f.d_desc + o_traj);
 
-    r->off_res = 0;
-    r->off_audio = align256(pl.sbs.size() * sizeof(DevResult));
-    r->off_rds = r->off_audio + align256((size_t)pl.tot_audio * 4);
-    r->off_ext = r->off_rds + align256((size_t)pl.tot_rds * 8);
-    DevResult *d_res = (DevResult *)(r->d_out + r->off_res);
-    float *d_audio = (float *)(r->d_out + r->off_audio);
-    float2 *d_rds = (float2 *)(r->d_out + r->off_rds);
-    float2 *d_ext = (float2 *)(r->d_out + r->off_ext);
-    const int W = (int)r->wk_cap;
+    f.off_res = 0;
+    f.off_audio = align256(pl.sbs.size() * sizeof(DevResult));
+    f.off_rds = f.off_audio + align256((size_t)pl.tot_audio * 4);
+    f.off_ext = f.off_rds + align256((size_t)pl.tot_rds * 8);
+    DevResult *d_res = (DevResult *)(f.d_out + f.off_res);
+    float *d_audio = (float *)(f.d_out + f.off_audio);
+    float2 *d_rds = (float2 *)(f.d_out + f.off_rds);
+    float2 *d_ext = (float2 *)(f.d_out + f.off_ext);
+    const int W = (int)f.wk_cap;
     const WfmTaps *wt = (const WfmTaps *)r->d_wtaps;
     int nl = 0;
+    // ---- front half ----
     for (int L = 0; L <= kDenseMaxL; ++L) {
         if (pl.w_dense[L].empty()) continue;
-        prof_mark(r, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str() : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
-        CK(launch_extract_dense(L, (int)pl.w_dense[L].size(), pl.dense_smem[L], r->stream, d_w + w_dense_off[L],
-                                d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
+        prof_mark(r, f, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str()
+                                : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
+        CK(launch_extract_dense(L, (int)pl.w_dense[L].size(), pl.dense_smem[L], f.s, d_w + w_dense_off[L], d_sb,
+                                r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_wide.empty()) {
-        prof_mark(r, "extract_wide");
-        CK(launch_extract_wide((int)pl.w_wide.size(), pl.wide_smem, r->stream, d_w + o_wide, d_sb, r->d_prm, r->d_st,
-                               x_dev, n, r->d_hist, r->d_taps, d_ext));
+        prof_mark(r, f, "extract_wide");
+        CK(launch_extract_wide((int)pl.w_wide.size(), pl.wide_smem, f.s, d_w + o_wide, d_sb, r->d_prm, r->d_st, x_dev,
+                               n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_demod.empty()) {
-        prof_mark(r, "demod");
-        CK(launch_demod((int)pl.w_demod.size(), r->stream, d_w + o_dem, d_sb, r->d_prm, r->d_st, d_ext, r->d_wk,
-                        d_audio));
+        prof_mark(r, f, "demod");
+        CK(launch_demod((int)pl.w_demod.size(), f.s, d_w + o_dem, d_sb, r->d_prm, r->d_st, d_ext, f.d_wk, d_audio));
         nl++;
     }
     if (!pl.w_am.empty()) {
-        prof_mark(r, "am");
-        CK(launch_am((int)pl.w_am.size(), r->stream, d_w + o_am, d_sb, d_ext, d_audio));
+        prof_mark(r, f, "am");
+        CK(launch_am((int)pl.w_am.size(), f.s, d_w + o_am, d_sb, d_ext, d_audio));
         nl++;
     }
     if (!pl.w_fir.empty()) {
-        prof_mark(r, "wfm_fir");
-        CK(launch_wfm_fir((int)pl.w_fir.size(), r->stream, d_w + o_fir, d_sb, r->d_prm, wt, r->d_wk, W, r->d_comp_dl));
+        prof_mark(r, f, "wfm_fir");
+        CK(launch_wfm_fir((int)pl.w_fir.size(), f.s, d_w + o_fir, d_sb, r->d_prm, wt, f.d_wk, W, r->d_comp_dl));
         nl++;
+    }
+    if (!pl.w_rds.empty()) {
+        prof_mark(r, f, "rds");
+        CK(launch_rds((int)pl.w_rds.size(), pl.rds_smem, f.s, d_w + o_rds, d_sb, r->d_prm, r->d_st, wt, r->d_tabs,
+                      f.d_wk, r->d_rds_dl, d_rds));
+        nl++;
+    }
+    if (!pl.sbs.empty()) {
+        prof_mark(r, f, "post_front");
+        CK(launch_post_front((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_ext, f.d_wk,
+                             r->d_comp_dl, r->d_rds_dl, r->d_tabs, d_res));
+        nl++;
+    }
+    CK(cudaEventRecord(f.ev_front, f.s));
+    // ---- back half: after the previous block's back half ----
+    if (prev) {
+        prof_mark(r, f, "wait_prev_back");
+        CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
     }
     if (!pl.pll_list.empty()) {
         const int *done = nullptr;
@@ -915,217 +835,469 @@ static int enqueue_block(gpud_runner *r, BlockPlan &pl, const float2 *x_dev, int
             while (cluster < 8 && nch * cluster * 2 <= 3 * r->num_sms &&
                    max_n / (cluster * 2 * pll_newton_threads()) >= 8)
                 cluster *= 2;
-            prof_mark(r, "pll_newton");
-            CK(launch_pll_newton(nch, cluster, r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W, r->d_traj,
-                                 d_traj_off, r->d_done));
+            prof_mark(r, f, "pll_newton");
+            CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, f.d_traj, d_traj_off,
+                                 f.d_done));
             nl++;
-            done = r->d_done;
+            done = f.d_done;
         }
-        prof_mark(r, "pll_serial");
-        CK(launch_pll((int)pl.pll_list.size(), r->stream, d_pll, d_sb, r->d_prm, r->d_st, r->d_wk, W, done));
+        prof_mark(r, f, "pll_serial");
+        CK(launch_pll((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, done));
         nl++;
     }
     if (!pl.w_out.empty()) {
-        prof_mark(r, "wfm_out");
-        CK(launch_wfm_out((int)pl.w_out.size(), r->stream, d_w + o_out, d_sb, r->d_prm, r->d_st, wt, r->d_wk, W,
-                          r->d_lr_dl, r->d_audio_dl, d_audio));
-        nl++;
-    }
-    if (!pl.w_rds.empty()) {
-        prof_mark(r, "rds");
-        CK(launch_rds((int)pl.w_rds.size(), pl.rds_smem, r->stream, d_w + o_rds, d_sb, r->d_prm, r->d_st, wt,
-                      r->d_tabs, r->d_wk, r->d_rds_dl, d_rds));
+        prof_mark(r, f, "wfm_out");
+        CK(launch_wfm_out((int)pl.w_out.size(), f.s, d_w + o_out, d_sb, r->d_prm, r->d_st, wt, f.d_wk, W, r->d_lr_dl,
+                          r->d_audio_dl, d_audio));
         nl++;
     }
     if (!pl.sbs.empty()) {
-        prof_mark(r, "post");
-        CK(launch_post((int)pl.sbs.size(), r->stream, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_ext, r->d_wk, W,
-                       r->d_comp_dl, r->d_lr_dl, r->d_audio_dl, r->d_rds_dl, r->d_tabs, d_res));
+        prof_mark(r, f, "post_back");
+        CK(launch_post_back((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->d_lr_dl, r->d_audio_dl,
+                            d_res));
         nl++;
     }
-    prof_mark(r, "d2h");
+    CK(cudaEventRecord(f.ev_back, f.s));
+    prof_mark(r, f, "d2h");
     r->launches += (uint64_t)nl;
     gpud_count_launch(nl);
-    r->out_bytes = r->off_ext + (size_t)pl.tot_emit_ext * 8;
-    if (r->host_outputs) {
-        CK(cudaMemcpyAsync(r->h_out, r->d_out, r->out_bytes, cudaMemcpyDeviceToHost, r->stream));
-        r->last_d2h += r->out_bytes;
+    f.out_bytes = f.off_ext + (size_t)pl.tot_emit_ext * 8;
+    f.host_outputs = r->host_outputs;
+    if (f.host_outputs) {
+        CK(cudaMemcpyAsync(f.h_out, f.d_out, f.out_bytes, cudaMemcpyDeviceToHost, f.s));
+        f.d2h += f.out_bytes;
     } else {
-        // keep the results table on the host (small); payload stays on the device
-        CK(cudaMemcpyAsync(r->h_out, r->d_out, r->off_audio, cudaMemcpyDeviceToHost, r->stream));
-        r->last_d2h += r->off_audio;
+        // the results table comes back; the payload stays on the device
+        CK(cudaMemcpyAsync(f.h_out, f.d_out, f.off_audio, cudaMemcpyDeviceToHost, f.s));
+        f.d2h += f.off_audio;
     }
-    r->last_h2d += dbytes;
-    prof_mark(r, "end");
+    prof_mark(r, f, "end");
     return 0;
 }
 
-static int stage_input(gpud_runner *r, const gpud_float2 *iq, int n, int on_device, const float2 **x_dev) {
-    if (n == 0) {
-        *x_dev = r->d_block;
-        return 0;
+static int apply_pending(gpud_runner *r, Frame &f) {
+    size_t off = 0;
+    for (auto &op : r->pending) {
+        std::memcpy(f.h_stage + off, op.data.data(), op.data.size());
+        CK(cudaMemcpyAsync(op.dst, f.h_stage + off, op.data.size(), cudaMemcpyHostToDevice, f.s));
+        f.h2d += op.data.size();
+        off += align256(op.data.size());
     }
-    if (!iq) return set_err(r, GPUD_E_ARG, "null IQ block");
-    if (on_device) {
-        *x_dev = (const float2 *)iq;
-        return 0;
-    }
-    cudaPointerAttributes at{};
-    bool pinned = cudaPointerGetAttributes(&at, iq) == cudaSuccess && at.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    const void *src = iq;
-    if (!pinned) {
-        std::memcpy(r->h_in, iq, (size_t)n * sizeof(float2));
-        src = r->h_in;
-    }
-    CK(cudaMemcpyAsync(r->d_block, src, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, r->stream));
-    r->last_h2d += (uint64_t)n * sizeof(float2);
-    *x_dev = r->d_block;
+    r->pending.clear();
     return 0;
 }
 
-static void record_latency(gpud_runner *r) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
-    r->last_ms = ms;
-    r->lat_ms[r->lat_pos % r->lat_ms.size()] = ms;
-    r->lat_pos++;
+static void build_rows(gpud_runner *r, Frame &f) {
+    f.row_of_slot.assign((size_t)r->max_ch, -1);
+    for (size_t i = 0; i < f.plan.sbs.size(); ++i) f.row_of_slot[(size_t)f.plan.sbs[i].slot] = (int)i;
 }
 
-static int run_block(gpud_runner *r, const gpud_float2 *iq, int n, int on_device, bool wait) {
-    if (n < 0 || n > r->max_block) return set_err(r, GPUD_E_BLOCK, "block larger than max_block");
-    if (r->pending_ticket != r->done_ticket) {
-        CK(cudaEventSynchronize(r->ev_done));
-        r->done_ticket = r->pending_ticket;
+static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_device) {
+    const int fi = r->nxt;
+    Frame &f = r->fr[fi];
+    if (f.inflight) {
+        int rc = finish_frame(r, fi, -1);
+        if (rc) return rc;
     }
-    r->prof_n = 0;
-    r->last_h2d = r->last_d2h = 0;
-    CK(cudaEventRecord(r->ev0, r->stream));
-    prof_mark(r, "h2d");
-    const float2 *x = nullptr;
-    int rc = stage_input(r, iq, n, on_device, &x);
+    if (r->done_frame == fi) r->done_frame = -1;  // its results are about to be overwritten
+    Frame *prev = (r->last >= 0 && r->fr[r->last].inflight) ? &r->fr[r->last] : nullptr;
+    BlockPlan &pl = f.plan;
+    pl.sbs.clear();
+    pl.n = n;
+    for (int i = 0; i < r->max_ch; ++i)
+        if (r->slots[(size_t)i].active) plan_slot(r, pl, i, n);
+    finish_plan(r, pl);
+    int rc = ensure_frame(r, f, pl);
     if (rc) return rc;
-    if (r->schedule == GPUD_SCHED_BATCHED) {
-        BlockPlan &pl = r->plan;
-        pl.sbs.clear();
-        pl.sb_slot.clear();
-        pl.n = n;
-        for (int i = 0; i < r->max_ch; ++i)
-            if (r->slots[(size_t)i].active) plan_slot(r, pl, i, n);
-        finish_plan(r, pl);
-        rc = ensure_buffers(r, pl);
+    f.h2d = f.d2h = 0;
+    f.prof_n = 0;
+    CK(cudaEventRecord(f.ev0, f.s));
+    prof_mark(r, f, "h2d");
+    const float2 *x = nullptr;
+    rc = stage_input(r, f, iq, n, on_device, &x);
+    if (rc) return rc;
+    // parameter updates and the front half wait for the previous front half
+    if (prev) {
+        prof_mark(r, f, "wait_prev_front");
+        CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
+    }
+    rc = apply_pending(r, f);
+    if (rc) return rc;
+    if (!pl.sbs.empty()) {
+        rc = enqueue_block(r, f, prev, pl, x, n);
         if (rc) return rc;
-        if (!pl.sbs.empty()) {
-            rc = enqueue_block(r, pl, x, n);
-            if (rc) return rc;
-        }
-        advance_mirrors(r, pl, n);
-        for (size_t i = 0; i < pl.sbs.size(); ++i) r->slots[(size_t)pl.sbs[i].slot].res_row = (int)i;
     } else {
-        // Plain per-signal schedule (mirrors executeStreamingGPUNativePrepared,
-        // streaming_gpu_native_prepare.go:25-106): each channel alone, its own
-        // descriptor upload, launches and D2H, synchronised before the next.
-        // Results are gathered into the same host arena layout.
-        BlockPlan full;
-        full.n = n;
-        for (int i = 0; i < r->max_ch; ++i)
-            if (r->slots[(size_t)i].active) plan_slot(r, full, i, n);
-        finish_plan(r, full);
-        rc = ensure_buffers(r, full);
-        if (rc) return rc;
-        std::vector<char> gathered;
-        size_t res_b = align256(full.sbs.size() * sizeof(DevResult));
-        size_t a_off = res_b, r_off = a_off + align256((size_t)full.tot_audio * 4),
-               e_off = r_off + align256((size_t)full.tot_rds * 8);
-        gathered.assign(e_off + align256((size_t)full.tot_ext * 8), 0);
-        for (size_t k = 0; k < full.sbs.size(); ++k) {
-            BlockPlan one;
-            one.n = n;
-            SlotBlock sb = full.sbs[k];
-            int slot = sb.slot;
-            Slot &s = r->slots[(size_t)slot];
-            if (!on_device && n > 0) {  // the reference copies the whole block per signal
-                rc = stage_input(r, iq, n, 0, &x);
-                if (rc) return rc;
-            }
-            plan_slot(r, one, slot, n);
-            finish_plan(r, one);
-            rc = enqueue_block(r, one, x, n);
-            if (rc) return rc;
-            CK(cudaStreamSynchronize(r->stream));
-            const SlotBlock &o = one.sbs[0];
-            const SlotBlock &f = full.sbs[k];
-            std::memcpy(gathered.data() + k * sizeof(DevResult), r->h_out + r->off_res, sizeof(DevResult));
-            std::memcpy(gathered.data() + a_off + (size_t)f.audio_off * 4, r->h_out + r->off_audio +
-                        (size_t)o.audio_off * 4, (size_t)o.n_audio * 4);
-            std::memcpy(gathered.data() + r_off + (size_t)f.rds_off * 8, r->h_out + r->off_rds + (size_t)o.rds_off * 8,
-                        (size_t)o.n_rds * 8);
-            if (s.spec.flags & GPUD_CH_EMIT_IQ)
-                std::memcpy(gathered.data() + e_off + (size_t)f.ext_off * 8,
-                            r->h_out + r->off_ext + (size_t)o.ext_off * 8, (size_t)o.n_out * 8);
-            advance_mirrors(r, one, n);
-        }
-        std::memcpy(r->h_out, gathered.data(), gathered.size());
-        r->off_res = 0;
-        r->off_audio = a_off;
-        r->off_rds = r_off;
-        r->off_ext = e_off;
-        r->plan = full;
-        for (size_t i = 0; i < full.sbs.size(); ++i) {
-            Slot &s = r->slots[(size_t)full.sbs[i].slot];
-            s.res_row = (int)i;
-            s.sb = full.sbs[i];
-        }
+        CK(cudaEventRecord(f.ev_front, f.s));
+        CK(cudaEventRecord(f.ev_back, f.s));
+        f.off_res = f.off_audio = f.off_rds = f.off_ext = f.out_bytes = 0;
     }
-    CK(cudaEventRecord(r->ev1, r->stream));
-    CK(cudaEventRecord(r->ev_done, r->stream));
-    r->pending_ticket++;
+    CK(cudaEventRecord(f.ev1, f.s));
+    CK(cudaEventRecord(f.ev_done, f.s));
+    CK(cudaStreamWaitEvent(r->stream, f.ev_done, 0));  // join stream tracks every block
+    advance_mirrors(r, pl, n, &f.after);
+    build_rows(r, f);
+    f.inflight = true;
+    f.ticket = ++r->submitted;
+    r->last = fi;
+    r->nxt = 1 - fi;
     r->blocks++;
-    if (wait) {
-        CK(cudaEventSynchronize(r->ev_done));
-        r->done_ticket = r->pending_ticket;
-        record_latency(r);
-        prof_collect(r);
-    }
     return 0;
+}
+
+// Plain per-signal schedule (mirrors executeStreamingGPUNativePrepared,
+// streaming_gpu_native_prepare.go:25-106): each channel alone -- block H2D,
+// its own descriptors and launches, D2H, synchronised -- before the next.
+static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device) {
+    int rc = drain(r);
+    if (rc) return rc;
+    Frame &f = r->fr[0];
+    r->done_frame = -1;
+    BlockPlan full;
+    full.n = n;
+    for (int i = 0; i < r->max_ch; ++i)
+        if (r->slots[(size_t)i].active) plan_slot(r, full, i, n);
+    finish_plan(r, full);
+    rc = ensure_frame(r, f, full);
+    if (rc) return rc;
+    f.h2d = f.d2h = 0;
+    f.prof_n = 0;
+    std::vector<char> gathered;
+    size_t res_b = align256(full.sbs.size() * sizeof(DevResult));
+    size_t a_off = res_b, r_off = a_off + align256((size_t)full.tot_audio * 4),
+           e_off = r_off + align256((size_t)full.tot_rds * 8);
+    gathered.assign(e_off + align256((size_t)full.tot_ext * 8), 0);
+    CK(cudaEventRecord(f.ev0, f.s));
+    rc = apply_pending(r, f);
+    if (rc) return rc;
+    std::vector<SlotAfter> after;
+    for (size_t k = 0; k < full.sbs.size(); ++k) {
+        BlockPlan one;
+        one.n = n;
+        int slot = full.sbs[k].slot;
+        Slot &s = r->slots[(size_t)slot];
+        const float2 *x = nullptr;
+        rc = stage_input(r, f, iq, n, on_device, &x);  // the reference copies the whole block per signal
+        if (rc) return rc;
+        plan_slot(r, one, slot, n);
+        finish_plan(r, one);
+        rc = enqueue_block(r, f, nullptr, one, x, n);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(f.s));
+        const SlotBlock &o = one.sbs[0];
+        const SlotBlock &fb = full.sbs[k];
+        std::memcpy(gathered.data() + k * sizeof(DevResult), f.h_out + f.off_res, sizeof(DevResult));
+        std::memcpy(gathered.data() + a_off + (size_t)fb.audio_off * 4, f.h_out + f.off_audio + (size_t)o.audio_off * 4,
+                    (size_t)o.n_audio * 4);
+        std::memcpy(gathered.data() + r_off + (size_t)fb.rds_off * 8, f.h_out + f.off_rds + (size_t)o.rds_off * 8,
+                    (size_t)o.n_rds * 8);
+        if (s.spec.flags & GPUD_CH_EMIT_IQ)
+            std::memcpy(gathered.data() + e_off + (size_t)fb.ext_off * 8, f.h_out + f.off_ext + (size_t)o.ext_off * 8,
+                        (size_t)o.n_out * 8);
+        std::vector<SlotAfter> a1;
+        advance_mirrors(r, one, n, &a1);
+        after.push_back(a1[0]);
+    }
+    if (gathered.size() > f.out_cap) return set_err(r, GPUD_E_CUDA, "plain gather overflow");
+    std::memcpy(f.h_out, gathered.data(), gathered.size());
+    f.off_res = 0;
+    f.off_audio = a_off;
+    f.off_rds = r_off;
+    f.off_ext = e_off;
+    f.host_outputs = true;
+    f.plan = full;
+    f.after = after;
+    build_rows(r, f);
+    CK(cudaEventRecord(f.ev1, f.s));
+    CK(cudaEventRecord(f.ev_done, f.s));
+    f.inflight = true;
+    f.ticket = ++r->submitted;
+    r->last = 0;
+    r->nxt = 1;
+    r->blocks++;
+    return finish_frame(r, 0, -1);
+}
+
+static int run_block(gpud_runner *r, const gpud_float2 *iq, int n, int on_device, bool wait, uint64_t *ticket) {
+    if (n < 0 || n > r->max_block) return set_err(r, GPUD_E_BLOCK, "block larger than max_block");
+    int rc;
+    if (r->schedule == GPUD_SCHED_PLAIN) {
+        rc = run_plain(r, iq, n, on_device);
+    } else {
+        rc = submit_batched(r, iq, n, on_device);
+        if (!rc && wait) rc = drain(r);  // oldest first: the results are this block's
+    }
+    if (ticket) *ticket = r->submitted;
+    return rc;
 }
 
 extern "C" {
 
+GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int max_channels, int max_taps,
+                                          uint64_t device_mem_budget, gpud_runner **out) {
+    if (!out || sample_rate <= 0 || max_block <= 0 || max_channels <= 0 || max_channels > 4096 || max_taps <= 0 ||
+        max_taps > 4096)
+        return GPUD_E_ARG;
+    auto *r = new gpud_runner();
+    r->fs = sample_rate;
+    r->max_block = max_block;
+    r->max_ch = max_channels;
+    r->max_taps = max_taps;
+    r->budget = device_mem_budget;
+    r->tapcap = 2 * max_taps + 64;
+    r->slots.resize((size_t)max_channels);
+    r->lat_ms.assign(4096, 0.f);
+#define CKC(call)                    \
+    do {                             \
+        if ((call) != cudaSuccess) { \
+            gpud_runner_destroy(r);  \
+            return GPUD_E_CUDA;      \
+        }                            \
+    } while (0)
+    CKC(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&r->admin, cudaStreamNonBlocking));
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+            r->num_sms = sms;
+    }
+    for (auto &f : r->fr) {
+        CKC(cudaStreamCreateWithFlags(&f.s, cudaStreamNonBlocking));
+        CKC(cudaEventCreateWithFlags(&f.ev_front, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&f.ev_back, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&f.ev_done, cudaEventDisableTiming));
+        CKC(cudaEventCreate(&f.ev0));
+        CKC(cudaEventCreate(&f.ev1));
+        CKC(dalloc(&f.d_block, (size_t)max_block));
+        CKC(cudaMallocHost((void **)&f.h_in, (size_t)max_block * sizeof(float2)));
+    }
+    size_t M = (size_t)max_channels;
+    CKC(dalloc(&r->d_prm, M));
+    CKC(dalloc(&r->d_st, M));
+    CKC(dalloc(&r->d_taps, M * 2 * (size_t)r->tapcap));
+    CKC(dalloc(&r->d_hist, M * 2 * (size_t)max_taps));
+    CKC(dalloc(&r->d_comp_dl, M * kWfmHist));
+    CKC(dalloc(&r->d_lr_dl, M * kWfmHist));
+    CKC(dalloc(&r->d_audio_dl, M * kAudioDlStrideH));
+    CKC(dalloc(&r->d_rds_dl, M * kWfmHist));
+    CKC(dalloc(&r->d_wtaps, (size_t)kMaxWfmClasses));
+    CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses));
+#undef CKC
+    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 16;
+    *out = r;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
+    if (!r) return 0;
+    for (auto &f : r->fr) {
+        if (f.s) cudaStreamSynchronize(f.s);
+    }
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    if (r->admin) cudaStreamSynchronize(r->admin);
+    for (auto &f : r->fr) {
+        cudaFree(f.d_desc);
+        cudaFree(f.d_out);
+        cudaFree(f.d_wk);
+        cudaFree(f.d_traj);
+        cudaFree(f.d_done);
+        cudaFree(f.d_block);
+        if (f.h_desc) cudaFreeHost(f.h_desc);
+        if (f.h_out) cudaFreeHost(f.h_out);
+        if (f.h_stage) cudaFreeHost(f.h_stage);
+        if (f.h_in) cudaFreeHost(f.h_in);
+        for (auto e : {f.ev_front, f.ev_back, f.ev_done, f.ev0, f.ev1})
+            if (e) cudaEventDestroy(e);
+        for (auto e : f.prof_ev) cudaEventDestroy(e);
+        if (f.s) cudaStreamDestroy(f.s);
+    }
+    cudaFree(r->d_prm);
+    cudaFree(r->d_st);
+    cudaFree(r->d_taps);
+    cudaFree(r->d_hist);
+    cudaFree(r->d_comp_dl);
+    cudaFree(r->d_lr_dl);
+    cudaFree(r->d_audio_dl);
+    cudaFree(r->d_rds_dl);
+    cudaFree(r->d_wtaps);
+    cudaFree(r->d_tabs);
+    if (r->stream) cudaStreamDestroy(r->stream);
+    if (r->admin) cudaStreamDestroy(r->admin);
+    delete r;
+    return 0;
+}
+
+GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r) { return r ? r->err.c_str() : "null runner"; }
+
+GPUD_API int GPUD_CALL gpud_runner_stream(gpud_runner *r, gpud_stream_handle *out) {
+    if (!r || !out) return GPUD_E_ARG;
+    *out = (gpud_stream_handle)r->stream;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_set_schedule(gpud_runner *r, int schedule) {
+    if (!r || (schedule != GPUD_SCHED_BATCHED && schedule != GPUD_SCHED_PLAIN)) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    int rc = drain(r);
+    if (rc) return rc;
+    r->schedule = schedule;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_channel_spec *spec, uint64_t *bytes) {
+    if (!r || !bytes) return GPUD_E_ARG;
+    int D, T;
+    int rc = validate_spec(r, spec, &D, &T);
+    if (rc) return rc;
+    *bytes = slot_block_bytes(r, D, spec->mode, spec->flags);
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out) {
+    if (!r || !slot_out) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    int D, T;
+    int rc = validate_spec(r, spec, &D, &T);
+    if (rc) return rc;
+    uint64_t fp = slot_block_bytes(r, D, spec->mode, spec->flags);
+    if (r->budget && r->used + fp > r->budget) return set_err(r, GPUD_E_BUDGET, "device-memory budget exhausted");
+    // a free slot no block in flight still touches; drain if only such slots are left
+    int slot = -1;
+    bool busy_free = false;
+    for (int i = 0; i < r->max_ch; ++i) {
+        const Slot &s = r->slots[(size_t)i];
+        if (s.active) continue;
+        if (s.reusable_after <= r->completed) {
+            slot = i;
+            break;
+        }
+        busy_free = true;
+    }
+    if (slot < 0 && busy_free) {
+        rc = drain(r);
+        if (rc) return rc;
+        for (int i = 0; i < r->max_ch && slot < 0; ++i)
+            if (!r->slots[(size_t)i].active) slot = i;
+    }
+    if (slot < 0) return set_err(r, GPUD_E_SLOTS, "channel cap reached");
+    bool wfm = spec->mode == GPUD_MODE_WFM || spec->mode == GPUD_MODE_WFM_STEREO;
+    int rclass = -1;
+    if (wfm) {
+        rclass = rate_class_for(r, spec->out_rate);
+        if (rclass < 0) return set_err(r, GPUD_E_CUDA, "WFM rate classes exhausted");
+    }
+    drop_pending(r, slot);
+    Slot &s = r->slots[(size_t)slot];
+    s = Slot{};
+    s.spec = *spec;
+    s.spec.num_taps = T;
+    s.D = D;
+    s.T = T;
+    s.P = std::min(D, T);
+    s.L = (T + D - 1) / D;
+    s.hcap = r->max_taps;
+    s.taps_off = slot * 2 * r->tapcap;
+    s.dtaps_off = s.taps_off + r->tapcap;
+    s.hist_off = slot * 2 * r->max_taps;
+    s.wfm_idx = wfm ? slot : -1;
+    s.rate_class = rclass;
+    int smem = dense_smem_bytes_host(s.P, s.L);
+    s.ext_kind = (s.L >= 2 && s.L <= kDenseMaxL && smem <= kDenseSmemLimit) ? 0 : 1;
+    s.footprint = fp;
+    // The slot's memory is unused by every block in flight: write it now.
+    std::vector<float> pm, h;
+    design_taps(r, s, spec->bandwidth, pm, h, &s.cutoff);
+    ChanParams p;
+    fill_params(r, slot, &p);
+    ChanState st{};
+    st.pll_freq = 2 * GPUD_PI * 19000 / (double)s.spec.out_rate;  // stereoDecodeStateful init (streamer.go:1546-1555)
+    CK(cudaMemcpyAsync(r->d_taps + s.taps_off, pm.data(), pm.size() * 4, cudaMemcpyHostToDevice, r->admin));
+    CK(cudaMemcpyAsync(r->d_taps + s.dtaps_off, h.data(), h.size() * 4, cudaMemcpyHostToDevice, r->admin));
+    CK(cudaMemcpyAsync(r->d_prm + slot, &p, sizeof p, cudaMemcpyHostToDevice, r->admin));
+    CK(cudaMemcpyAsync(r->d_st + slot, &st, sizeof st, cudaMemcpyHostToDevice, r->admin));
+    if (s.wfm_idx >= 0) {
+        CK(cudaMemsetAsync(r->d_comp_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
+        CK(cudaMemsetAsync(r->d_lr_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
+        CK(cudaMemsetAsync(r->d_audio_dl + (size_t)s.wfm_idx * kAudioDlStrideH, 0, kAudioDlStrideH * 4, r->admin));
+        CK(cudaMemsetAsync(r->d_rds_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 8, r->admin));
+    }
+    // complete before the next submit, which is the first block to read them
+    CK(cudaStreamSynchronize(r->admin));
+    s.active = true;
+    r->used += fp;
+    *slot_out = slot;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot) {
+    if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
+    Slot &s = r->slots[(size_t)slot];
+    r->used -= s.footprint;
+    s.active = false;
+    s.reusable_after = r->submitted;
+    drop_pending(r, slot);
+    for (auto it = r->by_signal.begin(); it != r->by_signal.end(); ++it)
+        if (it->second == slot) {
+            r->by_signal.erase(it);
+            break;
+        }
+    return 0;
+}
+
+// The new taps / parameters are written on the next block's stream once the
+// block before it has passed its front half.  That block's back half may
+// still be reading ChanParams; of what an update changes (NCO increment,
+// taps) the back half reads nothing.
+GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offset_hz, double bandwidth) {
+    if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
+    Slot &s = r->slots[(size_t)slot];
+    double cutoff = bandwidth / 2;
+    if (cutoff < 200) cutoff = 200;
+    if (cutoff != s.cutoff) {
+        std::vector<float> pm, h;
+        design_taps(r, s, bandwidth, pm, h, &s.cutoff);
+        queue_write(r, slot, r->d_taps + s.taps_off, pm.data(), pm.size() * 4);
+        queue_write(r, slot, r->d_taps + s.dtaps_off, h.data(), h.size() * 4);
+    }
+    s.spec.bandwidth = bandwidth;
+    if (offset_hz != s.spec.offset_hz) {
+        s.spec.offset_hz = offset_hz;
+        ChanParams p;
+        fill_params(r, slot, &p);
+        queue_write(r, slot, r->d_prm + slot, &p, sizeof p);
+    }
+    return 0;
+}
+
 GPUD_API int GPUD_CALL gpud_runner_process_block(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device) {
     if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    return run_block(r, iq, n, iq_on_device, true);
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    return run_block(r, iq, n, iq_on_device, true, nullptr);
 }
 
 GPUD_API int GPUD_CALL gpud_runner_submit(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device,
                                           uint64_t *ticket) {
     if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    int rc = run_block(r, iq, n, iq_on_device, false);
-    if (rc) return rc;
-    if (ticket) *ticket = r->pending_ticket;
-    return 0;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    return run_block(r, iq, n, iq_on_device, false, ticket);
 }
 
 GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int timeout_ms) {
     if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
-    if (ticket <= r->done_ticket) return 0;
-    // bounded poll: never block past timeout_ms
-    double waited = 0;
-    while (true) {
-        cudaError_t q = cudaEventQuery(r->ev_done);
-        if (q == cudaSuccess) break;
-        if (q != cudaErrorNotReady) return set_err(r, GPUD_E_CUDA, "event query", q);
-        if (timeout_ms >= 0 && waited >= timeout_ms) return set_err(r, GPUD_E_TIMEOUT, "wait timed out");
-        struct timespec ts{0, 50000};
-        nanosleep(&ts, nullptr);
-        waited += 0.05;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    // finish blocks in order until `ticket` has completed
+    while (r->completed < ticket) {
+        int a = -1;
+        for (int k = 0; k < 2; ++k)
+            if (r->fr[k].inflight && (a < 0 || r->fr[k].ticket < r->fr[a].ticket)) a = k;
+        if (a < 0) break;
+        int rc = finish_frame(r, a, timeout_ms < 0 ? -1 : timeout_ms);
+        if (rc) return rc;
     }
-    r->done_ticket = r->pending_ticket;
-    record_latency(r);
-    prof_collect(r);
     return 0;
 }
 
@@ -1155,25 +1327,33 @@ GPUD_API int GPUD_CALL gpud_runner_stage_times(gpud_runner *r, gpud_stage_time *
     return 0;
 }
 
+// Results of the most recently completed block (gpud_runner_wait /
+// gpud_runner_process_block) that included the slot.
 GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel_result *out) {
     if (!r || !out) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
-    if (r->pending_ticket != r->done_ticket) return set_err(r, GPUD_E_TIMEOUT, "block still in flight");
     Slot &s = r->slots[(size_t)slot];
     std::memset(out, 0, sizeof *out);
     out->signal_id = s.spec.signal_id;
     out->rate = s.spec.out_rate;
-    out->phase_count = s.pc;
-    out->history_len = s.hist_len;
     out->audio_channels = s.spec.mode == GPUD_MODE_WFM_STEREO ? 2 : (s.spec.mode == GPUD_MODE_IQ ? 0 : 1);
     out->rds_rate = s.spec.out_rate / std::max(1, s.spec.out_rate / 19000);
-    if (s.res_row < 0 || s.res_row >= (int)r->plan.sbs.size() || r->plan.sbs[(size_t)s.res_row].slot != slot) {
-        return 0;  // admitted after the last block: no outputs yet
+    out->phase_count = s.pc;
+    out->history_len = s.hist_len;
+    if (r->done_frame < 0) {
+        if (r->fr[0].inflight || r->fr[1].inflight) return set_err(r, GPUD_E_TIMEOUT, "block still in flight");
+        return 0;
     }
-    const SlotBlock &sb = s.sb;
-    const DevResult *res = (const DevResult *)(r->h_out + r->off_res) + s.res_row;
+    Frame &f = r->fr[r->done_frame];
+    if (f.row_of_slot.size() != (size_t)r->max_ch) return 0;
+    int row = f.row_of_slot[(size_t)slot];
+    if (row < 0) return 0;  // admitted after that block
+    const SlotBlock &sb = f.plan.sbs[(size_t)row];
+    const DevResult *res = (const DevResult *)(f.h_out + f.off_res) + row;
     out->n_iq = sb.n_out;
+    out->phase_count = f.after[(size_t)row].pc;
+    out->history_len = f.after[(size_t)row].hist_len;
     out->nco_phase = res->nco_phase;
     out->n_audio = sb.n_audio;
     out->n_rds = sb.n_rds;
@@ -1183,16 +1363,16 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->err_avg = res->err_avg;
     out->pll_path = res->status;
     out->pll_iters = res->pll_iters;
-    const char *base = r->host_outputs ? r->h_out : r->d_out;
-    out->audio = (const float *)(base + r->off_audio) + sb.audio_off;
-    out->rds = (const gpud_float2 *)(base + r->off_rds) + sb.rds_off;
-    out->iq = (s.spec.flags & GPUD_CH_EMIT_IQ) ? (const gpud_float2 *)(base + r->off_ext) + sb.ext_off : nullptr;
+    const char *base = f.host_outputs ? f.h_out : f.d_out;
+    out->audio = (const float *)(base + f.off_audio) + sb.audio_off;
+    out->rds = (const gpud_float2 *)(base + f.off_rds) + sb.rds_off;
+    out->iq = (s.spec.flags & GPUD_CH_EMIT_IQ) ? (const gpud_float2 *)(base + f.off_ext) + sb.ext_off : nullptr;
     return 0;
 }
 
 GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *out) {
     if (!r || !out) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     std::memset(out, 0, sizeof *out);
     out->blocks = r->blocks;
     int act = 0;
@@ -1211,8 +1391,17 @@ GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *
     }
     out->kernel_launches = r->launches;
     out->graph_rebuilds = r->graph_rebuilds;
-    out->last_h2d_bytes = r->last_h2d;
-    out->last_d2h_bytes = r->last_d2h;
+    if (r->done_frame >= 0) {
+        out->last_h2d_bytes = r->fr[r->done_frame].h2d;
+        out->last_d2h_bytes = r->fr[r->done_frame].d2h;
+    }
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_reset_stats(gpud_runner *r) {
+    if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    r->lat_pos = 0;
     return 0;
 }
 
@@ -1235,7 +1424,7 @@ static uint64_t snap_bytes(const Slot &s) {
 
 GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob, uint64_t *bytes) {
     if (!r || !bytes) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
     Slot &s = r->slots[(size_t)slot];
     uint64_t need = snap_bytes(s);
@@ -1244,7 +1433,8 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
         return 0;
     }
     if (*bytes < need) return set_err(r, GPUD_E_ARG, "snapshot buffer too small");
-    CK(cudaStreamSynchronize(r->stream));
+    int rc = drain(r);
+    if (rc) return rc;
     char *p = (char *)blob;
     SnapHeader h{0x47505544u, 1, s.D, s.T, s.spec.mode, s.wfm_idx >= 0, s.pc, s.hist_len, s.hist_sel,
                  s.comp_hist_len, s.has_last ? 1 : 0, 0, s.rds_count, s.cutoff};
@@ -1272,7 +1462,7 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
 
 GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void *blob, uint64_t bytes) {
     if (!r || !blob) return GPUD_E_ARG;
-    std::lock_guard<std::mutex> lk(r->mu);
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
     Slot &s = r->slots[(size_t)slot];
     if (bytes < snap_bytes(s)) return set_err(r, GPUD_E_STATE, "snapshot size mismatch");
@@ -1282,7 +1472,9 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     p += sizeof h;
     if (h.magic != 0x47505544u || h.D != s.D || h.T != s.T || h.mode != s.spec.mode || h.wfm != (s.wfm_idx >= 0))
         return set_err(r, GPUD_E_STATE, "snapshot geometry mismatch");
-    CK(cudaStreamSynchronize(r->stream));
+    int rc = drain(r);
+    if (rc) return rc;
+    drop_pending(r, slot);  // the restored state replaces queued updates of this slot
     CK(cudaMemcpy(r->d_st + slot, p, sizeof(ChanState), cudaMemcpyHostToDevice));
     p += sizeof(ChanState);
     s.hist_sel = 0;
@@ -1305,14 +1497,17 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     s.has_last = h.has_last != 0;
     s.rds_count = h.rds_count;
     if (h.cutoff != s.cutoff) {
-        int rc = upload_taps(r, slot, 2 * h.cutoff);
-        if (rc) return rc;
+        std::vector<float> pm, hh;
+        design_taps(r, s, 2 * h.cutoff, pm, hh, &s.cutoff);
+        CK(cudaMemcpy(r->d_taps + s.taps_off, pm.data(), pm.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(r->d_taps + s.dtaps_off, hh.data(), hh.size() * 4, cudaMemcpyHostToDevice));
     }
     return 0;
 }
 
 GPUD_API int GPUD_CALL gpud_runner_reset_signal(gpud_runner *r, int64_t signal_id) {
     if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     auto it = r->by_signal.find(signal_id);
     if (it == r->by_signal.end()) return 0;
     return gpud_runner_retire(r, it->second);
@@ -1320,6 +1515,7 @@ GPUD_API int GPUD_CALL gpud_runner_reset_signal(gpud_runner *r, int64_t signal_i
 
 GPUD_API int GPUD_CALL gpud_runner_reset_all_signals(gpud_runner *r) {
     if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     std::vector<int> slots;
     for (auto &kv : r->by_signal) slots.push_back(kv.second);
     for (int s : slots) gpud_runner_retire(r, s);
@@ -1335,6 +1531,7 @@ GPUD_API int GPUD_CALL gpud_runner_streaming_extract(gpud_runner *r, const gpud_
                                                      gpud_channel_result *results, gpud_float2 *iq_out,
                                                      int iq_out_cap) {
     if (!r || n < 0 || n_jobs < 0 || (n_jobs > 0 && (!jobs || !results))) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
     std::vector<int> job_slot((size_t)n_jobs, -1);
     std::map<int64_t, bool> active;
     for (int i = 0; i < n_jobs; ++i) {
@@ -1371,7 +1568,9 @@ GPUD_API int GPUD_CALL gpud_runner_streaming_extract(gpud_runner *r, const gpud_
     for (auto &kv : r->by_signal)
         if (!active.count(kv.first)) to_retire.push_back(kv.second);
     for (int s : to_retire) gpud_runner_retire(r, s);
-    // channels admitted through the slot API stay untouched but only the jobs' slots run
+    // channels admitted through the slot API are left untouched: only the jobs' slots run
+    int rc = drain(r);
+    if (rc) return rc;
     std::vector<int> parked;
     for (int i = 0; i < r->max_ch; ++i) {
         Slot &s = r->slots[(size_t)i];
@@ -1382,11 +1581,7 @@ GPUD_API int GPUD_CALL gpud_runner_streaming_extract(gpud_runner *r, const gpud_
             parked.push_back(i);
         }
     }
-    int rc;
-    {
-        std::lock_guard<std::mutex> lk(r->mu);
-        rc = run_block(r, iq, n, 0, true);
-    }
+    rc = run_block(r, iq, n, 0, true, nullptr);
     for (int i : parked) r->slots[(size_t)i].active = true;
     if (rc) return rc;
     int64_t pos = 0;

@@ -1098,12 +1098,15 @@ __device__ void shift_delay_line(float *dl, const float *__restrict__ src, int n
     __syncthreads();
 }
 
+// Front half: everything the next block's extraction, demod, stereo FIR bank
+// and RDS read (extraction history and NCO phase, discriminator bridge,
+// composite delay line, RDS stream history).  Runs right after those stages,
+// so the next block's front half can overlap this block's PLL.
 __global__ void __launch_bounds__(128)
-k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
-       const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, const float2 *__restrict__ ext,
-       const float *__restrict__ wk, int W, float *__restrict__ comp_dl, float *__restrict__ lr_dl,
-       float *__restrict__ audio_dl, float2 *__restrict__ rds_dl, const BinadeTable *__restrict__ tabs,
-       DevResult *__restrict__ res) {
+k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
+             const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, const float2 *__restrict__ ext,
+             const float *__restrict__ wk, float *__restrict__ comp_dl, float2 *__restrict__ rds_dl,
+             const BinadeTable *__restrict__ tabs, DevResult *__restrict__ res) {
     const SlotBlock sb = sbt[blockIdx.x];
     const ChanParams &cp = prm[sb.slot];
     ChanState &s = st[sb.slot];
@@ -1123,15 +1126,6 @@ k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, Ch
     __syncthreads();
     if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
         const float *comp = wk + sb.comp_off;
-        const bool fallback = (cp.mode == 2) || !s.enabled;
-        if (fallback) {
-            float *adl = audio_dl + cp.wfm_idx * kAudioDlStride;
-            int valid = __float_as_int(adl[kWfmHist]);
-            shift_delay_line(adl, comp, sb.n_disc);
-            if (threadIdx.x == 0) adl[kWfmHist] = __int_as_float(min(kWfmHist, valid + sb.n_disc));
-            __syncthreads();
-        }
-        if (cp.mode == 3) shift_delay_line(lr_dl + cp.wfm_idx * kWfmHist, wk + 4 * W + sb.comp_off, sb.n_disc);
         // RDS shifted history: the last 100 values of cplx over the stream
         if (cp.flags & 2) {
             __shared__ float2 rtmp[kWfmHist];
@@ -1168,8 +1162,33 @@ k_post(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, Ch
             s.rds_count += sb.n_disc;
             s.rds_hist_len = (int)min((int64_t)kWfmHist, s.rds_count);
         }
+        res[sb.res_idx].nco_phase = q64_to_rad(s.nco_q);
+    }
+}
+
+// Back half: the L-R and mono-fallback delay lines and the block's lock
+// flags, margins and PLL solver info, after the PLL and the stereo output.
+__global__ void __launch_bounds__(128)
+k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
+            const float *__restrict__ wk, int W, float *__restrict__ lr_dl, float *__restrict__ audio_dl,
+            DevResult *__restrict__ res) {
+    const SlotBlock sb = sbt[blockIdx.x];
+    const ChanParams &cp = prm[sb.slot];
+    ChanState &s = st[sb.slot];
+    if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
+        const float *comp = wk + sb.comp_off;
+        const bool fallback = (cp.mode == 2) || !s.enabled;
+        if (fallback) {
+            float *adl = audio_dl + cp.wfm_idx * kAudioDlStride;
+            int valid = __float_as_int(adl[kWfmHist]);
+            shift_delay_line(adl, comp, sb.n_disc);
+            if (threadIdx.x == 0) adl[kWfmHist] = __int_as_float(min(kWfmHist, valid + sb.n_disc));
+            __syncthreads();
+        }
+        if (cp.mode == 3) shift_delay_line(lr_dl + cp.wfm_idx * kWfmHist, wk + 4 * W + sb.comp_off, sb.n_disc);
+    }
+    if (threadIdx.x == 0) {
         DevResult &o = res[sb.res_idx];
-        o.nco_phase = q64_to_rad(s.nco_q);
         o.flags = (cp.mode == 3 && sb.n_disc > 0) ? ((s.locked ? 1 : 0) | (s.enabled ? 2 : 0))
                                                   : (s.enabled ? 2 : 0);
         o.coherence = s.coherence;
@@ -1280,11 +1299,16 @@ cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_post(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
-                        const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, int W,
-                        float *comp_dl, float *lr_dl, float *audio_dl, float2 *rds_dl, const BinadeTable *tabs,
-                        DevResult *res) {
-    k_post<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, W, comp_dl, lr_dl, audio_dl, rds_dl, tabs, res);
+cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                              const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
+                              float2 *rds_dl, const BinadeTable *tabs, DevResult *res) {
+    k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, comp_dl, rds_dl, tabs, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                             const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res) {
+    k_post_back<<<grid, 128, 0, sm>>>(sbt, prm, st, wk, W, lr_dl, audio_dl, res);
     return cudaGetLastError();
 }
 

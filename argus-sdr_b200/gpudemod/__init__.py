@@ -187,14 +187,15 @@ class ChannelRunner:
         ptr, n, dev, keep = _iq_ptr(iq)
         t = C.c_uint64()
         _check(self._r, lib.gpud_runner_submit(self._r, ptr, n, dev, C.byref(t)))
-        self._keep = keep
+        # two blocks may be in flight: keep both inputs alive
+        self._keep = (getattr(self, "_keep", (None, None))[1], keep)
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 10000):
         _check(self._r, lib.gpud_runner_wait(self._r, int(ticket), int(timeout_ms)))
 
     def result(self, slot: int, payload: bool = True) -> dict:
-        """Results of the last block.  With payload=False (required while host
+        """Results of the most recently completed block.  With payload=False (required while host
         outputs are off: the payload pointers are then device pointers) only
         counts, flags and margins are returned."""
         res = ChannelResult()
@@ -226,6 +227,10 @@ class ChannelRunner:
             "pll_path": res.pll_path,
             "pll_iters": res.pll_iters,
         }
+
+    def reset_stats(self):
+        """Clear the block-latency window (p50 / p99)."""
+        _check(self._r, lib.gpud_runner_reset_stats(self._r))
 
     def stats(self) -> dict:
         s = RunnerStats()

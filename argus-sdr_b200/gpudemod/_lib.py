@@ -118,6 +118,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_wait": (i, [P, C.c_uint64, i]),
         "gpud_runner_result": (i, [P, i, C.POINTER(ChannelResult)]),
         "gpud_runner_stats_get": (i, [P, C.POINTER(RunnerStats)]),
+        "gpud_runner_reset_stats": (i, [P]),
         "gpud_runner_stream": (i, [P, C.POINTER(P)]),
         "gpud_runner_last_error": (C.c_char_p, [P]),
         "gpud_runner_snapshot": (i, [P, i, P, C.POINTER(C.c_uint64)]),
