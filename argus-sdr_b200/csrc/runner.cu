@@ -46,10 +46,9 @@ cudaError_t launch_am(int grid, cudaStream_t sm, const int2 *work, const SlotBlo
 cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const WfmTaps *taps, float *wk, int W, const float *comp_dl);
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W, const int *done);
+                       ChanState *st, float *wk, int W);
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
-                              const ChanParams *prm, ChanState *st, float *wk, int W, double *traj,
-                              const int64_t *traj_off, int *done);
+                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters);
 int pll_newton_threads();
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
@@ -74,6 +73,7 @@ constexpr int kAudioDlStrideH = kWfmHist + 4;
 constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
+constexpr int kPllMaxIters = 64;
 
 // ---------------------------------------------------------------------------
 // DSP design helpers (host) -- restated from the reference
@@ -179,8 +179,6 @@ struct BlockPlan {
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
-    std::vector<int64_t> pll_traj_off;  // doubles, per pll_list entry
-    int64_t tot_traj = 0;
     int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_rds = 0;
 };
 
@@ -207,10 +205,6 @@ struct Frame {
     size_t stage_cap = 0;
     float *d_wk = nullptr;
     int64_t wk_cap = 0;
-    double *d_traj = nullptr;
-    int64_t traj_cap = 0;
-    int *d_done = nullptr;
-    int64_t done_cap = 0;
     float2 *d_block = nullptr;
     float2 *h_in = nullptr;
     BlockPlan plan;
@@ -252,6 +246,7 @@ struct gpud_runner {
     BinadeTable *d_tabs = nullptr;
     std::vector<int> class_rate;  // rate of each WFM rate class
     bool pll_parallel = true;
+    int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
     // frames
     Frame fr[2];
@@ -328,7 +323,6 @@ static uint64_t slot_block_bytes(const gpud_runner *r, int D, int mode, int flag
     uint64_t b = nout * 8;  // extracted IQ (in the output arena)
     bool wfm = mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO;
     if (wfm) b += 5 * (nout + 8) * 4;  // composite work arrays
-    if (mode == GPUD_MODE_WFM_STEREO) b += 8 * (nout + 1) * 8;  // PLL trajectories
     if (mode != GPUD_MODE_IQ) b += nout * 4 * (mode == GPUD_MODE_WFM_STEREO ? 2 : 1);
     if (wfm && (flags & GPUD_CH_RDS)) b += (nout / 16 + 4) * 8;
     return 2 * b;
@@ -586,8 +580,6 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.w_out.clear();
     pl.w_rds.clear();
     pl.pll_list.clear();
-    pl.pll_traj_off.clear();
-    pl.tot_traj = 0;
     pl.rds_smem = 0;
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
@@ -609,8 +601,6 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         if (mode == GPUD_MODE_WFM_STEREO && sb.n_disc > 0) {
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_fir.push_back(make_int2(i, t));
             pl.pll_list.push_back(i);
-            pl.pll_traj_off.push_back(pl.tot_traj);
-            pl.tot_traj += 8 * ((int64_t)sb.n_disc + 1);
         }
         if ((mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO) && sb.n_disc > 0)
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_out.push_back(make_int2(i, t));
@@ -631,20 +621,6 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         f.wk_cap = cap;
         r->graph_rebuilds++;
     }
-    if (pl.tot_traj > f.traj_cap) {
-        cudaFree(f.d_traj);
-        f.d_traj = nullptr;
-        int64_t cap = std::max<int64_t>(pl.tot_traj * 5 / 4, 1 << 16);
-        CK(dalloc(&f.d_traj, (size_t)cap));
-        f.traj_cap = cap;
-    }
-    if ((int64_t)pl.pll_list.size() > f.done_cap) {
-        cudaFree(f.d_done);
-        f.d_done = nullptr;
-        int64_t cap = std::max<int64_t>((int64_t)pl.pll_list.size() * 2, 64);
-        CK(dalloc(&f.d_done, (size_t)cap));
-        f.done_cap = cap;
-    }
     size_t res = align256(pl.sbs.size() * sizeof(DevResult));
     size_t need = res + align256((size_t)pl.tot_audio * 4) + align256((size_t)pl.tot_rds * 8) +
                   align256((size_t)pl.tot_ext * 8);
@@ -664,7 +640,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
-                   align256(pl.pll_list.size() * 4) + align256(pl.pll_list.size() * 8) + 4096;
+                   align256(pl.pll_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
         cudaFree(f.d_desc);
         if (f.h_desc) cudaFreeHost(f.h_desc);
@@ -754,15 +730,12 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
            o_out = put(pl.w_out), o_rds = put(pl.w_rds);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
-    size_t o_traj = o_pll + align256(pl.pll_list.size() * 4);
-    std::memcpy(hd + o_traj, pl.pll_traj_off.data(), pl.pll_traj_off.size() * 8);
-    size_t dbytes = o_traj + pl.pll_traj_off.size() * 8;
+    size_t dbytes = o_pll + pl.pll_list.size() * 4;
     CK(cudaMemcpyAsync(f.d_desc, hd, dbytes, cudaMemcpyHostToDevice, f.s));
     f.h2d += dbytes;
     const SlotBlock *d_sb = (const SlotBlock *)(f.d_desc + o_sb);
     const int2 *d_w = (const int2 *)(f.d_desc + o_w);
     const int *d_pll = (const int *)(f.d_desc + o_pll);
-    const int64_t *d_traj_off = (const int64_t *)(f.d_desc + o_traj);
 
     f.off_res = 0;
     f.off_audio = align256(pl.sbs.size() * sizeof(DevResult));
@@ -824,7 +797,6 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
     }
     if (!pl.pll_list.empty()) {
-        const int *done = nullptr;
         if (r->pll_parallel) {
             // cluster size: enough CTAs to cover the SMs, no more than 8 per
             // channel, at least 8 steps per thread
@@ -836,13 +808,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                    max_n / (cluster * 2 * pll_newton_threads()) >= 8)
                 cluster *= 2;
             prof_mark(r, f, "pll_newton");
-            CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, f.d_traj, d_traj_off,
-                                 f.d_done));
-            nl++;
-            done = f.d_done;
+            CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->pll_max_iters));
+        } else {
+            prof_mark(r, f, "pll_serial");
+            CK(launch_pll((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W));
         }
-        prof_mark(r, f, "pll_serial");
-        CK(launch_pll((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, done));
         nl++;
     }
     if (!pl.w_out.empty()) {
@@ -1099,8 +1069,6 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_desc);
         cudaFree(f.d_out);
         cudaFree(f.d_wk);
-        cudaFree(f.d_traj);
-        cudaFree(f.d_done);
         cudaFree(f.d_block);
         if (f.h_desc) cudaFreeHost(f.h_desc);
         if (f.h_out) cudaFreeHost(f.h_out);
@@ -1308,8 +1276,9 @@ GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on) {
 }
 
 GPUD_API int GPUD_CALL gpud_runner_set_pll_solver(gpud_runner *r, int parallel) {
-    if (!r) return GPUD_E_ARG;
+    if (!r || parallel < 0) return GPUD_E_ARG;
     r->pll_parallel = parallel != 0;
+    r->pll_max_iters = parallel > 1 ? std::min(parallel, 4096) : kPllMaxIters;
     return 0;
 }
 

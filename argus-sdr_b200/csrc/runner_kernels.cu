@@ -10,6 +10,7 @@
 //   k_post                                per-slot state carry (histories, phases)
 // Every kernel takes a work list of (slot-block index, tile) pairs so channels
 // with uneven taps / decimation run in the same launch.
+#include <climits>
 #include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -532,14 +533,12 @@ constexpr int kPllChunk = 2048;
 
 __global__ void __launch_bounds__(64)
 k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
-      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
-      const int *__restrict__ done) {
+      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W) {
     __shared__ float s_pil[2][kPllChunk];
     __shared__ float s_th[2][kPllChunk];
     __shared__ double s_red[32];
     const int idx = blockIdx.x;
     if (idx >= count) return;
-    if (done && done[idx]) return;  // solved by the parallel-in-time kernel
     const SlotBlock sb = sbt[list[idx]];
     const int n = sb.n_disc;
     if (n <= 0) return;
@@ -612,21 +611,33 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
 
 
 // ===========================================================================
-// Pilot PLL, parallel in time.
+// Pilot PLL, parallel in time: multiple-shooting Newton.
 // ===========================================================================
 // The block's loop trajectory x_t = (phase, freq, I, Q), t = 0..n, obeys
-// x_{t+1} = F(x_t, p_t) with the serial kernel's exact step F.  Newton's method
-// on the whole trajectory: with the current iterate X and J_t = dF/dx at X_t,
-//     delta_{t+1} = J_t delta_t + (F(X_t) - X_{t+1}),   delta_0 = 0,
-//     X_{t+1} <- X_{t+1} + delta_{t+1},
-// a linear recurrence solved by an associative scan over affine maps (4x4 matrix
-// + vector, float32; the residual and the iterate are float64).  The fixed point
-// is the serial trajectory; a locked loop converges quadratically from the
-// free-running guess phase_0 + t*freq_0 in 3-4 iterations.  A block that has
-// not converged after kMaxNewton iterations (acquisition, no pilot) is left to
-// the serial kernel (done[idx] = 0).
+// x_{t+1} = F(x_t, p_t) with the serial kernel's exact step F.  The block is
+// cut into one segment of S consecutive steps per thread; the unknowns are the
+// segment start states s_g.  Each iteration every thread integrates its
+// segment with F from s_g (the exact nonlinear loop, no linearisation inside
+// the segment), giving the end state E_g(s_g) and the segment Jacobian
+// M_g = J_{t1-1} ... J_{t0}.  Newton's update of the start states,
+//     d_{g+1} = M_g d_g + (E_g(s_g) - s_{g+1}),   d_0 = 0,   s_g <- s_g + d_g,
+// is a linear recurrence over segments, solved by an associative scan over
+// affine maps (4x4 matrix + vector, float32; states and residuals float64 /
+// float32 as in F): warp shuffles, then shared memory across warps, then
+// distributed shared memory across the cluster's CTAs.  The fixed point is the
+// serial trajectory.  From the free-running guess s_g = (phase_0 + t0 freq_0,
+// freq_0, I_0, Q_0) a locked loop converges in 3-5 iterations; acquisition
+// from zero I/Q and noise-driven loops (no pilot) take tens to a hundred, since
+// a segment whose start is exact is exact after one more iteration.  A block
+// not converged after max_iters iterations keeps its consistent prefix and one
+// thread runs the serial loop over the rest.  No trajectory is stored: a last
+// pass integrates each segment from its converged start and writes the
+// outputs.
 constexpr int kNewtonThreads = 256;
-constexpr int kMaxNewton = 8;
+// Convergence: the last correction of every segment start is below what the
+// outputs resolve (the float32 sin/cos/atan2 and lowpass states leave a floor
+// near 1e-10 rad and 1e-9 in I/Q).
+constexpr float kTolPhase = 1e-8f, kTolFreq = 1e-12f, kTolIQ = 1e-7f;
 constexpr int kNW = kNewtonThreads / 32;
 
 struct Aff {
@@ -634,21 +645,16 @@ struct Aff {
     float b[4];
 };
 
-// (J, R) o (A, b): A <- J A, b <- J b + R, with J's sparsity.
-__device__ __forceinline__ void aff_push(Aff &m, const PllEval &o, float om, const float R[4]) {
+// M <- J M, with J's sparsity (phase/freq rows dense, I/Q rows phase + diagonal).
+__device__ __forceinline__ void mat_push(float (&m)[16], const PllEval &o, float om) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float p0 = m.a[j], f0 = m.a[4 + j], i0 = m.a[8 + j], q0 = m.a[12 + j];
-        m.a[j] = fmaf(o.ja, p0, fmaf(o.jb, f0, fmaf(o.jc, i0, o.jd * q0)));
-        m.a[4 + j] = fmaf(o.ka, p0, fmaf(o.kb, f0, fmaf(o.kc, i0, o.kd * q0)));
-        m.a[8 + j] = fmaf(o.iphi, p0, om * i0);
-        m.a[12 + j] = fmaf(o.qphi, p0, om * q0);
+        const float p0 = m[j], f0 = m[4 + j], i0 = m[8 + j], q0 = m[12 + j];
+        m[j] = fmaf(o.ja, p0, fmaf(o.jb, f0, fmaf(o.jc, i0, o.jd * q0)));
+        m[4 + j] = fmaf(o.ka, p0, fmaf(o.kb, f0, fmaf(o.kc, i0, o.kd * q0)));
+        m[8 + j] = fmaf(o.iphi, p0, om * i0);
+        m[12 + j] = fmaf(o.qphi, p0, om * q0);
     }
-    const float p0 = m.b[0], f0 = m.b[1], i0 = m.b[2], q0 = m.b[3];
-    m.b[0] = fmaf(o.ja, p0, fmaf(o.jb, f0, fmaf(o.jc, i0, fmaf(o.jd, q0, R[0]))));
-    m.b[1] = fmaf(o.ka, p0, fmaf(o.kb, f0, fmaf(o.kc, i0, fmaf(o.kd, q0, R[1]))));
-    m.b[2] = fmaf(o.iphi, p0, fmaf(om, i0, R[2]));
-    m.b[3] = fmaf(o.qphi, p0, fmaf(om, q0, R[3]));
 }
 
 // hi o lo (lo applied first)
@@ -673,17 +679,6 @@ __device__ __forceinline__ void aff_shfl_up(Aff &dst, const Aff &src, int d) {
     for (int i = 0; i < 16; ++i) dst.a[i] = __shfl_up_sync(0xffffffffu, src.a[i], d);
 #pragma unroll
     for (int i = 0; i < 4; ++i) dst.b[i] = __shfl_up_sync(0xffffffffu, src.b[i], d);
-}
-
-// One trajectory entry (state after t steps), deviation form.
-struct TStep {
-    double dphi, df;
-    float I, Q;
-};
-
-__device__ __forceinline__ TStep tstep_load(const TStep *X, bool guess, int t, float I0, float Q0) {
-    if (guess) return TStep{0.0, 0.0, I0, Q0};  // free-running ramp, constant lowpass states
-    return X[t];
 }
 
 __device__ __forceinline__ void aff_identity(Aff &m) {
@@ -713,21 +708,26 @@ __device__ __forceinline__ void aff_apply(float out[4], const Aff &m, const floa
         out[i] = fmaf(m.a[4 * i], x[0], fmaf(m.a[4 * i + 1], x[1], fmaf(m.a[4 * i + 2], x[2], fmaf(m.a[4 * i + 3], x[3], m.b[i]))));
 }
 
+// Segment start state, deviation form (see pll_step).
+struct SegState {
+    double dphi, df;
+    float I, Q;
+};
+
 // One channel-block per cluster of `gridDim.x / count` CTAs; the block's steps
-// are split evenly over all threads of the cluster.  Segment maps are scanned
-// within each warp (shuffles), across warps (shared memory) and across the
-// cluster's CTAs (distributed shared memory).
+// are split into one contiguous segment per thread of the cluster.
 __global__ void __launch_bounds__(kNewtonThreads, 3)
 k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
              const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
-             double *__restrict__ traj, const int64_t *__restrict__ traj_off, int *__restrict__ done) {
+             int max_iters) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float s_tot[kNW][20];     // warp totals
     __shared__ float s_wex[kNW][20];     // exclusive warp prefix (A, b) within the CTA
     __shared__ float s_cta[2][20];       // CTA total, double-buffered across iterations
     __shared__ float s_max[kNW][4];
-    __shared__ float s_cmax[2][4];       // CTA max |delta|, double-buffered
+    __shared__ float s_cmax[2][4];       // CTA max |d|, double-buffered
+    __shared__ SegState s_first[kNW];    // each warp's first segment start (lane 0)
     __shared__ double s_sum[kNW][2];
     __shared__ double s_csum[2];
     const int csize = (int)cl.num_blocks();
@@ -736,10 +736,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     if (idx >= count) return;  // uniform per cluster
     const SlotBlock sb = sbt[list[idx]];
     const int n = sb.n_disc;
-    if (n <= 0) {
-        if (threadIdx.x == 0 && crank == 0) done[idx] = 0;
-        return;  // uniform per cluster
-    }
+    if (n <= 0) return;  // uniform per cluster
     const ChanParams &cp = prm[sb.slot];
     ChanState &s = st[sb.slot];
     const float *pil = wk + 3 * W + sb.comp_off;
@@ -753,39 +750,51 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     const int S = (n + gthreads - 1) / gthreads;
     const int g = crank * kNewtonThreads + (int)threadIdx.x;
     const int t0 = min(n, g * S), t1 = min(n, t0 + S);
-    TStep *B0 = reinterpret_cast<TStep *>(traj + traj_off[idx]);
-    TStep *B1 = B0 + (n + 1);
-    int cur = -1;  // -1: the free-running guess
-    bool converged = false;
+    const bool has_next = t1 < n;  // the next thread's segment is not empty
+    SegState x0{0.0, 0.0, I0, Q0};  // this segment's start: the free-running guess
+    bool converged = false, bad = true;
     int iters = 0;
-    for (int it = 0; it < kMaxNewton && !converged; ++it) {
+    for (int it = 0; it < max_iters && !converged; ++it) {
         iters = it + 1;
         const int pb = it & 1;
-        const bool guess = cur < 0;
-        const TStep *X = (guess || cur == 0) ? B0 : B1;
-        TStep *Z = (guess || cur == 1) ? B0 : B1;
-        // ---- phase A: this thread's segment map ---------------------------
-        Aff m;
-        aff_identity(m);
-        if (t0 < t1) {
-            TStep a = tstep_load(X, guess, t0, I0, Q0);
-            TStep b = tstep_load(X, guess, t0 + 1, I0, Q0);
-            float pt = __ldg(pil + t0);
-            for (int t = t0; t < t1; ++t) {
-                TStep c = b;
-                float pn = pt;
-                if (t + 2 <= t1) c = tstep_load(X, guess, t + 2, I0, Q0);
-                if (t + 1 < t1) pn = __ldg(pil + t + 1);
-                PllEval o;
-                pll_step<true>(t, a.dphi, a.df, a.I, a.Q, pt, k, o);
-                const float R[4] = {(float)(o.dphi1 - b.dphi), (float)(o.df1 - b.df), o.I1 - b.I, o.Q1 - b.Q};
-                aff_push(m, o, om, R);
-                a = b;
-                b = c;
-                pt = pn;
+        // ---- the next segment's start state ------------------------------
+        SegState nx{0.0, 0.0, I0, Q0};
+        {
+            const double a = __shfl_down_sync(0xffffffffu, x0.dphi, 1);
+            const double b = __shfl_down_sync(0xffffffffu, x0.df, 1);
+            const float c = __shfl_down_sync(0xffffffffu, x0.I, 1);
+            const float d = __shfl_down_sync(0xffffffffu, x0.Q, 1);
+            if (it > 0 && has_next) {
+                if (lane < 31)
+                    nx = SegState{a, b, c, d};
+                else if (warp < kNW - 1)
+                    nx = s_first[warp + 1];
+                else
+                    nx = *cl.map_shared_rank(&s_first[0], crank + 1);
             }
         }
-        // ---- phase B: scan ------------------------------------------------
+        // ---- integrate the segment: end state and Jacobian ----------------
+        Aff m;
+        aff_identity(m);
+        SegState x = x0;
+        if (t0 < t1) {
+            float pt = __ldg(pil + t0);
+            for (int t = t0; t < t1; ++t) {
+                const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
+                PllEval o;
+                pll_step<true>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                mat_push(m.a, o, om);
+                x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+                pt = pn;
+            }
+            if (has_next) {
+                m.b[0] = (float)(x.dphi - nx.dphi);
+                m.b[1] = (float)(x.df - nx.df);
+                m.b[2] = x.I - nx.I;
+                m.b[3] = x.Q - nx.Q;
+            }
+        }
+        // ---- scan: d at each segment start -------------------------------
         Aff inc = m;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -815,7 +824,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             if (lane == kNW - 1) aff_store(s_cta[pb], wv);
         }
         cl.sync();  // CTA totals of the whole cluster are visible
-        float dcta[4] = {0.f, 0.f, 0.f, 0.f};  // delta at this CTA's first step
+        float dcta[4] = {0.f, 0.f, 0.f, 0.f};  // d at this CTA's first segment
         for (int r = 0; r < crank; ++r) {
             Aff rm;
             aff_load(rm, cl.map_shared_rank(&s_cta[pb][0], r));
@@ -834,40 +843,22 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             aff_apply(dw, wx, dcta);
             aff_apply(dl, exl, dw);
         }
-        // ---- phase C: apply, write the next iterate ----------------------
+        // ---- update the start state --------------------------------------
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
+        bad = false;
         if (t0 < t1) {
-            if (t0 == 0) Z[0] = TStep{0.0, 0.0, I0, Q0};
-            TStep a = tstep_load(X, guess, t0, I0, Q0);
-            TStep b = tstep_load(X, guess, t0 + 1, I0, Q0);
-            float pt = __ldg(pil + t0);
-            for (int t = t0; t < t1; ++t) {
-                TStep c = b;
-                float pn = pt;
-                if (t + 2 <= t1) c = tstep_load(X, guess, t + 2, I0, Q0);
-                if (t + 1 < t1) pn = __ldg(pil + t + 1);
-                PllEval o;
-                pll_step<true>(t, a.dphi, a.df, a.I, a.Q, pt, k, o);
-                const float R[4] = {(float)(o.dphi1 - b.dphi), (float)(o.df1 - b.df), o.I1 - b.I, o.Q1 - b.Q};
-                const float d0 = fmaf(o.ja, dl[0], fmaf(o.jb, dl[1], fmaf(o.jc, dl[2], fmaf(o.jd, dl[3], R[0]))));
-                const float d1 = fmaf(o.ka, dl[0], fmaf(o.kb, dl[1], fmaf(o.kc, dl[2], fmaf(o.kd, dl[3], R[1]))));
-                const float d2 = fmaf(o.iphi, dl[0], fmaf(om, dl[2], R[2]));
-                const float d3 = fmaf(o.qphi, dl[0], fmaf(om, dl[3], R[3]));
-                dl[0] = d0;
-                dl[1] = d1;
-                dl[2] = d2;
-                dl[3] = d3;
-                Z[t + 1] = TStep{b.dphi + (double)d0, b.df + (double)d1, b.I + d2, b.Q + d3};
-                mx[0] = fmaxf(mx[0], fabsf(d0));
-                mx[1] = fmaxf(mx[1], fabsf(d1));
-                mx[2] = fmaxf(mx[2], fabsf(d2));
-                mx[3] = fmaxf(mx[3], fabsf(d3));
-                a = b;
-                b = c;
-                pt = pn;
-            }
+            bad = fabsf(dl[0]) > kTolPhase || fabsf(dl[1]) > kTolFreq || fabsf(dl[2]) > kTolIQ ||
+                  fabsf(dl[3]) > kTolIQ;
+            x0.dphi += (double)dl[0];
+            x0.df += (double)dl[1];
+            x0.I += dl[2];
+            x0.Q += dl[3];
+            mx[0] = fabsf(dl[0]);
+            mx[1] = fabsf(dl[1]);
+            mx[2] = fabsf(dl[2]);
+            mx[3] = fabsf(dl[3]);
         }
-        cur = guess ? 0 : 1 - cur;
+        if (lane == 0) s_first[warp] = x0;
         // ---- convergence, agreed by every CTA of the cluster ---------------
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1)
@@ -882,7 +873,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             for (int w2 = 0; w2 < kNW; ++w2) v = fmaxf(v, s_max[w2][threadIdx.x]);
             s_cmax[pb][threadIdx.x] = v;
         }
-        cl.sync();  // also orders this iteration's trajectory writes before the next reads
+        cl.sync();  // also publishes s_first for the next iteration's reads
         float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
         for (int r = 0; r < csize; ++r) {
             const float *rm = cl.map_shared_rank(&s_cmax[pb][0], r);
@@ -891,30 +882,49 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             m2 = fmaxf(m2, rm[2]);
             m3 = fmaxf(m3, rm[3]);
         }
-        // Converged once the last correction is below what the outputs resolve
-        // (the float32 sin/cos/atan2 and lowpass states leave a floor near
-        // 1e-10 rad and 1e-9 in I/Q).
-        converged = (m0 <= 1e-8f && m1 <= 1e-12f && m2 <= 1e-7f && m3 <= 1e-7f);
+        converged = (m0 <= kTolPhase && m1 <= kTolFreq && m2 <= kTolIQ && m3 <= kTolIQ);
     }
+    // ---- not converged: the longest consistent prefix is kept ------------
+    // Segments before the first one whose start still moved by more than the
+    // tolerance form a consistent trajectory from the block start, and that
+    // segment's updated start is its exact start; one thread continues the
+    // serial loop from there to the block end.
+    __shared__ int s_bad[kNW];
+    __shared__ int s_cbad;
+    int gstar = INT_MAX;
     if (!converged) {
-        if (threadIdx.x == 0 && crank == 0) {
-            done[idx] = 0;
-            s.pll_iters = iters;
+        int v = bad ? g : INT_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if (lane == 0) s_bad[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int c = INT_MAX;
+            for (int w2 = 0; w2 < kNW; ++w2) c = min(c, s_bad[w2]);
+            s_cbad = c;
         }
-        // No CTA may leave while a peer can still be reading its shared memory
-        // (the s_cmax reads just above).
         cl.sync();
-        return;  // uniform per cluster: the serial kernel takes this block
+        for (int r = 0; r < csize; ++r) gstar = min(gstar, *cl.map_shared_rank(&s_cbad, r));
+        if (gstar == INT_MAX) gstar = 0;  // cannot happen (not converged means one start moved)
     }
-    // ---- outputs from the converged trajectory --------------------------
-    const TStep *X = cur == 0 ? B0 : B1;
+    // ---- outputs: each converged segment again from its start --------------
     double es = 0.0, pp = 0.0;
-    for (int t = t0; t < t1; ++t) {
-        const TStep x1 = X[t + 1];
-        es += fabs((double)atan2f(x1.Q, x1.I));
-        const double p = (double)pil[t];
-        pp += p * p;
-        lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x1.dphi);
+    SegState x = x0;
+    if (t0 < t1) {
+        const bool out = g < gstar;
+        float pt = __ldg(pil + t0);
+        for (int t = t0; t < t1; ++t) {
+            const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
+            pp += (double)pt * (double)pt;
+            if (out) {
+                PllEval o;
+                pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+                es += fabs((double)o.e);
+                lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x.dphi);
+            }
+            pt = pn;
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -936,21 +946,35 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
         s_csum[1] = b;
     }
     cl.sync();
-    if (threadIdx.x == 0 && crank == 0) {
-        es = 0;
-        pp = 0;
+    // the owner finishes the block: the thread holding the last segment, or
+    // the thread at the first inconsistent segment start
+    const int owner = converged ? (n - 1) / S : gstar;
+    double es_all = 0.0, pp_all = 0.0;
+    if (g == owner) {
         for (int r = 0; r < csize; ++r) {
             const double *rs = cl.map_shared_rank(&s_csum[0], r);
-            es += rs[0];
-            pp += rs[1];
+            es_all += rs[0];
+            pp_all += rs[1];
         }
-        const TStep xn = X[n];
-        pll_finish(s, cp, n, pll_phase_at(k, n, xn.dphi), s.pll_freq + xn.df, (double)xn.I, (double)xn.Q, es, pp);
-        s.pll_path = 1;
-        s.pll_iters = iters;
-        done[idx] = 1;
     }
-    cl.sync();  // keep shared memory alive until rank 0 has read it
+    cl.sync();  // no shared memory of another CTA is read after this
+    if (g != owner) return;
+    if (!converged) {
+        // serial loop from the exact start of segment gstar to the block end
+        float pt = __ldg(pil + t0);
+        for (int t = t0; t < n; ++t) {
+            const float pn = (t + 1 < n) ? __ldg(pil + t + 1) : 0.f;
+            PllEval o;
+            pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+            x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+            es_all += fabs((double)o.e);
+            lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x.dphi);
+            pt = pn;
+        }
+    }
+    pll_finish(s, cp, n, pll_phase_at(k, n, x.dphi), s.pll_freq + x.df, (double)x.I, (double)x.Q, es_all, pp_all);
+    s.pll_path = converged ? 1 : 2;
+    s.pll_iters = iters;
 }
 
 // L-R lowpass and L/R matrix when stereo is enabled; otherwise the 15 kHz mono
@@ -1260,14 +1284,13 @@ cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const Sl
 }
 
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W, const int *done) {
-    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W, done);
+                       ChanState *st, float *wk, int W) {
+    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
-                              const ChanParams *prm, ChanState *st, float *wk, int W, double *traj,
-                              const int64_t *traj_off, int *done) {
+                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(count * cluster), 1, 1);
     cfg.blockDim = dim3(kNewtonThreads, 1, 1);
@@ -1280,7 +1303,7 @@ cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_pll_newton, list, count, sbt, prm, st, wk, W, traj, traj_off, done);
+    return cudaLaunchKernelEx(&cfg, k_pll_newton, list, count, sbt, prm, st, wk, W, max_iters);
 }
 
 int pll_newton_threads() { return kNewtonThreads; }

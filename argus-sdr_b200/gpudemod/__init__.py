@@ -240,8 +240,11 @@ class ChannelRunner:
     def set_host_outputs(self, on: bool):
         _check(self._r, lib.gpud_runner_set_host_outputs(self._r, 1 if on else 0))
 
-    def set_pll_solver(self, parallel: bool):
-        _check(self._r, lib.gpud_runner_set_pll_solver(self._r, 1 if parallel else 0))
+    def set_pll_solver(self, parallel: bool, max_iters: int = 0):
+        """parallel=False: serial loop only.  max_iters > 1 caps the Newton
+        iterations before a block falls back to the serial loop."""
+        v = 0 if not parallel else (int(max_iters) if max_iters > 1 else 1)
+        _check(self._r, lib.gpud_runner_set_pll_solver(self._r, v))
 
     def set_profiling(self, on: bool):
         _check(self._r, lib.gpud_runner_set_profiling(self._r, 1 if on else 0))

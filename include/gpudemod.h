@@ -287,10 +287,13 @@ GPUD_API const char *GPUD_CALL gpud_runner_last_error(gpud_runner *r);
 GPUD_API int GPUD_CALL gpud_runner_set_host_outputs(gpud_runner *r, int on);
 
 /* Stereo pilot PLL solver: 1 (default) solves each block's loop trajectory in
- * parallel (Newton iteration over the block with an associative scan) and
- * falls back per channel to the serial loop when it has not converged; 0 runs
- * the serial loop only.  Both compute the same recurrence
- * (recorder/streamer.go:1588-1613). */
+ * parallel (multiple-shooting Newton over one segment per thread with an
+ * associative scan) and falls back per channel to the serial loop when it has
+ * not converged within 64 iterations (keeping the consistent prefix of the
+ * trajectory and running the serial loop over the rest); a value n > 1 sets
+ * that limit to n
+ * (at most 4096); 0 runs the serial loop only.  Both compute the same
+ * recurrence (recorder/streamer.go:1588-1613). */
 GPUD_API int GPUD_CALL gpud_runner_set_pll_solver(gpud_runner *r, int parallel);
 
 /* Per-kernel device time of the last block (CUDA events between the

@@ -223,7 +223,8 @@ def test_parallel_pll_equals_serial_pll(cuda):
             assert rel_l2(a["audio"], b["audio"]) <= 1e-6, rel_l2(a["audio"], b["audio"])
             assert a["locked"] == b["locked"] and a["stereo"] == b["stereo"]
             assert abs(a["coherence"] - b["coherence"]) <= 1e-5
-        assert all(p == 1 for p in paths[2:]), paths
+        # acquisition from zero I/Q included: every block by the parallel solver
+        assert all(p == 1 for p in paths), paths
     finally:
         rp.close()
         rs.close()
@@ -240,23 +241,30 @@ def test_parallel_pll_fallback_and_clusters(cuda):
              (3, 800_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, 0)]
     rp = G.ChannelRunner(fs, 262_144, max_channels=4)
     rs = G.ChannelRunner(fs, 262_144, max_channels=4)
+    rc = G.ChannelRunner(fs, 262_144, max_channels=4)
     rs.set_pll_solver(False)
+    rc.set_pll_solver(True, max_iters=3)  # too few for acquisition: those blocks fall back
     sp = [rp.admit(*s) for s in specs]
     ss = [rs.admit(*s) for s in specs]
-    paths = set()
+    sc = [rc.admit(*s) for s in specs]
+    paths, cpaths = set(), set()
     try:
         for x in blocks:
-            rp.process_block(x)
-            rs.process_block(x)
-            for a_slot, b_slot in zip(sp, ss):
-                a, b = rp.result(a_slot), rs.result(b_slot)
+            for r in (rp, rs, rc):
+                r.process_block(x)
+            for a_slot, b_slot, c_slot in zip(sp, ss, sc):
+                a, b, c = rp.result(a_slot), rs.result(b_slot), rc.result(c_slot)
                 paths.add(a["pll_path"])
-                assert rel_l2(a["audio"], b["audio"]) <= 1e-6, rel_l2(a["audio"], b["audio"])
-                assert a["locked"] == b["locked"] and a["stereo"] == b["stereo"]
+                cpaths.add(c["pll_path"])
+                for o in (a, c):
+                    assert rel_l2(o["audio"], b["audio"]) <= 1e-6, rel_l2(o["audio"], b["audio"])
+                    assert o["locked"] == b["locked"] and o["stereo"] == b["stereo"]
         assert 1 in paths
+        assert 2 in cpaths, cpaths
     finally:
         rp.close()
         rs.close()
+        rc.close()
 
 
 
