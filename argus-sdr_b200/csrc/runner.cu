@@ -491,13 +491,6 @@ static int drain(gpud_runner *r) {
 // ---------------------------------------------------------------------------
 // block planning
 // ---------------------------------------------------------------------------
-int gpud::dense_smem_bytes_host(int P, int L) {
-    int M = 256 + L - 1;
-    int Mp = (M + (M >> 3) + 1) | 1;
-    int z = P * Mp * 8;
-    int red = 8 * (256 + 32) * 8;
-    return std::max(z, red) + P * L * 4 + 16;
-}
 
 static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
     Slot &s = r->slots[(size_t)slot];

@@ -49,13 +49,6 @@ __host__ __device__ inline int dense_row_stride(int L) {
     return (M + (M >> 3) + 1) | 1;
 }
 
-__host__ __device__ inline int dense_smem_bytes(int P, int L) {
-    int z = P * dense_row_stride(L) * 8;
-    int red = 8 * (kDenseOT + kDenseOT / 8) * 8;
-    int a = z > red ? z : red;
-    return a + P * L * 4 + 16;
-}
-
 __device__ __forceinline__ float2 shifted_sample(int i, int n, const float2 *__restrict__ x, uint64_t u0,
                                                  uint64_t inc, const float2 *__restrict__ hist, int H) {
     if (i >= 0) {
@@ -65,6 +58,22 @@ __device__ __forceinline__ float2 shifted_sample(int i, int n, const float2 *__r
     int hi = H + i;
     return hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
 }
+
+// Rotation table entries: one per 256-sample staging round.
+__host__ __device__ inline int dense_rounds(int P, int L) { return (P * (kDenseOT + L - 1) + kDenseThreads - 1) / kDenseThreads; }
+
+// Shared memory: Z (reused for the cross-warp reduction) | taps | rotation table.
+__host__ __device__ inline int dense_zbytes(int P, int L) {
+    int z = P * dense_row_stride(L) * 8;
+    int red = 8 * (kDenseOT + kDenseOT / 8) * 8;
+    return z > red ? z : red;
+}
+
+__host__ __device__ inline int dense_smem_bytes(int P, int L) {
+    return dense_zbytes(P, L) + ((P * L + 1) & ~1) * 4 + dense_rounds(P, L) * 8 + 16;
+}
+
+int dense_smem_bytes_host(int P, int L) { return dense_smem_bytes(P, L); }
 
 template <int L>
 __global__ void __launch_bounds__(kDenseThreads, 2)
@@ -84,11 +93,8 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     const int M = kDenseOT + L - 1;
     const int Mp = dense_row_stride(L);
     float2 *Z = reinterpret_cast<float2 *>(smem4);
-    const int zbytes = dense_smem_bytes(P, L) - P * L * 4 - 16;
-    float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smem4) + zbytes);
-
-    const float *tg = taps_arena + cp.taps_off;
-    for (int i = threadIdx.x; i < P * L; i += kDenseThreads) tsm[i] = tg[i];
+    float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smem4) + dense_zbytes(P, L));
+    float2 *wtab = reinterpret_cast<float2 *>(tsm + ((P * L + 1) & ~1));
 
     const int s0 = D - sb.pc - 1;
     const int m_base = j0 - (L - 1);
@@ -99,45 +105,64 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     // Staging.  Tile sample i' = 0..M*D-1 is block sample i = ibase + i' and
     // lands in Z[p][m] with m = i'/D, p = D-1 - i'%D.  Thread t takes
     // i' = t + 256*k: consecutive threads hit consecutive phases (odd row
-    // stride: no bank conflicts) and its rotator advances by w = exp(j*256*inc)
-    // per k, re-anchored from the exact Q0.64 phase every 8 steps.
+    // stride: no bank conflicts), and (m, p) advance by a constant step with
+    // one carry.  The rotation of sample i' is exp(j*phi(ibase + t)) *
+    // exp(j*256*k*inc), both exact from the Q0.64 phase (the second from a
+    // per-tile table).
     const int total = P * M;  // P == D in the dense form
     const int ibase = s0 + m_base * D - (D - 1);
-    const float invD = 1.0f / (float)D;
-    const float2 w256 = q64_phasor((uint64_t)kDenseThreads * inc);
-    float2 rot = make_float2(1.f, 0.f);
+    const int nk = dense_rounds(P, L);
+    const float *tg = taps_arena + cp.taps_off;
+    for (int i = threadIdx.x; i < P * L; i += kDenseThreads) tsm[i] = tg[i];
+    for (int k = threadIdx.x; k < nk; k += kDenseThreads)
+        wtab[k] = q64_phasor((uint64_t)k * (uint64_t)kDenseThreads * inc);
+    const int t = (int)threadIdx.x;
+    int mr = t / D, q = t - (t / D) * D;
+    const int dm = kDenseThreads / D, dq = kDenseThreads - dm * D;
+    const float2 a_t = q64_phasor(u0 + (uint64_t)(int64_t)(ibase + t) * inc);
+    __syncthreads();
+    const int nfull = total / kDenseThreads;  // rounds in which every thread has a sample
+    const bool interior = ibase >= 0 && ibase + total <= n;
     constexpr int U = 4;
-    for (int k0 = 0; k0 * kDenseThreads < total; k0 += U) {
-        float2 xv[U];
-        int zi[U], ii[U];
+    int k = 0;
+    if (interior) {
+        const float2 *xp = x + ibase + t;
+        for (; k + U <= nfull; k += U) {
+            float2 xv[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int ip = (int)threadIdx.x + (k0 + u) * kDenseThreads;
-            const int i = ibase + ip;
-            const int mr = (int)(((float)ip + 0.5f) * invD);
-            const int p = D - 1 - (ip - mr * D);
-            zi[u] = ip < total ? p * Mp + mr + (mr >> 3) : -1;
-            ii[u] = i;
-            xv[u] = (ip < total && i >= 0 && i < n) ? __ldg(x + i) : make_float2(0.f, 0.f);
-        }
+            for (int u = 0; u < U; ++u) xv[u] = __ldg(xp + (k + u) * kDenseThreads);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int k = k0 + u;
-            if ((k & 7) == 0) {
-                rot = q64_phasor(u0 + (uint64_t)(int64_t)(ibase + (int)threadIdx.x + k * kDenseThreads) * inc);
-            } else {
-                rot = cmulf(rot, w256);
+            for (int u = 0; u < U; ++u) {
+                const float2 rot = cmulf(a_t, wtab[k + u]);
+                Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = cmulf(xv[u], rot);
+                q += dq;
+                mr += dm;
+                if (q >= D) {
+                    q -= D;
+                    ++mr;
+                }
             }
-            if (zi[u] < 0) continue;
-            const int i = ii[u];
+        }
+    }
+    // remaining rounds, and every round of tiles at the block edges
+    for (; k < nk; ++k) {
+        const int ip = t + k * kDenseThreads;
+        if (ip < total) {
+            const int i = ibase + ip;
             float2 v;
             if (i >= 0) {
-                v = i < n ? cmulf(xv[u], rot) : make_float2(0.f, 0.f);
+                v = i < n ? cmulf(__ldg(x + i), cmulf(a_t, wtab[k])) : make_float2(0.f, 0.f);
             } else {
                 const int hi = H + i;
                 v = hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
             }
-            Z[zi[u]] = v;
+            Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = v;
+        }
+        q += dq;
+        mr += dm;
+        if (q >= D) {
+            q -= D;
+            ++mr;
         }
     }
     __syncthreads();
@@ -147,13 +172,11 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
 #pragma unroll
     for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
     for (int p = warp; p < P; p += 8) {
-        const float2 *zrow = Z + p * Mp;
+        // lane window: columns lane*R + tt, stored at (lane*R + tt) + (lane*R + tt)/8
+        const float2 *zrow = Z + p * Mp + lane * (R + 1);
         float2 win[R + L - 1];
 #pragma unroll
-        for (int t = 0; t < R + L - 1; ++t) {
-            int c = lane * R + t;
-            win[t] = zrow[c + (c >> 3)];
-        }
+        for (int tt = 0; tt < R + L - 1; ++tt) win[tt] = zrow[tt + (tt >> 3)];
         float h[L];
 #pragma unroll
         for (int u = 0; u < L; ++u) h[u] = tsm[p * L + u];
@@ -169,24 +192,21 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     }
     __syncthreads();
     constexpr int RS = kDenseOT + kDenseOT / 8;
-    float2 *red = Z;
+    float2 *red = Z + warp * RS + lane * (R + 1);
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        int o = lane * R + r;
-        red[warp * RS + o + (o >> 3)] = make_float2(ar[r], ai[r]);
-    }
+    for (int r = 0; r < R; ++r) red[r] = make_float2(ar[r], ai[r]);
     __syncthreads();
     {
-        int o = threadIdx.x;
-        float2 s = make_float2(0.f, 0.f);
+        const int o = threadIdx.x;
+        float2 sum = make_float2(0.f, 0.f);
 #pragma unroll
         for (int wv = 0; wv < 8; ++wv) {
-            float2 v = red[wv * RS + o + (o >> 3)];
-            s.x += v.x;
-            s.y += v.y;
+            const float2 v = Z[wv * RS + o + (o >> 3)];
+            sum.x += v.x;
+            sum.y += v.y;
         }
-        int j = j0 + o;
-        if (j < sb.n_out) ext[sb.ext_off + j] = s;
+        const int j = j0 + o;
+        if (j < sb.n_out) ext[sb.ext_off + j] = sum;
     }
 }
 
@@ -728,6 +748,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     __shared__ float s_max[kNW][4];
     __shared__ float s_cmax[2][4];       // CTA max |d|, double-buffered
     __shared__ SegState s_first[kNW];    // each warp's first segment start (lane 0)
+    __shared__ float s_jac[16][kNewtonThreads];  // each segment's Jacobian, kept for chord steps
     __shared__ double s_sum[kNW][2];
     __shared__ double s_csum[2];
     const int csize = (int)cl.num_blocks();
@@ -753,6 +774,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     const bool has_next = t1 < n;  // the next thread's segment is not empty
     SegState x0{0.0, 0.0, I0, Q0};  // this segment's start: the free-running guess
     bool converged = false, bad = true;
+    float prev_m0 = 1e30f;  // last iteration's largest phase correction (uniform in the cluster)
     int iters = 0;
     for (int it = 0; it < max_iters && !converged; ++it) {
         iters = it + 1;
@@ -774,18 +796,36 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             }
         }
         // ---- integrate the segment: end state and Jacobian ----------------
+        // Close to the solution (the last corrections below 1e-2 rad) the
+        // segment Jacobians barely move: they are kept from the last full
+        // evaluation (chord steps), which converge as fast as Newton there.
+        const bool jac = it < 2 || prev_m0 > 1e-2f;
         Aff m;
         aff_identity(m);
         SegState x = x0;
         if (t0 < t1) {
             float pt = __ldg(pil + t0);
-            for (int t = t0; t < t1; ++t) {
-                const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
-                PllEval o;
-                pll_step<true>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
-                mat_push(m.a, o, om);
-                x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
-                pt = pn;
+            if (jac) {
+                for (int t = t0; t < t1; ++t) {
+                    const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
+                    PllEval o;
+                    pll_step<true>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                    mat_push(m.a, o, om);
+                    x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+                    pt = pn;
+                }
+#pragma unroll
+                for (int i = 0; i < 16; ++i) s_jac[i][threadIdx.x] = m.a[i];
+            } else {
+                for (int t = t0; t < t1; ++t) {
+                    const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
+                    PllEval o;
+                    pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                    x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+                    pt = pn;
+                }
+#pragma unroll
+                for (int i = 0; i < 16; ++i) m.a[i] = s_jac[i][threadIdx.x];
             }
             if (has_next) {
                 m.b[0] = (float)(x.dphi - nx.dphi);
@@ -883,6 +923,14 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             m3 = fmaxf(m3, rm[3]);
         }
         converged = (m0 <= kTolPhase && m1 <= kTolFreq && m2 <= kTolIQ && m3 <= kTolIQ);
+        // Accepted one iteration early when the next correction is predicted
+        // below the tolerance: corrections shrinking at least linearly at rate
+        // m0 / prev_m0 leave a next one of m0^2 / prev_m0 (Newton's quadratic
+        // rate leaves less), with the other components already near their floor.
+        if (!converged && it >= 1 && m0 <= 1e-5f && m0 * m0 <= kTolPhase * prev_m0 && m1 <= 1e-10f &&
+            m2 <= 1e-6f && m3 <= 1e-6f)
+            converged = true;
+        prev_m0 = m0;
     }
     // ---- not converged: the longest consistent prefix is kept ------------
     // Segments before the first one whose start still moved by more than the
