@@ -50,6 +50,7 @@ cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBl
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
                               const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters);
 int pll_newton_threads();
+int pll_cluster_for(int max_n);
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
                            const float *audio_dl, float *audio);
@@ -791,15 +792,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     }
     if (!pl.pll_list.empty()) {
         if (r->pll_parallel) {
-            // cluster size: enough CTAs to cover the SMs, no more than 8 per
-            // channel, at least 8 steps per thread
+            // cluster size: one thread per segment of the longest block
             int nch = (int)pl.pll_list.size();
             int max_n = 0;
             for (int i : pl.pll_list) max_n = std::max(max_n, pl.sbs[(size_t)i].n_disc);
-            int cluster = 1;
-            while (cluster < 8 && nch * cluster * 2 <= 3 * r->num_sms &&
-                   max_n / (cluster * 2 * pll_newton_threads()) >= 8)
-                cluster *= 2;
+            const int cluster = pll_cluster_for(max_n);
             prof_mark(r, f, "pll_newton");
             CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->pll_max_iters));
         } else {

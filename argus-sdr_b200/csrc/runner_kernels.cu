@@ -654,6 +654,25 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
 // pass integrates each segment from its converged start and writes the
 // outputs.
 constexpr int kNewtonThreads = 256;
+constexpr int kNewtonMaxCluster = 8;
+constexpr int kNewtonMinSeg = 16;
+
+// Steps per segment (per thread) for a block of n loop steps.
+__host__ __device__ inline int pll_segment_len(int n) {
+    const int cap = kNewtonMaxCluster * kNewtonThreads;
+    const int s = (n + cap - 1) / cap;
+    return s > kNewtonMinSeg ? s : kNewtonMinSeg;
+}
+
+// CTAs per cluster that give every channel of a launch (at most max_n steps)
+// one thread per segment.
+int pll_cluster_for(int max_n) {
+    const int seg = (max_n + pll_segment_len(max_n) - 1) / pll_segment_len(max_n);
+    int c = (seg + kNewtonThreads - 1) / kNewtonThreads;
+    int p = 1;
+    while (p < c) p *= 2;
+    return p < 1 ? 1 : (p > kNewtonMaxCluster ? kNewtonMaxCluster : p);
+}
 // Convergence: the last correction of every segment start is below what the
 // outputs resolve (the float32 sin/cos/atan2 and lowpass states leave a floor
 // near 1e-10 rad and 1e-9 in I/Q).
@@ -767,8 +786,11 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     const float om = 1.f - k.lpa;
     const float I0 = (float)s.pll_i, Q0 = (float)s.pll_q;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gthreads = csize * kNewtonThreads;
-    const int S = (n + gthreads - 1) / gthreads;
+    // The segment length depends on the channel's own block length only, so a
+    // channel's trajectory (and every rounding in it) is the same whatever
+    // other channels share the launch; the cluster supplies at least
+    // ceil(n / S) threads.
+    const int S = pll_segment_len(n);
     const int g = crank * kNewtonThreads + (int)threadIdx.x;
     const int t0 = min(n, g * S), t1 = min(n, t0 + S);
     const bool has_next = t1 < n;  // the next thread's segment is not empty

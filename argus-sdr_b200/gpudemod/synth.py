@@ -296,3 +296,61 @@ def fm_band_scene(device="cpu", block=1 << 20, n_stations=40, seconds=8.0, seed=
         stations.append(make_wfm_station(rng, off, amp, seconds=seconds))
     sigma = noise_sigma_for_snr(0.01 * noise_amp, 0.0, 200_000.0, fs)
     return WidebandScene(fs, block, stations, sigma, seed, device), stations
+
+
+# Channel parameters per mode, as the benchmark configurations give them:
+# (mode name, output rate, FIR taps, extraction bandwidth).  WFM channels are
+# stereo with RDS (FM band batch); the narrow modes follow the mixed batch.
+MODE_TABLE = {
+    "WFM": (312_500, 256, 250_000.0),
+    "NFM": (25_000, 512, 12_500.0),
+    "AM": (25_000, 384, 10_000.0),
+    "USB": (12_500, 256, 3_000.0),
+    "LSB": (12_500, 256, 3_000.0),
+    "CW": (5_000, 128, 500.0),
+}
+
+
+def mixed_scene(device="cpu", block=1 << 20, seed=CONFIG_SEEDS[2]):
+    """Mixed-mode uneven batch: 10 MS/s, 120 channels at random non-overlapping
+    offsets (25 kHz grid) with SNR 5-35 dB: 40 NFM, 30 AM, 15 USB, 15 LSB,
+    20 CW.  Returns the scene and [(kind, offset_hz)] per channel."""
+    rng = np.random.default_rng(seed)
+    fs = 10_000_000
+    kinds = ["NFM"] * 40 + ["AM"] * 30 + ["USB"] * 15 + ["LSB"] * 15 + ["CW"] * 20
+    grid = np.arange(-4_900_000.0, 4_900_001.0, 25_000.0)
+    offs = rng.choice(grid, size=len(kinds), replace=False)
+    snrs = rng.uniform(5.0, 35.0, len(kinds))
+    stations, chans = [], []
+    for kind, off, snr in zip(kinds, offs, snrs):
+        bw = MODE_TABLE[kind][2]
+        amp = math.sqrt(10 ** (snr / 10)) * 0.01 * math.sqrt(bw / 12_500.0)
+        stations.append(make_narrow_station(rng, kind, float(off), amp))
+        chans.append((kind, float(off)))
+    sigma = noise_sigma_for_snr(0.01, 0.0, 12_500.0, fs)
+    return WidebandScene(fs, block, stations, sigma, seed, device), chans
+
+
+def serving_scene(device="cpu", block=262144, seconds=10.0, seed=CONFIG_SEEDS[3]):
+    """Serving stream source: a continuous 10 MS/s band with 12 WFM stations
+    (stereo + RDS) and 48 narrow stations (NFM / AM / SSB / CW) at random
+    non-overlapping positions, SNR 5-35 dB, plus AWGN.  Demod requests land
+    at uniform-random frequencies over the band, on a station or on noise."""
+    rng = np.random.default_rng(seed)
+    fs = 10_000_000
+    wfm_grid = np.arange(-4_700_000.0, 4_700_001.0, 400_000.0)
+    wfm_offs = rng.choice(wfm_grid, size=12, replace=False)
+    narrow_grid = np.array([f for f in np.arange(-4_900_000.0, 4_900_001.0, 25_000.0)
+                            if np.min(np.abs(wfm_offs - f)) > 150_000.0])
+    narrow_offs = rng.choice(narrow_grid, size=48, replace=False)
+    kinds = ["NFM"] * 16 + ["AM"] * 12 + ["USB"] * 6 + ["LSB"] * 6 + ["CW"] * 8
+    stations = []
+    for off in wfm_offs:
+        amp = math.sqrt(10 ** (rng.uniform(5.0, 35.0) / 10)) * 0.01
+        stations.append(make_wfm_station(rng, float(off), amp, seconds=seconds + 1))
+    for kind, off in zip(kinds, narrow_offs):
+        bw = MODE_TABLE[kind][2]
+        amp = math.sqrt(10 ** (rng.uniform(5.0, 35.0) / 10)) * 0.01 * math.sqrt(bw / 12_500.0)
+        stations.append(make_narrow_station(rng, kind, float(off), amp))
+    sigma = noise_sigma_for_snr(0.01, 0.0, 200_000.0, fs)
+    return WidebandScene(fs, block, stations, sigma, seed, device), stations
