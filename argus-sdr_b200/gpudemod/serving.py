@@ -90,12 +90,13 @@ class ServingLoop:
         self.admitted = 0
         self.retired = 0
 
-    def _admit(self, req: Request) -> bool:
+    def _admit(self, req: Request):
+        """True when admitted; otherwise the refusal code (E_BUDGET / E_SLOTS)."""
         try:
             slot = self.r.admit(*channel_spec(req))
         except GPUDError as e:
             if e.code in (E_BUDGET, E_SLOTS):
-                return False
+                return e.code
             raise
         self.live[req.rid] = (slot, req)
         self.admitted += 1
@@ -110,8 +111,13 @@ class ServingLoop:
             self.retired += 1
         waiting = [q for q in self.pending if q.t_end > t_now] + list(arrivals)
         self.pending = []
+        full = False
         for q in waiting:
-            if not self._admit(q):
+            # no slot frees up before the next boundary once the cap is hit; a
+            # budget refusal still lets a smaller channel through
+            got = False if full else self._admit(q)
+            if got is not True:
+                full = full or got == E_SLOTS
                 self.refused.add(q.rid)
                 self.pending.append(q)
 
