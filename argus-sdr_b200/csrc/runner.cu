@@ -11,9 +11,10 @@
 //   - one launch sequence per block for all channels, with per-kernel work
 //     lists of (slot, tile) pairs for uneven taps / decimation,
 //   - one H2D of the block, one H2D of the descriptors, one D2H of all outputs,
-//   - two frames in flight: block k+1's front half (extraction, demod, stereo
-//     FIR bank, RDS) overlaps block k's back half (pilot PLL, stereo output),
-//     ordered by events, with the copies overlapping compute.
+//   - up to three blocks in flight, each with its own frame of buffers: block
+//     k+1's front half (extraction, demod, stereo FIR bank, RDS) overlaps
+//     block k's back half (pilot PLL, stereo output), ordered by events, and
+//     the copies of neighbouring blocks overlap compute.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -64,6 +65,7 @@ cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, co
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res);
 int rds_smem_bytes(int dr);
 int dense_smem_bytes_host(int P, int L);
+int wide_smem_bytes_host(int T);
 
 constexpr int kWfmTapsPadH = 104;
 struct WfmTapsHost {
@@ -75,6 +77,7 @@ constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
 constexpr int kPllMaxIters = 64;
+constexpr int kFrames = 3;  // blocks in flight
 
 // ---------------------------------------------------------------------------
 // DSP design helpers (host) -- restated from the reference
@@ -250,7 +253,7 @@ struct gpud_runner {
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
     // frames
-    Frame fr[2];
+    Frame fr[kFrames];
     int nxt = 0;        // frame the next block uses
     int last = -1;      // frame of the last submitted block
     int done_frame = -1;  // frame whose results gpud_runner_result reads
@@ -479,10 +482,15 @@ static int finish_frame(gpud_runner *r, int fi, int timeout_ms) {
 }
 
 // Wait for every block in flight (oldest first).
+static int oldest_inflight(const gpud_runner *r) {
+    int a = -1;
+    for (int k = 0; k < kFrames; ++k)
+        if (r->fr[k].inflight && (a < 0 || r->fr[k].ticket < r->fr[a].ticket)) a = k;
+    return a;
+}
+
 static int drain(gpud_runner *r) {
-    for (int k = 0; k < 2; ++k) {
-        int a = r->fr[0].inflight && (!r->fr[1].inflight || r->fr[0].ticket < r->fr[1].ticket) ? 0 : 1;
-        if (!r->fr[a].inflight) continue;
+    for (int a = oldest_inflight(r); a >= 0; a = oldest_inflight(r)) {
         int rc = finish_frame(r, a, -1);
         if (rc) return rc;
     }
@@ -584,7 +592,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
                 pl.dense_smem[s.L] = std::max(pl.dense_smem[s.L], dense_smem_bytes_host(s.P, s.L));
             } else {
                 for (int t = 0; t * 32 < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));
-                pl.wide_smem = std::max(pl.wide_smem, s.T * 4);
+                pl.wide_smem = std::max(pl.wide_smem, wide_smem_bytes_host(s.T));
             }
         }
         int mode = s.spec.mode;
@@ -899,7 +907,7 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
     f.inflight = true;
     f.ticket = ++r->submitted;
     r->last = fi;
-    r->nxt = 1 - fi;
+    r->nxt = (fi + 1) % kFrames;
     r->blocks++;
     return 0;
 }
@@ -1249,9 +1257,7 @@ GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int tim
     std::lock_guard<std::recursive_mutex> lk(r->mu);
     // finish blocks in order until `ticket` has completed
     while (r->completed < ticket) {
-        int a = -1;
-        for (int k = 0; k < 2; ++k)
-            if (r->fr[k].inflight && (a < 0 || r->fr[k].ticket < r->fr[a].ticket)) a = k;
+        const int a = oldest_inflight(r);
         if (a < 0) break;
         int rc = finish_frame(r, a, timeout_ms < 0 ? -1 : timeout_ms);
         if (rc) return rc;
@@ -1301,7 +1307,7 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->phase_count = s.pc;
     out->history_len = s.hist_len;
     if (r->done_frame < 0) {
-        if (r->fr[0].inflight || r->fr[1].inflight) return set_err(r, GPUD_E_TIMEOUT, "block still in flight");
+        if (oldest_inflight(r) >= 0) return set_err(r, GPUD_E_TIMEOUT, "block still in flight");
         return 0;
     }
     Frame &f = r->fr[r->done_frame];

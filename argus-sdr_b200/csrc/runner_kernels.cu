@@ -211,47 +211,90 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
 }
 
 // Wide form (short polyphase arms, or tiles too large for shared memory): one
-// warp per output, lanes stride the taps, warp-shuffle reduction.
+// warp per kWideOPW outputs, lanes stride the taps, warp-shuffle reduction.
+// The NCO rotation is folded into the taps: for a sample of this block,
+//     h[k] * x[n-k] * exp(j phi(n-k)) = exp(j phi(n)) * (h[k] exp(-j k inc)) * x[n-k],
+// so each CTA builds the modulated taps hc[k] = h[k] exp(-j k inc) once (exact
+// Q0.64 phases) and each output takes one rotation exp(j phi(n)) at the end;
+// history samples (already shifted) take the real taps directly.
 constexpr int kWideOPW = 4;                  // outputs per warp
 constexpr int kWideOT = 8 * kWideOPW;        // outputs per 256-thread tile
+
+int wide_smem_bytes_host(int T) { return T * 12; }
 
 __global__ void __launch_bounds__(256)
 k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
                const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
                const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
                float2 *__restrict__ ext) {
-    extern __shared__ float smemf[];
+    extern __shared__ float4 smemw4[];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const int j0 = w.y * kWideOT;
     if (j0 >= sb.n_out) return;
     const ChanParams &cp = prm[sb.slot];
     const int T = cp.ntaps, D = cp.decim;
-    for (int i = threadIdx.x; i < T; i += 256) smemf[i] = taps_arena[cp.dtaps_off + i];
+    const uint64_t u0 = st[sb.slot].nco_q;
+    const uint64_t inc = cp.inc_q;
+    float2 *hc = reinterpret_cast<float2 *>(smemw4);
+    float *hr = reinterpret_cast<float *>(hc + T);
+    for (int k = threadIdx.x; k < T; k += 256) {
+        const float h = taps_arena[cp.dtaps_off + k];
+        const float2 ph = q64_phasor((uint64_t)0 - (uint64_t)k * inc);
+        hr[k] = h;
+        hc[k] = make_float2(h * ph.x, h * ph.y);
+    }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = D - sb.pc - 1;
-    const uint64_t u0 = st[sb.slot].nco_q;
-    const uint64_t inc = cp.inc_q;
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
     const int H = sb.hist_len;
-    for (int o = 0; o < kWideOPW; ++o) {
-        int j = j0 + warp * kWideOPW + o;
-        if (j >= sb.n_out) break;
-        int nj = s0 + j * D;
-        float ar = 0.f, ai = 0.f;
-        for (int k = lane; k < T; k += 32) {
-            float2 v = shifted_sample(nj - k, n, x, u0, inc, hist, H);
-            float h = smemf[k];
-            ar = fmaf(h, v.x, ar);
-            ai = fmaf(h, v.y, ai);
+    const int jw = j0 + warp * kWideOPW;
+    if (jw >= sb.n_out) return;
+    const int no = min(kWideOPW, sb.n_out - jw);
+    float ar[kWideOPW], ai[kWideOPW], br[kWideOPW], bi[kWideOPW];
+#pragma unroll
+    for (int o = 0; o < kWideOPW; ++o) ar[o] = ai[o] = br[o] = bi[o] = 0.f;
+    const int nj0 = s0 + jw * D;
+    for (int k = lane; k < T; k += 32) {
+        const float2 c = hc[k];
+#pragma unroll
+        for (int o = 0; o < kWideOPW; ++o) {
+            if (o >= no) break;
+            const int i = nj0 + o * D - k;
+            if (i >= 0) {
+                const float2 v = __ldg(x + i);
+                ar[o] = fmaf(c.x, v.x, fmaf(-c.y, v.y, ar[o]));
+                ai[o] = fmaf(c.x, v.y, fmaf(c.y, v.x, ai[o]));
+            } else if (H + i >= 0) {
+                const float2 v = hist[H + i];
+                const float h = hr[k];
+                br[o] = fmaf(h, v.x, br[o]);
+                bi[o] = fmaf(h, v.y, bi[o]);
+            }
         }
+    }
+#pragma unroll
+    for (int o = 0; o < kWideOPW; ++o) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
-            ar += __shfl_xor_sync(0xffffffffu, ar, off);
-            ai += __shfl_xor_sync(0xffffffffu, ai, off);
+            ar[o] += __shfl_xor_sync(0xffffffffu, ar[o], off);
+            ai[o] += __shfl_xor_sync(0xffffffffu, ai[o], off);
+            br[o] += __shfl_xor_sync(0xffffffffu, br[o], off);
+            bi[o] += __shfl_xor_sync(0xffffffffu, bi[o], off);
         }
-        if (lane == 0) ext[sb.ext_off + j] = make_float2(ar, ai);
+    }
+    if (lane < no) {
+        // lane o writes output o (register arrays indexed by a compile-time loop)
+#pragma unroll
+        for (int o = 0; o < kWideOPW; ++o) {
+            if (o == lane) {
+                const int nj = nj0 + o * D;
+                const float2 rot = q64_phasor(u0 + (uint64_t)(int64_t)nj * inc);
+                const float2 y = cmulf(make_float2(ar[o], ai[o]), rot);
+                ext[sb.ext_off + jw + o] = make_float2(y.x + br[o], y.y + bi[o]);
+            }
+        }
     }
 }
 

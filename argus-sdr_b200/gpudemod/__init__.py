@@ -187,8 +187,8 @@ class ChannelRunner:
         ptr, n, dev, keep = _iq_ptr(iq)
         t = C.c_uint64()
         _check(self._r, lib.gpud_runner_submit(self._r, ptr, n, dev, C.byref(t)))
-        # two blocks may be in flight: keep both inputs alive
-        self._keep = (getattr(self, "_keep", (None, None))[1], keep)
+        # three blocks may be in flight: keep their inputs alive
+        self._keep = (getattr(self, "_keep", (None, None, None)) + (keep,))[-3:]
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 10000):

@@ -316,17 +316,16 @@ def run_reference(args):
     barrier(world)
 
 
-def pipelined(runner, inputs):
-    """Submit every block with two in flight; each block's outputs are in host
-    memory (or the device arena) after its wait."""
-    prev = None
+def pipelined(runner, inputs, depth=3):
+    """Submit every block with up to `depth` in flight; each block's outputs
+    are in host memory (or the device arena) after its wait."""
+    tickets = []
     for x in inputs:
-        t = runner.submit(x)
-        if prev is not None:
-            runner.wait(prev)
-        prev = t
-    if prev is not None:
-        runner.wait(prev)
+        tickets.append(runner.submit(x))
+        if len(tickets) >= depth:
+            runner.wait(tickets[-depth])
+    if tickets:
+        runner.wait(tickets[-1])
 
 
 def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, make_plain, cpu_baseline):
@@ -353,15 +352,14 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)  # the runner's join stream: events there follow every submitted block
-    prev = None
+    tickets = []
     for s in range(args.steps):
-        t = runner.submit(blocks[(args.warmup + s) % n_scene])  # two blocks in flight
-        if prev is not None:
-            runner.wait(prev)
+        tickets.append(runner.submit(blocks[(args.warmup + s) % n_scene]))  # three blocks in flight
+        if len(tickets) >= 3:
+            runner.wait(tickets[-3])
             for name, ms in runner.stage_times():
                 stage_acc.setdefault(name, []).append(ms)
-        prev = t
-    runner.wait(prev)
+    runner.wait(tickets[-1])
     for name, ms in runner.stage_times():
         stage_acc.setdefault(name, []).append(ms)
     e1.record(stream)

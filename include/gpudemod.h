@@ -260,16 +260,17 @@ GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_
 GPUD_API int GPUD_CALL gpud_runner_process_block(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device);
 /* Asynchronous form: enqueue the block and return a ticket; wait returns 0
  * once the outputs of every block up to that ticket are in host memory
- * (GPUD_E_TIMEOUT after timeout_ms).  Two blocks may be in flight: block k+1's
- * extraction / demod / stereo FIR / RDS stages run while block k's pilot PLL
- * and stereo output finish; a third submit first completes the oldest block.
+ * (GPUD_E_TIMEOUT after timeout_ms).  Three blocks may be in flight: block
+ * k+1's extraction / demod / stereo FIR / RDS stages run while block k's pilot
+ * PLL and stereo output finish, and their copies overlap; a fourth submit first
+ * completes the oldest block.
  * A pinned host iq buffer is read asynchronously and must stay unchanged until
  * its block completed; pageable buffers are copied before submit returns. */
 GPUD_API int GPUD_CALL gpud_runner_submit(gpud_runner *r, const gpud_float2 *iq, int n, int iq_on_device,
                                           uint64_t *ticket);
 GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int timeout_ms);
 /* Outputs of the most recently completed block (process_block or wait).  The
- * pointers stay valid until the second submit after that block;
+ * pointers stay valid until the third submit after that block;
  * GPUD_E_TIMEOUT when blocks are in flight and none has completed since. */
 GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel_result *out);
 GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *out);

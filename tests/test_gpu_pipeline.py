@@ -268,8 +268,9 @@ def test_parallel_pll_fallback_and_clusters(cuda):
 
 
 
-def test_pipelined_submit_equals_sequential(cuda):
-    """Two blocks in flight (block k+1's front half overlapping block k's PLL
+@pytest.mark.parametrize("depth", [2, 3])
+def test_pipelined_submit_equals_sequential(cuda, depth):
+    """Two or three blocks in flight (block k+1's front half overlapping block k's PLL
     and stereo output), with drift updates, retires and admissions made while
     a block is in flight: every output is bit-identical to the one block at a
     time runner given the same calls at the same block boundaries."""
@@ -310,12 +311,13 @@ def test_pipelined_submit_equals_sequential(cuda):
         tickets = []
         for k, x in enumerate(blocks):
             tickets.append(rp.submit(x))
-            if k >= 1:
-                rp.wait(tickets[k - 1])
+            if k >= depth - 1:
+                rp.wait(tickets[k - depth + 1])
                 pipe.append(collect(rp, live_p))
             calls(rp, live_p, k)
-        rp.wait(tickets[-1])
-        pipe.append(collect(rp, live_p))
+        for k in range(len(blocks) - depth + 1, len(blocks)):
+            rp.wait(tickets[k])
+            pipe.append(collect(rp, live_p))
         assert len(seq) == len(pipe) == len(blocks)
         for k, (a, b) in enumerate(zip(seq, pipe)):
             # block k's results are read after the calls made while it was in

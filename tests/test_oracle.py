@@ -241,3 +241,22 @@ def test_demod_semantics():
     assert d.size == 999
     assert np.allclose(d, np.angle(iq[1:].astype(np.complex128) * np.conj(iq[:-1].astype(np.complex128))),
                        atol=1e-6)
+
+
+def test_truth64_chain_agrees_with_oracle():
+    """The float64 truth chain and the reference-precision restatement differ
+    only by float32 rounding (pins the truth's sample timing, taps, PLL, lock
+    and RDS stream)."""
+    from gpudemod import synth
+    from oracle import truth64 as T64
+    scene, _ = synth.plain_wfm_scene(block=65_536)
+    o = O.OracleChannel(2_400_000, 300_000.0, 250_000.0, 300_000, 128, O.MODE_WFM_STEREO, rds=True)
+    t = T64.Truth64Channel(2_400_000, 300_000.0, 250_000.0, 300_000, 128, T64.MODE_WFM_STEREO, rds=True)
+    for _ in range(3):
+        x = scene.next_block().numpy()
+        a, b = o.process(x), t.process(x)
+        for key in ("iq", "audio", "rds"):
+            assert a[key].size == b[key].size
+            d = np.linalg.norm(a[key] - b[key]) / np.linalg.norm(b[key])
+            assert d < 2e-6, (key, d)
+        assert a["locked"] == b["locked"]
