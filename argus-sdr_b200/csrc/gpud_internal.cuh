@@ -78,13 +78,14 @@ struct ChanParams {
     int32_t hcap;     // history capacity (>= T-1)
     int32_t wfm_idx;  // index into WFM arenas (-1 when not WFM)
     int32_t rds_dr;   // RDS decimation floor(out_rate/19000)
-    int32_t pad0;
+    int32_t rs_bank;  // 48 kHz resampler bank id (GPUD_CH_AUDIO48K)
     double ssb_inc;   // 2*pi*(+-700)/out_rate for USB/LSB/CW
     double pll_alpha, pll_beta, pll_lpa;   // stereo PLL constants
     double pll_fmin, pll_fmax;             // freq clamp (rad/sample)
     double rds_inc;                        // 2*pi*57000/out_rate
     int32_t rds_tab;                       // binade table id for the RDS phase
-    int32_t pad1;
+    int32_t aud_ch;                        // audio channels (2 for WFM_STEREO, else 1)
+    double deemph_a;                       // de-emphasis coefficient exp(-1/(48000 tau)), 0: none
 };
 
 // Per-slot state carried across blocks.
@@ -122,6 +123,25 @@ struct SlotBlock {
     int32_t rds_first; // first composite index of this block that is kept (-1: none)
     int32_t comp_hist_len; // valid samples in the composite delay line (<= 100)
     int32_t res_idx;   // index into the results table
+    // 48 kHz audio back end (GPUD_CH_AUDIO48K)
+    int32_t rs_t0;     // resampler phase counter before the block (outTime)
+    int32_t rs_nout;   // 48 kHz frames produced this block
+    int32_t pcm_off;   // int16 offset into the PCM output region
+    int32_t rs_frames; // demod-rate frames consumed this block
+};
+
+// Rational polyphase resampler bank (dsp/resample.go:45-93) for one input rate.
+constexpr int kRsTaps = 33;     // taps per arm at 32 taps per phase (odd prototype)
+constexpr int kRsMaxL = 128;
+struct RsBank {
+    int32_t L, M, K, pad;
+    double arm[kRsMaxL * kRsTaps];  // arm[p*K + t]
+};
+
+// Per-slot audio back-end state.
+struct AudState {
+    float dl[2][kRsTaps];  // resampler delay lines, [0] newest
+    double y[2];           // de-emphasis states
 };
 
 // Results table row written by the device each block.

@@ -63,6 +63,8 @@ cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, c
                               float2 *rds_dl, const BinadeTable *tabs, DevResult *res);
 cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res);
+cudaError_t launch_audio48(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
+                           const RsBank *banks, AudState *aud, const float *audio, int16_t *pcm);
 int rds_smem_bytes(int dr);
 int dense_smem_bytes_host(int P, int L);
 int wide_smem_bytes_host(int T);
@@ -78,6 +80,7 @@ constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
 constexpr int kPllMaxIters = 64;
 constexpr int kFrames = 3;  // blocks in flight
+constexpr int kMaxRsClasses = 16;  // 48 kHz resampler banks (one per demod rate)
 
 // ---------------------------------------------------------------------------
 // DSP design helpers (host) -- restated from the reference
@@ -169,6 +172,8 @@ struct Slot {
     int pc = 0, hist_len = 0, hist_sel = 0, comp_hist_len = 0;
     bool has_last = false;
     int64_t rds_count = 0;
+    int64_t rs_t = 0;  // 48 kHz resampler phase counter (outTime)
+    int rs_class = -1, rs_L = 1, rs_M = 1, aud_ch = 1;
     uint64_t footprint = 0;
 };
 
@@ -183,7 +188,9 @@ struct BlockPlan {
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
-    int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_rds = 0;
+    std::vector<int> aud_list;  // entries with a 48 kHz back end and input this block
+    int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_audio_host = 0, tot_rds = 0,
+            tot_pcm = 0;
 };
 
 struct SlotAfter {
@@ -214,7 +221,7 @@ struct Frame {
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
-    size_t off_res = 0, off_audio = 0, off_rds = 0, off_ext = 0, out_bytes = 0;
+    size_t off_res = 0, off_pcm = 0, off_audio = 0, off_rds = 0, off_ext = 0, out_bytes = 0;
     bool host_outputs = true;
     uint64_t ticket = 0;
     bool inflight = false;
@@ -249,6 +256,10 @@ struct gpud_runner {
     WfmTapsHost *d_wtaps = nullptr;
     BinadeTable *d_tabs = nullptr;
     std::vector<int> class_rate;  // rate of each WFM rate class
+    AudState *d_aud = nullptr;    // per slot
+    RsBank *d_banks = nullptr;
+    std::vector<int> rs_rate;     // input rate of each resampler bank
+    std::vector<int3> rs_lmk;     // (L, M, K) of each bank
     bool pll_parallel = true;
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
@@ -329,12 +340,108 @@ static uint64_t slot_block_bytes(const gpud_runner *r, int D, int mode, int flag
     if (wfm) b += 5 * (nout + 8) * 4;  // composite work arrays
     if (mode != GPUD_MODE_IQ) b += nout * 4 * (mode == GPUD_MODE_WFM_STEREO ? 2 : 1);
     if (wfm && (flags & GPUD_CH_RDS)) b += (nout / 16 + 4) * 8;
-    return 2 * b;
+    if (flags & GPUD_CH_AUDIO48K) {
+        // s16le at 48 kHz: at most nout * 48000 / out_rate + 2 frames
+        uint64_t out_rate = (uint64_t)r->fs / (uint64_t)D;
+        b += (nout * 48000 / out_rate + 4) * 2 * (mode == GPUD_MODE_WFM_STEREO ? 2 : 1);
+    }
+    return kFrames * b;
 }
 
 static uint64_t slot_state_bytes(const gpud_runner *r) {
     return sizeof(ChanParams) + sizeof(ChanState) + (uint64_t)r->tapcap * 2 * 4 + (uint64_t)2 * r->max_taps * 8 +
-           (kWfmHist * 3 + kAudioDlStrideH) * 8;
+           (kWfmHist * 3 + kAudioDlStrideH) * 8 + sizeof(AudState);
+}
+
+// NewResampler (dsp/resample.go:45-93, 256-295): L/M from the gcd, odd
+// prototype of L*32(+1) taps, windowed sinc fc = 0.90/max(L, M), Kaiser
+// beta 6 (bessel0 series), gain L, split into L arms of K taps.
+static double rs_bessel0(double x) {
+    double sum = 1.0, term = 1.0;
+    for (int k = 1; k < 30; k++) {
+        term *= (x / (2 * (double)k)) * (x / (2 * (double)k));
+        sum += term;
+        if (term < 1e-12 * sum) break;
+    }
+    return sum;
+}
+
+static int rs_gcd(int a, int b) {
+    while (b != 0) {
+        int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a < 0 ? -a : a;
+}
+
+static bool build_rs_bank(int in_rate, int out_rate, RsBank *bk) {
+    std::memset(bk, 0, sizeof *bk);
+    const int g = rs_gcd(in_rate, out_rate);
+    const int l = out_rate / g, m = in_rate / g;
+    int plen = l * 32;
+    if (plen % 2 == 0) plen++;
+    const int k = (plen + l - 1) / l;
+    if (l > kRsMaxL || k > kRsTaps) return false;
+    const double fc = 0.90 / (double)std::max(l, m);
+    const double mid = (double)(plen - 1) / 2.0, b0 = rs_bessel0(6.0);
+    for (int p = 0; p < l; ++p)
+        for (int t = 0; t < k; ++t) {
+            const int n = p + t * l;
+            double v = 0.0;
+            if (n < plen) {
+                const double x = (double)n - mid;
+                const double sn = std::fabs(x) < 1e-12 ? 2 * GPUD_PI * fc : std::sin(2 * GPUD_PI * fc * x) / x;
+                const double xx = x / mid;
+                v = sn * (rs_bessel0(6.0 * std::sqrt(1 - xx * xx)) / b0) * (double)l;
+            }
+            bk->arm[p * k + t] = v;
+        }
+    bk->L = l;
+    bk->M = m;
+    bk->K = k;
+    return true;
+}
+
+static int rs_class_for(gpud_runner *r, int rate) {
+    for (size_t i = 0; i < r->rs_rate.size(); ++i)
+        if (r->rs_rate[i] == rate) return (int)i;
+    if ((int)r->rs_rate.size() >= kMaxRsClasses) return -1;
+    std::vector<char> buf(sizeof(RsBank));
+    RsBank *bk = reinterpret_cast<RsBank *>(buf.data());
+    if (!build_rs_bank(rate, 48000, bk)) return -1;
+    const int id = (int)r->rs_rate.size();
+    // a new bank id is not referenced by any block in flight
+    if (cudaMemcpyAsync(r->d_banks + id, bk, sizeof(RsBank), cudaMemcpyHostToDevice, r->admin) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(r->admin) != cudaSuccess) return -1;
+    r->rs_rate.push_back(rate);
+    r->rs_lmk.push_back(make_int3(bk->L, bk->M, bk->K));
+    return id;
+}
+
+// Resampler.Process over n inputs from phase counter t0 (dsp/resample.go:
+// 105-153): frames produced and the counter after, including the method's
+// exit inside its consume loop (the counter is reduced by L for the sample it
+// could not consume).  Output o is produced iff floor((t0+oM)/L) <= n and, for
+// o >= 1, floor((t0+(o-1)M)/L) < n.
+static void rs_advance(int64_t L, int64_t M, int64_t t0, int64_t n, int64_t *nout, int64_t *t1) {
+    if (n <= 0) {
+        *nout = 0;
+        *t1 = t0;
+        return;
+    }
+    if (L == M) {
+        *nout = n;
+        *t1 = t0;
+        return;
+    }
+    auto cdiv = [](int64_t a, int64_t b) { return a >= 0 ? (a + b - 1) / b : -((-a) / b); };
+    const int64_t A = cdiv((n + 1) * L - t0, M) - 1;
+    int64_t last = -1;
+    if (A >= 0) last = std::max<int64_t>(0, std::min(A, cdiv(n * L - t0, M)));
+    const int64_t c_last = last >= 0 ? (t0 + last * M) / L : 0;
+    *nout = last + 1;
+    *t1 = t0 + (last + 1) * M - n * L - (c_last < n ? L : 0);
 }
 
 static int rate_class_for(gpud_runner *r, int rate) {
@@ -414,6 +521,13 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     p->pll_fmax = 2 * GPUD_PI * 21000 / (double)rate;
     p->rds_inc = -2 * GPUD_PI * (-57000.0) / (double)rate;
     p->rds_tab = s.rate_class < 0 ? 0 : s.rate_class;
+    p->rs_bank = s.rs_class < 0 ? 0 : s.rs_class;
+    p->aud_ch = s.aud_ch;
+    // de-emphasis tau (recorder/streamer.go:1443-1463): 50 us default, WFM only
+    const bool wfm = s.spec.mode == GPUD_MODE_WFM || s.spec.mode == GPUD_MODE_WFM_STEREO;
+    double tau_us = (s.spec.flags & GPUD_CH_DEEMPH75) ? 75.0 : 50.0;
+    if (s.spec.flags & GPUD_CH_NO_DEEMPH) tau_us = 0.0;
+    p->deemph_a = (wfm && tau_us > 0) ? std::exp(-1.0 / (48000.0 * tau_us * 1e-6)) : 0.0;
 }
 
 static void queue_write(gpud_runner *r, int slot, void *dst, const void *src, size_t bytes) {
@@ -540,6 +654,14 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
             sb.n_rds = (sb.n_disc - 1 - qf) / dr + 1;
         }
     }
+    sb.rs_t0 = (int)s.rs_t;
+    sb.rs_nout = sb.rs_frames = sb.pcm_off = 0;
+    if ((s.spec.flags & GPUD_CH_AUDIO48K) && s.rs_class >= 0 && sb.n_audio > 0) {
+        int64_t nout, t1;
+        sb.rs_frames = sb.n_audio / s.aud_ch;
+        rs_advance(s.rs_L, s.rs_M, s.rs_t, sb.rs_frames, &nout, &t1);
+        sb.rs_nout = (int)nout;
+    }
     sb.res_idx = (int)pl.sbs.size();
     pl.sbs.push_back(sb);
 }
@@ -557,19 +679,34 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             if (pass == 0) pl.tot_emit_ext = ext;
         }
     pl.tot_ext = ext;
-    int64_t comp = 0, audio = 0, rds = 0;
-    for (auto &sb : pl.sbs) {
+    int64_t comp = 0, audio = 0, rds = 0, pcm = 0;
+    // demod-rate audio: channels that return it to the host first, then those
+    // whose audio only feeds the 48 kHz back end on the device
+    pl.tot_audio_host = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (auto &sb : pl.sbs) {
+            const bool dev = (r->slots[(size_t)sb.slot].spec.flags & GPUD_CH_AUDIO48K) != 0;
+            if (dev != (pass == 1)) continue;
+            sb.audio_off = (int)audio;
+            audio += (sb.n_audio + 3) & ~3;
+            if (pass == 0) pl.tot_audio_host = audio;
+        }
+    pl.aud_list.clear();
+    for (int i = 0; i < (int)pl.sbs.size(); ++i) {
+        SlotBlock &sb = pl.sbs[(size_t)i];
         Slot &s = r->slots[(size_t)sb.slot];
         sb.comp_off = (int)comp;
         if (s.wfm_idx >= 0) comp += (sb.n_disc + 8 + 7) & ~7;
-        sb.audio_off = (int)audio;
-        audio += (sb.n_audio + 3) & ~3;
         sb.rds_off = (int)rds;
         rds += (sb.n_rds + 1) & ~1;
+        sb.pcm_off = (int)pcm;
+        pcm += ((int64_t)sb.rs_nout * s.aud_ch + 7) & ~7;
+        if (sb.rs_frames > 0) pl.aud_list.push_back(i);
     }
     pl.tot_comp = comp;
     pl.tot_audio = audio;
     pl.tot_rds = rds;
+    pl.tot_pcm = pcm;
     for (int L = 0; L <= kDenseMaxL; ++L) {
         pl.w_dense[L].clear();
         pl.dense_smem[L] = 0;
@@ -624,8 +761,8 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         r->graph_rebuilds++;
     }
     size_t res = align256(pl.sbs.size() * sizeof(DevResult));
-    size_t need = res + align256((size_t)pl.tot_audio * 4) + align256((size_t)pl.tot_rds * 8) +
-                  align256((size_t)pl.tot_ext * 8);
+    size_t need = res + align256((size_t)pl.tot_pcm * 2) + align256((size_t)pl.tot_audio * 4) +
+                  align256((size_t)pl.tot_rds * 8) + align256((size_t)pl.tot_ext * 8);
     if (need > f.out_cap) {
         cudaFree(f.d_out);
         if (f.h_out) cudaFreeHost(f.h_out);
@@ -642,7 +779,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
-                   align256(pl.pll_list.size() * 4) + 4096;
+                   align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
         cudaFree(f.d_desc);
         if (f.h_desc) cudaFreeHost(f.h_desc);
@@ -677,6 +814,11 @@ static void advance_mirrors(gpud_runner *r, const BlockPlan &pl, int n, std::vec
         if (s.wfm_idx >= 0) {
             s.comp_hist_len = std::min(kWfmHist, s.comp_hist_len + sb.n_disc);
             s.rds_count += sb.n_disc;
+        }
+        if (sb.rs_frames > 0) {
+            int64_t nout, t1;
+            rs_advance(s.rs_L, s.rs_M, s.rs_t, sb.rs_frames, &nout, &t1);
+            s.rs_t = t1;
         }
         if (after) after->push_back(SlotAfter{s.pc, s.hist_len});
     }
@@ -732,18 +874,24 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
            o_out = put(pl.w_out), o_rds = put(pl.w_rds);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
-    size_t dbytes = o_pll + pl.pll_list.size() * 4;
+    size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
+    std::memcpy(hd + o_aud, pl.aud_list.data(), pl.aud_list.size() * 4);
+    size_t dbytes = o_aud + pl.aud_list.size() * 4;
     CK(cudaMemcpyAsync(f.d_desc, hd, dbytes, cudaMemcpyHostToDevice, f.s));
     f.h2d += dbytes;
     const SlotBlock *d_sb = (const SlotBlock *)(f.d_desc + o_sb);
     const int2 *d_w = (const int2 *)(f.d_desc + o_w);
     const int *d_pll = (const int *)(f.d_desc + o_pll);
+    const int *d_aud_list = (const int *)(f.d_desc + o_aud);
 
+    // output arena: results | PCM | RDS | audio (host part, then device part) | IQ (emitted part first)
     f.off_res = 0;
-    f.off_audio = align256(pl.sbs.size() * sizeof(DevResult));
-    f.off_rds = f.off_audio + align256((size_t)pl.tot_audio * 4);
-    f.off_ext = f.off_rds + align256((size_t)pl.tot_rds * 8);
+    f.off_pcm = align256(pl.sbs.size() * sizeof(DevResult));
+    f.off_rds = f.off_pcm + align256((size_t)pl.tot_pcm * 2);
+    f.off_audio = f.off_rds + align256((size_t)pl.tot_rds * 8);
+    f.off_ext = f.off_audio + align256((size_t)pl.tot_audio * 4);
     DevResult *d_res = (DevResult *)(f.d_out + f.off_res);
+    int16_t *d_pcm = (int16_t *)(f.d_out + f.off_pcm);
     float *d_audio = (float *)(f.d_out + f.off_audio);
     float2 *d_rds = (float2 *)(f.d_out + f.off_rds);
     float2 *d_ext = (float2 *)(f.d_out + f.off_ext);
@@ -819,6 +967,12 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                           r->d_audio_dl, d_audio));
         nl++;
     }
+    if (!pl.aud_list.empty()) {
+        prof_mark(r, f, "audio48k");
+        CK(launch_audio48((int)pl.aud_list.size(), f.s, d_aud_list, d_sb, r->d_prm, r->d_banks, r->d_aud, d_audio,
+                          d_pcm));
+        nl++;
+    }
     if (!pl.sbs.empty()) {
         prof_mark(r, f, "post_back");
         CK(launch_post_back((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->d_lr_dl, r->d_audio_dl,
@@ -832,12 +986,20 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     f.out_bytes = f.off_ext + (size_t)pl.tot_emit_ext * 8;
     f.host_outputs = r->host_outputs;
     if (f.host_outputs) {
-        CK(cudaMemcpyAsync(f.h_out, f.d_out, f.out_bytes, cudaMemcpyDeviceToHost, f.s));
-        f.d2h += f.out_bytes;
+        // results, PCM, RDS and the audio of channels without a 48 kHz back
+        // end; then the IQ of channels that emit it
+        const size_t head = f.off_audio + (size_t)pl.tot_audio_host * 4;
+        CK(cudaMemcpyAsync(f.h_out, f.d_out, head, cudaMemcpyDeviceToHost, f.s));
+        f.d2h += head;
+        if (pl.tot_emit_ext > 0) {
+            CK(cudaMemcpyAsync(f.h_out + f.off_ext, f.d_out + f.off_ext, (size_t)pl.tot_emit_ext * 8,
+                               cudaMemcpyDeviceToHost, f.s));
+            f.d2h += (size_t)pl.tot_emit_ext * 8;
+        }
     } else {
         // the results table comes back; the payload stays on the device
-        CK(cudaMemcpyAsync(f.h_out, f.d_out, f.off_audio, cudaMemcpyDeviceToHost, f.s));
-        f.d2h += f.off_audio;
+        CK(cudaMemcpyAsync(f.h_out, f.d_out, f.off_pcm, cudaMemcpyDeviceToHost, f.s));
+        f.d2h += f.off_pcm;
     }
     prof_mark(r, f, "end");
     return 0;
@@ -930,9 +1092,10 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
     f.h2d = f.d2h = 0;
     f.prof_n = 0;
     std::vector<char> gathered;
+    // the batched arena layout: results | PCM | RDS | audio | IQ
     size_t res_b = align256(full.sbs.size() * sizeof(DevResult));
-    size_t a_off = res_b, r_off = a_off + align256((size_t)full.tot_audio * 4),
-           e_off = r_off + align256((size_t)full.tot_rds * 8);
+    size_t p_off = res_b, r_off = p_off + align256((size_t)full.tot_pcm * 2),
+           a_off = r_off + align256((size_t)full.tot_rds * 8), e_off = a_off + align256((size_t)full.tot_audio * 4);
     gathered.assign(e_off + align256((size_t)full.tot_ext * 8), 0);
     CK(cudaEventRecord(f.ev0, f.s));
     rc = apply_pending(r, f);
@@ -954,8 +1117,11 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
         const SlotBlock &o = one.sbs[0];
         const SlotBlock &fb = full.sbs[k];
         std::memcpy(gathered.data() + k * sizeof(DevResult), f.h_out + f.off_res, sizeof(DevResult));
-        std::memcpy(gathered.data() + a_off + (size_t)fb.audio_off * 4, f.h_out + f.off_audio + (size_t)o.audio_off * 4,
-                    (size_t)o.n_audio * 4);
+        if (!(s.spec.flags & GPUD_CH_AUDIO48K))
+            std::memcpy(gathered.data() + a_off + (size_t)fb.audio_off * 4,
+                        f.h_out + f.off_audio + (size_t)o.audio_off * 4, (size_t)o.n_audio * 4);
+        std::memcpy(gathered.data() + p_off + (size_t)fb.pcm_off * 2, f.h_out + f.off_pcm + (size_t)o.pcm_off * 2,
+                    (size_t)o.rs_nout * (size_t)s.aud_ch * 2);
         std::memcpy(gathered.data() + r_off + (size_t)fb.rds_off * 8, f.h_out + f.off_rds + (size_t)o.rds_off * 8,
                     (size_t)o.n_rds * 8);
         if (s.spec.flags & GPUD_CH_EMIT_IQ)
@@ -968,6 +1134,7 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
     if (gathered.size() > f.out_cap) return set_err(r, GPUD_E_CUDA, "plain gather overflow");
     std::memcpy(f.h_out, gathered.data(), gathered.size());
     f.off_res = 0;
+    f.off_pcm = p_off;
     f.off_audio = a_off;
     f.off_rds = r_off;
     f.off_ext = e_off;
@@ -1050,8 +1217,10 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     CKC(dalloc(&r->d_rds_dl, M * kWfmHist));
     CKC(dalloc(&r->d_wtaps, (size_t)kMaxWfmClasses));
     CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses));
+    CKC(dalloc(&r->d_aud, M));
+    CKC(dalloc(&r->d_banks, (size_t)kMaxRsClasses));
 #undef CKC
-    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 16;
+    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 8 * kFrames + sizeof(RsBank) * kMaxRsClasses;
     *out = r;
     return 0;
 }
@@ -1087,6 +1256,8 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     cudaFree(r->d_rds_dl);
     cudaFree(r->d_wtaps);
     cudaFree(r->d_tabs);
+    cudaFree(r->d_aud);
+    cudaFree(r->d_banks);
     if (r->stream) cudaStreamDestroy(r->stream);
     if (r->admin) cudaStreamDestroy(r->admin);
     delete r;
@@ -1152,6 +1323,11 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
         rclass = rate_class_for(r, spec->out_rate);
         if (rclass < 0) return set_err(r, GPUD_E_CUDA, "WFM rate classes exhausted");
     }
+    int rsclass = -1;
+    if ((spec->flags & GPUD_CH_AUDIO48K) && spec->mode != GPUD_MODE_IQ) {
+        rsclass = rs_class_for(r, spec->out_rate);
+        if (rsclass < 0) return set_err(r, GPUD_E_ARG, "no 48 kHz resampler for this output rate");
+    }
     drop_pending(r, slot);
     Slot &s = r->slots[(size_t)slot];
     s = Slot{};
@@ -1167,6 +1343,12 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     s.hist_off = slot * 2 * r->max_taps;
     s.wfm_idx = wfm ? slot : -1;
     s.rate_class = rclass;
+    s.rs_class = rsclass;
+    s.aud_ch = spec->mode == GPUD_MODE_WFM_STEREO ? 2 : 1;
+    if (rsclass >= 0) {
+        s.rs_L = r->rs_lmk[(size_t)rsclass].x;
+        s.rs_M = r->rs_lmk[(size_t)rsclass].y;
+    }
     int smem = dense_smem_bytes_host(s.P, s.L);
     s.ext_kind = (s.L >= 2 && s.L <= kDenseMaxL && smem <= kDenseSmemLimit) ? 0 : 1;
     s.footprint = fp;
@@ -1181,6 +1363,7 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     CK(cudaMemcpyAsync(r->d_taps + s.dtaps_off, h.data(), h.size() * 4, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemcpyAsync(r->d_prm + slot, &p, sizeof p, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemcpyAsync(r->d_st + slot, &st, sizeof st, cudaMemcpyHostToDevice, r->admin));
+    CK(cudaMemsetAsync(r->d_aud + slot, 0, sizeof(AudState), r->admin));
     if (s.wfm_idx >= 0) {
         CK(cudaMemsetAsync(r->d_comp_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
         CK(cudaMemsetAsync(r->d_lr_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
@@ -1329,7 +1512,13 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->pll_path = res->status;
     out->pll_iters = res->pll_iters;
     const char *base = f.host_outputs ? f.h_out : f.d_out;
-    out->audio = (const float *)(base + f.off_audio) + sb.audio_off;
+    const bool a48 = (s.spec.flags & GPUD_CH_AUDIO48K) != 0 && s.rs_class >= 0;
+    out->audio = (a48 && f.host_outputs) ? nullptr : (const float *)(base + f.off_audio) + sb.audio_off;
+    if (a48) {
+        out->pcm = (const int16_t *)(base + f.off_pcm) + sb.pcm_off;
+        out->n_pcm = sb.rs_nout * s.aud_ch;
+        out->pcm_rate = 48000;
+    }
     out->rds = (const gpud_float2 *)(base + f.off_rds) + sb.rds_off;
     out->iq = (s.spec.flags & GPUD_CH_EMIT_IQ) ? (const gpud_float2 *)(base + f.off_ext) + sb.ext_off : nullptr;
     return 0;
@@ -1379,10 +1568,11 @@ struct SnapHeader {
     int32_t pc, hist_len, hist_sel, comp_hist_len, has_last, pad;
     int64_t rds_count;
     double cutoff;
+    int64_t rs_t;  // 48 kHz resampler phase counter
 };
 
 static uint64_t snap_bytes(const Slot &s) {
-    uint64_t b = sizeof(SnapHeader) + sizeof(ChanState) + (uint64_t)s.hcap * 8;
+    uint64_t b = sizeof(SnapHeader) + sizeof(ChanState) + (uint64_t)s.hcap * 8 + sizeof(AudState);
     if (s.wfm_idx >= 0) b += kWfmHist * 4 * 2 + kAudioDlStrideH * 4 + kWfmHist * 8;
     return b;
 }
@@ -1401,8 +1591,8 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
     int rc = drain(r);
     if (rc) return rc;
     char *p = (char *)blob;
-    SnapHeader h{0x47505544u, 1, s.D, s.T, s.spec.mode, s.wfm_idx >= 0, s.pc, s.hist_len, s.hist_sel,
-                 s.comp_hist_len, s.has_last ? 1 : 0, 0, s.rds_count, s.cutoff};
+    SnapHeader h{0x47505544u, 2, s.D, s.T, s.spec.mode, s.wfm_idx >= 0, s.pc, s.hist_len, s.hist_sel,
+                 s.comp_hist_len, s.has_last ? 1 : 0, 0, s.rds_count, s.cutoff, s.rs_t};
     std::memcpy(p, &h, sizeof h);
     p += sizeof h;
     CK(cudaMemcpy(p, r->d_st + slot, sizeof(ChanState), cudaMemcpyDeviceToHost));
@@ -1410,6 +1600,8 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
     CK(cudaMemcpy(p, r->d_hist + s.hist_off + (size_t)s.hist_sel * s.hcap, (size_t)s.hcap * 8,
                   cudaMemcpyDeviceToHost));
     p += (size_t)s.hcap * 8;
+    CK(cudaMemcpy(p, r->d_aud + slot, sizeof(AudState), cudaMemcpyDeviceToHost));
+    p += sizeof(AudState);
     if (s.wfm_idx >= 0) {
         size_t w = (size_t)s.wfm_idx;
         CK(cudaMemcpy(p, r->d_comp_dl + w * kWfmHist, kWfmHist * 4, cudaMemcpyDeviceToHost));
@@ -1435,7 +1627,7 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     SnapHeader h;
     std::memcpy(&h, p, sizeof h);
     p += sizeof h;
-    if (h.magic != 0x47505544u || h.D != s.D || h.T != s.T || h.mode != s.spec.mode || h.wfm != (s.wfm_idx >= 0))
+    if (h.magic != 0x47505544u || h.version != 2 || h.D != s.D || h.T != s.T || h.mode != s.spec.mode || h.wfm != (s.wfm_idx >= 0))
         return set_err(r, GPUD_E_STATE, "snapshot geometry mismatch");
     int rc = drain(r);
     if (rc) return rc;
@@ -1445,6 +1637,8 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     s.hist_sel = 0;
     CK(cudaMemcpy(r->d_hist + s.hist_off, p, (size_t)s.hcap * 8, cudaMemcpyHostToDevice));
     p += (size_t)s.hcap * 8;
+    CK(cudaMemcpy(r->d_aud + slot, p, sizeof(AudState), cudaMemcpyHostToDevice));
+    p += sizeof(AudState);
     if (s.wfm_idx >= 0) {
         size_t w = (size_t)s.wfm_idx;
         CK(cudaMemcpy(r->d_comp_dl + w * kWfmHist, p, kWfmHist * 4, cudaMemcpyHostToDevice));
@@ -1461,6 +1655,7 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     s.comp_hist_len = h.comp_hist_len;
     s.has_last = h.has_last != 0;
     s.rds_count = h.rds_count;
+    s.rs_t = h.rs_t;
     if (h.cutoff != s.cutoff) {
         std::vector<float> pm, hh;
         design_taps(r, s, 2 * h.cutoff, pm, hh, &s.cutoff);

@@ -1337,6 +1337,122 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
 }
 
 // ===========================================================================
+// 48 kHz audio back end (recorder/streamer.go:1408-1470, 569-575)
+// ===========================================================================
+// One CTA per channel.  Output o of the block sits at the resampler's phase
+// position t0 + o*M: it is produced after consuming c = floor((t0+o*M)/L)
+// inputs, at arm (t0+o*M) - c*L, over the last K consumed samples (earlier
+// blocks' samples from the carried delay line) -- the closed form of
+// Resampler.Process (dsp/resample.go:105-153); the host mirrors the phase
+// counter, including that method's exits, so every output is independent.
+// The float64 dot products are the reference's (separate multiply and add).
+// De-emphasis y = a*y + (1-a)*x (float64) is a first-order recurrence: each
+// thread runs a contiguous run of outputs, the runs' affine maps are scanned
+// across the CTA, and each run is replayed from its exact start.  Then the
+// WFM gain 0.35 and s16le: int16(clip(s * 32767)), truncating.
+constexpr int kAudThreads = 256;
+
+__global__ void __launch_bounds__(kAudThreads)
+k_audio48(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+          const RsBank *__restrict__ banks, AudState *__restrict__ aud, const float *__restrict__ audio,
+          int16_t *__restrict__ pcm) {
+    __shared__ double s_a[kAudThreads], s_b[2][kAudThreads];
+    __shared__ float s_dl[2][kRsTaps];
+    const SlotBlock sb = sbt[list[blockIdx.x]];
+    const ChanParams &cp = prm[sb.slot];
+    AudState &as = aud[sb.slot];
+    const int C = cp.aud_ch;
+    const int n = sb.rs_frames, nout = sb.rs_nout;
+    if (n <= 0) return;
+    const RsBank &bk = banks[cp.rs_bank];
+    const int L = bk.L, M = bk.M, K = bk.K;
+    const float *in = audio + sb.audio_off;
+    if (threadIdx.x < 2 * kRsTaps) s_dl[threadIdx.x / kRsTaps][threadIdx.x % kRsTaps] = as.dl[threadIdx.x / kRsTaps][threadIdx.x % kRsTaps];
+    __syncthreads();
+    const int per = (nout + kAudThreads - 1) / kAudThreads;
+    const int o0 = min(nout, (int)threadIdx.x * per), o1 = min(nout, o0 + per);
+    const bool wfm = cp.mode == 2 || cp.mode == 3;
+    const double a = cp.deemph_a;
+    // pass 1: this run's de-emphasis map y_end = A*y_start + B per channel
+    double A = 1.0, B[2] = {0.0, 0.0};
+    auto sample = [&](int o, int c) -> float {
+        if (L == M) return in[o * C + c];
+        const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
+        const int64_t cc = T / L;  // T >= 0
+        const int ph = (int)(T - cc * L);
+        const double *arm = bk.arm + ph * K;
+        double acc = 0.0;
+        for (int k = 0; k < K; ++k) {
+            const int64_t i = cc - 1 - k;
+            const float v = i >= 0 ? in[i * C + c] : s_dl[c][-1 - i];
+            acc = __dadd_rn(acc, __dmul_rn((double)v, arm[k]));
+        }
+        return (float)acc;
+    };
+    if (wfm && a > 0.0) {
+        for (int o = o0; o < o1; ++o) {
+            A = __dmul_rn(A, a);
+            for (int c = 0; c < C; ++c)
+                B[c] = __dadd_rn(__dmul_rn(a, B[c]), __dmul_rn(1.0 - a, (double)sample(o, c)));
+        }
+        s_a[threadIdx.x] = A;
+        s_b[0][threadIdx.x] = B[0];
+        s_b[1][threadIdx.x] = B[1];
+        __syncthreads();
+        // inclusive scan of the affine maps (later o applied after earlier)
+        for (int d = 1; d < kAudThreads; d <<= 1) {
+            double pa = 1.0, pb0 = 0.0, pb1 = 0.0;
+            if ((int)threadIdx.x >= d) {
+                pa = s_a[threadIdx.x - d];
+                pb0 = s_b[0][threadIdx.x - d];
+                pb1 = s_b[1][threadIdx.x - d];
+            }
+            __syncthreads();
+            if ((int)threadIdx.x >= d) {
+                const double ca = s_a[threadIdx.x];
+                s_b[0][threadIdx.x] = ca * pb0 + s_b[0][threadIdx.x];
+                s_b[1][threadIdx.x] = ca * pb1 + s_b[1][threadIdx.x];
+                s_a[threadIdx.x] = ca * pa;
+            }
+            __syncthreads();
+        }
+    }
+    // start values of this run: carried state through the runs before it
+    double y[2] = {as.y[0], as.y[1]};
+    if (wfm && a > 0.0 && threadIdx.x > 0) {
+        const double pa = s_a[threadIdx.x - 1];
+        y[0] = pa * as.y[0] + s_b[0][threadIdx.x - 1];
+        y[1] = pa * as.y[1] + s_b[1][threadIdx.x - 1];
+    }
+    for (int o = o0; o < o1; ++o) {
+        for (int c = 0; c < C; ++c) {
+            float s = sample(o, c);
+            if (wfm && a > 0.0) {
+                y[c] = __dadd_rn(__dmul_rn(a, y[c]), __dmul_rn(1.0 - a, (double)s));
+                s = (float)y[c];
+            }
+            if (wfm) s = s * 0.35f;
+            float v = s * 32767.0f;
+            v = fminf(fmaxf(v, -32768.0f), 32767.0f);
+            pcm[sb.pcm_off + o * C + c] = (int16_t)v;
+        }
+    }
+    __syncthreads();
+    // carried state: the last K consumed samples, newest first; the last y
+    if (threadIdx.x < 2 * kRsTaps && L != M) {
+        const int c = threadIdx.x / kRsTaps, k = threadIdx.x % kRsTaps;
+        if (c < C) {
+            const int i = n - 1 - k;
+            as.dl[c][k] = i >= 0 ? in[i * C + c] : s_dl[c][-1 - i];
+        }
+    }
+    if (wfm && a > 0.0 && nout > 0 && o1 == nout && o0 < o1) {
+        as.y[0] = y[0];
+        as.y[1] = y[1];
+    }
+}
+
+// ===========================================================================
 // launch helpers (host)
 // ===========================================================================
 template <int L>
@@ -1439,6 +1555,12 @@ cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, c
                               const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
                               float2 *rds_dl, const BinadeTable *tabs, DevResult *res) {
     k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, comp_dl, rds_dl, tabs, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_audio48(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
+                           const RsBank *banks, AudState *aud, const float *audio, int16_t *pcm) {
+    k_audio48<<<count, kAudThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, pcm);
     return cudaGetLastError();
 }
 

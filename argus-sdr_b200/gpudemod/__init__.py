@@ -24,7 +24,7 @@ DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
 MODE_IQ, MODE_NFM, MODE_WFM, MODE_WFM_STEREO, MODE_AM, MODE_USB, MODE_LSB, MODE_CW = range(8)
 MODE_BY_NAME = {"IQ": MODE_IQ, "NFM": MODE_NFM, "WFM": MODE_WFM, "WFM_STEREO": MODE_WFM_STEREO, "AM": MODE_AM,
                 "USB": MODE_USB, "LSB": MODE_LSB, "CW": MODE_CW}
-CH_EMIT_IQ, CH_RDS = 1, 2
+CH_EMIT_IQ, CH_RDS, CH_AUDIO48K, CH_DEEMPH75, CH_NO_DEEMPH = 1, 2, 4, 8, 16
 SCHED_BATCHED, SCHED_PLAIN = 0, 1
 
 E_ARG, E_DECIM, E_TAPS, E_BUDGET, E_SLOTS, E_SLOT, E_BLOCK, E_TIMEOUT, E_CUDA, E_MODE, E_DEVICE_STATUS, E_STATE = \
@@ -207,7 +207,13 @@ class ChannelRunner:
             buf = (C.c_float * (n * width)).from_address(C.addressof(ptr.contents))
             return np.frombuffer(buf, dtype=np.float32).view(dt).copy()
 
+        pcm = np.zeros(0, np.int16)
+        if payload and res.pcm and res.n_pcm > 0:
+            buf = (C.c_int16 * res.n_pcm).from_address(C.addressof(res.pcm.contents))
+            pcm = np.frombuffer(buf, dtype=np.int16).copy()
         return {
+            "pcm": pcm,
+            "pcm_rate": res.pcm_rate,
             "signal_id": res.signal_id,
             "rate": res.rate,
             "n_iq": res.n_iq,

@@ -54,6 +54,9 @@ class ChannelResult(C.Structure):
         ("rds", C.POINTER(GPUDFloat2)),
         ("pll_path", C.c_int32),
         ("pll_iters", C.c_int32),
+        ("pcm", C.POINTER(C.c_int16)),
+        ("n_pcm", C.c_int32),
+        ("pcm_rate", C.c_int32),
     ]
 
 

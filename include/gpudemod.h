@@ -170,6 +170,15 @@ enum {
 /* channel flags */
 #define GPUD_CH_EMIT_IQ 1 /* copy the extracted IQ back every block */
 #define GPUD_CH_RDS 2     /* WFM modes: produce the 57 kHz RDS baseband */
+/* 48 kHz audio stream (recorder/streamer.go:1408-1470, 569-575): the channel's
+ * audio resampled to 48 kHz by the rational polyphase resampler of
+ * dsp/resample.go (32 taps per arm, Kaiser beta 6), for WFM modes de-emphasised
+ * (one-pole, 50 us unless GPUD_CH_DEEMPH75 / GPUD_CH_NO_DEEMPH) and scaled by
+ * 0.35, encoded as s16le PCM.  With this flag only the PCM comes back to the
+ * host; the demod-rate audio stays in the device arena. */
+#define GPUD_CH_AUDIO48K 4
+#define GPUD_CH_DEEMPH75 8    /* 75 us de-emphasis (US/Japan) */
+#define GPUD_CH_NO_DEEMPH 16  /* no de-emphasis */
 
 /* Schedules for gpud_runner_set_schedule. */
 #define GPUD_SCHED_BATCHED 0 /* one fused launch sequence for all channels (graph-captured) */
@@ -207,10 +216,13 @@ typedef struct {
     float pilot_hz;
     float err_avg;
     const gpud_float2 *iq; /* host; NULL unless GPUD_CH_EMIT_IQ */
-    const float *audio;    /* host */
+    const float *audio;    /* host; NULL with GPUD_CH_AUDIO48K (it stays on the device) */
     const gpud_float2 *rds;
     int32_t pll_path;      /* WFM_STEREO: 1 parallel-in-time PLL solver, 2 serial loop */
     int32_t pll_iters;     /* Newton iterations of the last parallel solve */
+    const int16_t *pcm;    /* GPUD_CH_AUDIO48K: s16le samples, interleaved per audio channel */
+    int32_t n_pcm;         /* int16 samples in pcm (frames x audio_channels) */
+    int32_t pcm_rate;      /* 48000 with GPUD_CH_AUDIO48K, else 0 */
 } gpud_channel_result;
 
 /* Runner statistics. */

@@ -1148,3 +1148,190 @@ void or_channel_stereo_margins(const or_channel *ch, double *coherence, double *
 }
 
 void or_channel_set_offset(or_channel *ch, double offset_hz) { ch->offset_hz = offset_hz; }
+
+/* ------------------------------------------------------------------------ */
+/* Audio back end: internal/dsp/resample.go:45-232 (rational polyphase        */
+/* resampler), recorder/streamer.go:1408-1470 (48 kHz resample, de-emphasis,  */
+/* x0.35 for WFM) and :569-575 with wavwriter.go:77-85 (s16le encoding).      */
+/* ------------------------------------------------------------------------ */
+
+static int or_gcd(int a, int b) {
+    while (b != 0) {
+        int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a < 0 ? -a : a;
+}
+
+/* resample.go bessel0: series until the term drops below 1e-12 of the sum. */
+static double or_bessel0(double x) {
+    double sum = 1.0, term = 1.0;
+    for (int k = 1; k < 30; k++) {
+        term *= (x / (2 * (double)k)) * (x / (2 * (double)k));
+        sum += term;
+        if (term < 1e-12 * sum) break;
+    }
+    return sum;
+}
+
+#define OR_RS_MAXL 512
+#define OR_RS_MAXK 40
+typedef struct {
+    int l, m, taps; /* upsample L, downsample M, taps per arm */
+    double bank[OR_RS_MAXL * OR_RS_MAXK]; /* bank[p*taps + t] */
+    double delay[OR_RS_MAXK];             /* delay[0] newest */
+    int out_time;
+} or_resampler;
+
+size_t or_resampler_size(void) { return sizeof(or_resampler); }
+
+/* NewResampler (resample.go:45-93): L/M from the gcd, prototype of odd length
+ * L*tapsPerPhase(+1), windowed sinc fc = 0.90/max(L,M) with Kaiser beta 6 and
+ * gain L, split into L arms of ceil(len/L) taps.  Returns 0, or -1 when the
+ * bank does not fit. */
+int or_resampler_init(or_resampler *r, int in_rate, int out_rate, int taps_per_phase) {
+    memset(r, 0, sizeof *r);
+    if (in_rate <= 0 || out_rate <= 0) in_rate = out_rate = 1;
+    if (taps_per_phase < 4) taps_per_phase = 4;
+    int g = or_gcd(in_rate, out_rate);
+    int l = out_rate / g, m = in_rate / g;
+    int plen = l * taps_per_phase;
+    if (plen % 2 == 0) plen++;
+    int k = (plen + l - 1) / l;
+    if (l > OR_RS_MAXL || k > OR_RS_MAXK) return -1;
+    double fc = 0.90 / (double)(l > m ? l : m);
+    double mid = (double)(plen - 1) / 2.0;
+    double b0 = or_bessel0(6.0);
+    for (int p = 0; p < l; p++)
+        for (int t = 0; t < k; t++) {
+            int n = p + t * l;
+            double v = 0.0;
+            if (n < plen) {
+                double x = (double)n - mid;
+                double s = fabs(x) < 1e-12 ? 2 * OR_PI * fc : sin(2 * OR_PI * fc * x) / x;
+                double xx = ((double)n - mid) / mid;
+                double w = or_bessel0(6.0 * sqrt(1 - xx * xx)) / b0;
+                v = s * w * (double)l;
+            }
+            r->bank[p * k + t] = v;
+        }
+    r->l = l;
+    r->m = m;
+    r->taps = k;
+    return 0;
+}
+
+void or_resampler_ratio(const or_resampler *r, int *l, int *m, int *taps, int *out_time) {
+    *l = r->l;
+    *m = r->m;
+    *taps = r->taps;
+    *out_time = r->out_time;
+}
+
+void or_resampler_bank(const or_resampler *r, double *out) {
+    memcpy(out, r->bank, sizeof(double) * (size_t)(r->l * r->taps));
+}
+
+/* Resampler.Process (resample.go:105-153), including its exits: when the input
+ * runs out inside the consume loop the phase counter has already been reduced
+ * by L for the sample it could not consume.  Returns the output count. */
+int or_resampler_process(or_resampler *r, const float *in, int n, float *out) {
+    if (n == 0) return 0;
+    if (r->l == r->m) {
+        memcpy(out, in, sizeof(float) * (size_t)n);
+        return n;
+    }
+    int L = r->l, M = r->m, K = r->taps;
+    int pos = 0, t = r->out_time, nout = 0;
+    while (pos < n) {
+        while (t >= L) {
+            t -= L;
+            if (pos >= n) {
+                r->out_time = t;
+                return nout;
+            }
+            memmove(r->delay + 1, r->delay, sizeof(double) * (size_t)(K - 1));
+            r->delay[0] = (double)in[pos++];
+        }
+        const double *arm = r->bank + t * K;
+        double acc = 0;
+        for (int k = 0; k < K; k++) acc += r->delay[k] * arm[k];
+        out[nout++] = (float)acc;
+        t += M;
+    }
+    r->out_time = t;
+    return nout;
+}
+
+/* The 48 kHz back end of one channel: a resampler per audio channel
+ * (StereoResampler for 2), then for WFM modes the one-pole de-emphasis
+ * y = a*y + (1-a)*x, a = exp(-1/(48000*tau)) in float64 per channel and the
+ * x0.35 gain, then s16le: int16(clip(s*32767)) with Go's truncating
+ * conversion. */
+typedef struct {
+    int channels, wfm;
+    double deemph_us, y[2];
+    or_resampler rs[2];
+} or_audio48;
+
+size_t or_audio48_size(void) { return sizeof(or_audio48); }
+
+int or_audio48_init(or_audio48 *a, int in_rate, int channels, int wfm, double deemph_us) {
+    memset(a, 0, sizeof *a);
+    a->channels = channels;
+    a->wfm = wfm;
+    a->deemph_us = deemph_us;
+    for (int c = 0; c < channels; c++)
+        if (or_resampler_init(&a->rs[c], in_rate, 48000, 32) != 0) return -1;
+    return 0;
+}
+
+/* in: frames x channels interleaved at the demod rate.  Writes interleaved
+ * float audio (out_f, may be NULL) and s16le samples; returns the sample
+ * count (frames x channels). */
+int or_audio48_process(or_audio48 *a, const float *in, int frames, float *out_f, int16_t *pcm) {
+    int C = a->channels;
+    /* per-channel output capacity: frames * L / M plus the phase slack */
+    size_t cap = (size_t)((double)frames * (double)a->rs[0].l / (double)a->rs[0].m) + (size_t)frames / 1000 + 64;
+    float *tmp = (float *)malloc(sizeof(float) * (size_t)(frames + 8));
+    float *res = (float *)malloc(sizeof(float) * (size_t)C * cap);
+    int nf = -1;
+    float *outs[2] = {NULL, NULL};
+    int cnt[2] = {0, 0};
+    for (int c = 0; c < C; c++) {
+        for (int i = 0; i < frames; i++) tmp[i] = in[i * C + c];
+        outs[c] = res + (size_t)c * cap;
+        cnt[c] = or_resampler_process(&a->rs[c], tmp, frames, outs[c]);
+        if (nf < 0 || cnt[c] < nf) nf = cnt[c];
+    }
+    if (nf < 0) nf = 0;
+    float *audio = (float *)malloc(sizeof(float) * (size_t)(nf * C + 1));
+    for (int i = 0; i < nf; i++)
+        for (int c = 0; c < C; c++) audio[i * C + c] = outs[c][i];
+    if (a->wfm && a->deemph_us > 0) {
+        double tau = a->deemph_us * 1e-6;
+        double al = exp(-1.0 / (48000.0 * tau));
+        for (int c = 0; c < C; c++) {
+            double y = a->y[c];
+            for (int i = 0; i < nf; i++) {
+                y = al * y + (1 - al) * (double)audio[i * C + c];
+                audio[i * C + c] = (float)y;
+            }
+            a->y[c] = y;
+        }
+    }
+    if (a->wfm)
+        for (int i = 0; i < nf * C; i++) audio[i] *= 0.35f;
+    for (int i = 0; i < nf * C; i++) {
+        float v = audio[i] * 32767.0f;
+        if (v > 32767.0f) v = 32767.0f;
+        if (v < -32768.0f) v = -32768.0f;
+        pcm[i] = (int16_t)v; /* truncation toward zero, as Go's conversion */
+        if (out_f) out_f[i] = audio[i];
+    }
+    free(tmp);
+    free(res);
+    free(audio);
+    return nf * C;
+}

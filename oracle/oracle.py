@@ -70,6 +70,14 @@ def _load() -> C.CDLL:
         "or_channel_state": (None, [P, P, P, P]),
         "or_channel_stereo_margins": (None, [P, P, P, P]),
         "or_channel_set_offset": (None, [P, d]),
+        "or_resampler_size": (C.c_size_t, []),
+        "or_resampler_init": (i, [P, i, i, i]),
+        "or_resampler_ratio": (None, [P, P, P, P, P]),
+        "or_resampler_bank": (None, [P, P]),
+        "or_resampler_process": (i, [P, P, i, P]),
+        "or_audio48_size": (C.c_size_t, []),
+        "or_audio48_init": (i, [P, i, i, i, d]),
+        "or_audio48_process": (i, [P, P, i, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -420,3 +428,53 @@ class OracleChannel:
 
     def set_offset(self, offset_hz):
         _lib.or_channel_set_offset(self._buf, float(offset_hz))
+
+
+class Resampler:
+    """dsp.Resampler (internal/dsp/resample.go:45-153): rational polyphase
+    resampler, stateful across Process calls."""
+
+    def __init__(self, in_rate: int, out_rate: int, taps_per_phase: int = 32):
+        self._buf = C.create_string_buffer(_lib.or_resampler_size())
+        if _lib.or_resampler_init(self._buf, int(in_rate), int(out_rate), int(taps_per_phase)) != 0:
+            raise ValueError("resampler bank too large")
+
+    def ratio(self):
+        l, m, k, t = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _lib.or_resampler_ratio(self._buf, C.byref(l), C.byref(m), C.byref(k), C.byref(t))
+        return l.value, m.value, k.value, t.value
+
+    def bank(self) -> np.ndarray:
+        l, _, k, _ = self.ratio()
+        out = np.zeros(l * k, np.float64)
+        _lib.or_resampler_bank(self._buf, _p(out))
+        return out.reshape(l, k)
+
+    def process(self, x) -> np.ndarray:
+        x = _f32(x)
+        l, m, _, _ = self.ratio()
+        out = np.zeros(int(x.size * l / m) + 8, np.float32)
+        n = _lib.or_resampler_process(self._buf, _p(x), x.size, _p(out))
+        return out[:n].copy()
+
+
+class Audio48:
+    """48 kHz audio back end of one channel (recorder/streamer.go:1408-1470,
+    569-575): resample each audio channel to 48 kHz, de-emphasis and x0.35 for
+    WFM, s16le encoding."""
+
+    def __init__(self, in_rate: int, channels: int, wfm: bool, deemph_us: float = 50.0):
+        self.channels = channels
+        self.ratio = 48000.0 / in_rate
+        self._buf = C.create_string_buffer(_lib.or_audio48_size())
+        if _lib.or_audio48_init(self._buf, int(in_rate), int(channels), 1 if wfm else 0, float(deemph_us)) != 0:
+            raise ValueError("resampler bank too large")
+
+    def process(self, audio):
+        a = _f32(audio)
+        frames = a.size // self.channels
+        cap = self.channels * (int(frames * self.ratio) + frames // 1000 + 64)
+        f = np.zeros(cap, np.float32)
+        pcm = np.zeros(cap, np.int16)
+        n = _lib.or_audio48_process(self._buf, _p(a), frames, _p(f), _p(pcm))
+        return f[:n].copy(), pcm[:n].copy()

@@ -1,0 +1,114 @@
+"""48 kHz audio back end on the GPU (GPUD_CH_AUDIO48K) against the oracle:
+the channel chain's audio through dsp.Resampler (32 taps per arm), WFM
+de-emphasis and gain, s16le encoding (recorder/streamer.go:1408-1470,
+569-575)."""
+import numpy as np
+import pytest
+
+import gpudemod as G
+from gpudemod import synth
+from oracle import oracle as O
+from signals import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(g, w_pcm, ctx):
+    assert g["pcm_rate"] == 48000, ctx
+    assert g["pcm"].size == w_pcm.size, (ctx, g["pcm"].size, w_pcm.size)
+    if w_pcm.size:
+        d = np.abs(g["pcm"].astype(np.int32) - w_pcm.astype(np.int32))
+        assert d.max() <= 1, (ctx, int(d.max()))  # one LSB: float32 rounding at the truncation edge
+        assert rel_l2(g["pcm"].astype(np.float64), w_pcm.astype(np.float64)) <= 1e-4, ctx
+
+
+def test_wfm_stereo_pcm_matches_oracle(cuda):
+    scene, _ = synth.plain_wfm_scene(block=262_144)
+    fs, rate = 2_400_000, 300_000
+    r = G.ChannelRunner(fs, 262_144, max_channels=2)
+    flags = G.CH_RDS | G.CH_AUDIO48K
+    slot = r.admit(1, 300_000.0, 250_000.0, rate, 128, G.MODE_WFM_STEREO, flags)
+    oc = O.OracleChannel(fs, 300_000.0, 250_000.0, rate, 128, O.MODE_WFM_STEREO, rds=True)
+    back = O.Audio48(rate, 2, wfm=True, deemph_us=50.0)
+    try:
+        for b in range(8):
+            x = scene.next_block().numpy()
+            r.process_block(x)
+            g = r.result(slot)
+            w = oc.process(x)
+            _, w_pcm = back.process(w["audio"])
+            assert g["audio"].size == 0  # the demod-rate audio stays on the device
+            assert rel_l2(g["rds"], w["rds"]) <= 1e-5
+            _check(g, w_pcm, b)
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("mode,kind,flags", [
+    (G.MODE_NFM, "NFM", 0), (G.MODE_AM, "AM", 0), (G.MODE_USB, "USB", 0), (G.MODE_CW, "CW", 0),
+    (G.MODE_WFM, "WFM", G.CH_DEEMPH75), (G.MODE_WFM_STEREO, "WFM", G.CH_NO_DEEMPH)])
+def test_narrow_and_wfm_pcm_matches_oracle(cuda, mode, kind, flags):
+    fs, block = 10_000_000, 1 << 20
+    if kind == "WFM":
+        scene, st = synth.fm_band_scene(device="cuda", block=block, n_stations=40, seconds=4.0)
+        off, (rate, taps, bw) = st[3].offset_hz, synth.MODE_TABLE["WFM"]
+    else:
+        scene, chans = synth.mixed_scene(device="cuda", block=block)
+        off = next(o for k, o in chans if k == kind)
+        rate, taps, bw = synth.MODE_TABLE[kind]
+    r = G.ChannelRunner(fs, block, max_channels=2)
+    slot = r.admit(2, off, bw, rate, taps, mode, flags | G.CH_AUDIO48K)
+    oc = O.OracleChannel(fs, off, bw, rate, taps, mode, rds=False)
+    tau = 0.0 if flags & G.CH_NO_DEEMPH else (75.0 if flags & G.CH_DEEMPH75 else 50.0)
+    back = O.Audio48(rate, 2 if mode == G.MODE_WFM_STEREO else 1, wfm=(kind == "WFM"), deemph_us=tau)
+    try:
+        for b in range(3):
+            x = scene.next_block().cpu().numpy()
+            # odd block lengths move the resampler phase across calls
+            x = x[: block - 4097 * b]
+            r.process_block(x)
+            w = oc.process(x)
+            _, w_pcm = back.process(w["audio"])
+            _check(r.result(slot), w_pcm, (kind, b))
+    finally:
+        r.close()
+
+
+def test_pcm_snapshot_restore_and_pipelined(cuda):
+    """The back end's state (resampler delay lines and phase counter,
+    de-emphasis) moves with a snapshot, and three blocks in flight give the
+    same PCM as one at a time."""
+    scene, _ = synth.plain_wfm_scene(block=262_144)
+    blocks = [scene.next_block().numpy() for _ in range(6)]
+    spec = (1, 300_000.0, 250_000.0, 300_000, 128, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_AUDIO48K)
+    ra = G.ChannelRunner(2_400_000, 262_144, max_channels=2)
+    rb = G.ChannelRunner(2_400_000, 262_144, max_channels=2)
+    rp = G.ChannelRunner(2_400_000, 262_144, max_channels=2)
+    sa, sp = ra.admit(*spec), rp.admit(*spec)
+    try:
+        seq = []
+        for k, x in enumerate(blocks):
+            ra.process_block(x)
+            seq.append(ra.result(sa)["pcm"])
+            if k == 2:
+                blob = ra.snapshot(sa)
+                sb = rb.admit(*spec)
+                rb.restore(sb, blob)
+            if k >= 3:
+                rb.process_block(x)
+                assert np.array_equal(rb.result(sb)["pcm"], seq[k])
+        tickets, got = [], []
+        for k, x in enumerate(blocks):
+            tickets.append(rp.submit(x))
+            if k >= 2:
+                rp.wait(tickets[k - 2])
+                got.append(rp.result(sp)["pcm"])
+        for t in tickets[-2:]:
+            rp.wait(t)
+            got.append(rp.result(sp)["pcm"])
+        for a, b in zip(seq, got):
+            assert np.array_equal(a, b)
+    finally:
+        ra.close()
+        rb.close()
+        rp.close()

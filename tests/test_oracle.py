@@ -260,3 +260,104 @@ def test_truth64_chain_agrees_with_oracle():
             d = np.linalg.norm(a[key] - b[key]) / np.linalg.norm(b[key])
             assert d < 2e-6, (key, d)
         assert a["locked"] == b["locked"]
+
+
+# --- 48 kHz audio back end: the reference's resample_test.go cases ----------
+
+def test_resampler_ratio_kat():
+    # TestResamplerRatio (resample_test.go:26-44) and the gcd cases (:8-24)
+    for inr, outr, l, m in [(51200, 48000, 15, 16), (44100, 48000, 160, 147), (48000, 48000, 1, 1),
+                            (96000, 48000, 1, 2), (312500, 48000, 96, 625), (300000, 48000, 4, 25)]:
+        assert O.Resampler(inr, outr).ratio()[:2] == (l, m)
+    assert math.gcd(48000, 200000) == 8000  # gcd KAT restated by the ratio above
+
+
+def test_resampler_identity_and_output_length():
+    # TestResamplerIdentity (:46-62)
+    x = np.sin(2 * np.pi * 440 * np.arange(1000) / 48000).astype(np.float32)
+    y = O.Resampler(48000, 48000).process(x)
+    assert y.size == x.size and np.max(np.abs(y - x)) <= 1e-4
+    # TestResamplerOutputLength (:64-88)
+    for inr, outr, n in [(51200, 48000, 5120), (51200, 48000, 10240), (44100, 48000, 4410),
+                         (96000, 48000, 9600), (200000, 48000, 20000), (312500, 48000, 32768)]:
+        x = np.sin(2 * np.pi * 1000 * np.arange(n) / inr).astype(np.float32)
+        y = O.Resampler(inr, outr).process(x)
+        assert abs(y.size - n * outr / inr) <= 3
+
+
+def test_resampler_stream_continuity():
+    # TestResamplerStreamContinuity (:90-165): M-aligned chunks bit-exact,
+    # arbitrary chunks within one sample per chunk
+    inr, outr = 51200, 48000
+    sig = np.sin(2 * np.pi * 1000 * np.arange(inr) / inr).astype(np.float32)
+    one = O.Resampler(inr, outr).process(sig)
+    r2 = O.Resampler(inr, outr)
+    aligned = np.concatenate([r2.process(sig[i:i + 3200]) for i in range(0, sig.size, 3200)])
+    assert np.array_equal(one, aligned)
+    r3 = O.Resampler(inr, outr)
+    ch = inr // 15
+    arb = np.concatenate([r3.process(sig[i:i + ch]) for i in range(0, sig.size, ch)])
+    assert abs(arb.size - one.size) <= (sig.size + ch - 1) // ch
+
+
+def test_resampler_tone_and_stereo():
+    # TestResamplerTonePreservation (:176-202)
+    inr, outr = 51200, 48000
+    x = np.sin(2 * np.pi * 1000 * np.arange(inr) / inr).astype(np.float32)
+    y = O.Resampler(inr, outr).process(x)
+    z = y[101:]
+    crossings = np.count_nonzero((z[:-1] <= 0) & (z[1:] > 0) | (z[:-1] >= 0) & (z[1:] < 0))
+    assert abs(crossings / 2.0 * outr / (y.size - 101) - 1000) <= 10
+    # TestStereoResampler (:204-235) through the stereo back end (no de-emphasis)
+    n = inr // 2
+    st = np.empty(2 * n, np.float32)
+    st[0::2] = np.sin(2 * np.pi * 440 * np.arange(n) / inr)
+    st[1::2] = np.sin(2 * np.pi * 880 * np.arange(n) / inr)
+    f, pcm = O.Audio48(inr, 2, wfm=False).process(st)
+    assert abs(f.size // 2 - n * outr / inr) <= 3
+    assert np.sum(np.abs(f[100:200:2])) > 0.1 and np.sum(np.abs(f[101:201:2])) > 0.1
+    # s16le: int16(clip(s * 32767)), truncating
+    assert np.array_equal(pcm, np.clip(f * np.float32(32767), -32768, 32767).astype(np.int16))
+
+
+def test_audio48_deemphasis_and_gain():
+    # WFM: de-emphasis y = a y + (1-a) x (tau 50 us at 48 kHz) then x0.35
+    inr = 312_500
+    x = (0.5 * np.sin(2 * np.pi * 1000 * np.arange(32768) / inr)).astype(np.float32)
+    plain = O.Resampler(inr, 48000).process(x)
+    f, _ = O.Audio48(inr, 1, wfm=True, deemph_us=50.0).process(x)
+    a = math.exp(-1.0 / (48000 * 50e-6))
+    y, ref = 0.0, np.empty(plain.size, np.float32)
+    for i, v in enumerate(plain):
+        y = a * y + (1 - a) * float(v)
+        ref[i] = np.float32(y)
+    assert np.array_equal(f, ref * np.float32(0.35))
+
+
+def _rs_advance(L, M, t0, n):
+    """The closed form the runner's host mirror uses for Resampler.Process:
+    frames produced and the phase counter after n inputs from counter t0."""
+    if n <= 0:
+        return 0, t0
+    if L == M:
+        return n, t0
+    cdiv = lambda a, b: -((-a) // b)
+    A = cdiv((n + 1) * L - t0, M) - 1
+    last = -1 if A < 0 else max(0, min(A, cdiv(n * L - t0, M)))
+    c_last = (t0 + last * M) // L if last >= 0 else 0
+    return last + 1, t0 + (last + 1) * M - n * L - (L if c_last < n else 0)
+
+
+@pytest.mark.parametrize("in_rate", [312_500, 300_000, 25_000, 12_500, 5_000, 51_200, 44_100])
+def test_resampler_closed_form_counts(in_rate):
+    """The per-call output count and phase counter of Resampler.Process,
+    including its exit inside the consume loop, follow the closed form for
+    every chunk length (so each 48 kHz output can be computed independently)."""
+    rng = np.random.default_rng(in_rate)
+    r = O.Resampler(in_rate, 48000)
+    L, M, _, t = r.ratio()
+    for n in list(rng.integers(0, 9000, 40)) + [1, 2, 3, M, L, 32768]:
+        got = r.process(rng.standard_normal(int(n)).astype(np.float32)).size
+        want, t_next = _rs_advance(L, M, t, int(n))
+        t = r.ratio()[3]
+        assert (got, t) == (want, t_next), (n, got, want, t, t_next)
