@@ -63,8 +63,10 @@ cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, c
                               float2 *rds_dl, const BinadeTable *tabs, DevResult *res);
 cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res);
-cudaError_t launch_audio48(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                           const RsBank *banks, AudState *aud, const float *audio, int16_t *pcm);
+cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *work, const int *list,
+                           const SlotBlock *sbt, const ChanParams *prm, const RsBank *banks, AudState *aud,
+                           const float *audio, float *rs_buf, int16_t *pcm);
+int audio48_tile();
 int rds_smem_bytes(int dr);
 int dense_smem_bytes_host(int P, int L);
 int wide_smem_bytes_host(int T);
@@ -189,6 +191,7 @@ struct BlockPlan {
     int rds_smem = 0;
     std::vector<int> pll_list;
     std::vector<int> aud_list;  // entries with a 48 kHz back end and input this block
+    std::vector<int2> w_aud;    // (entry, tile) of the 48 kHz resampler
     int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_audio_host = 0, tot_rds = 0,
             tot_pcm = 0;
 };
@@ -218,6 +221,8 @@ struct Frame {
     int64_t wk_cap = 0;
     float2 *d_block = nullptr;
     float2 *h_in = nullptr;
+    float *d_rs = nullptr;  // resampled 48 kHz audio before de-emphasis
+    int64_t rs_cap = 0;
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
@@ -692,6 +697,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             if (pass == 0) pl.tot_audio_host = audio;
         }
     pl.aud_list.clear();
+    pl.w_aud.clear();
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         SlotBlock &sb = pl.sbs[(size_t)i];
         Slot &s = r->slots[(size_t)sb.slot];
@@ -701,7 +707,10 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         rds += (sb.n_rds + 1) & ~1;
         sb.pcm_off = (int)pcm;
         pcm += ((int64_t)sb.rs_nout * s.aud_ch + 7) & ~7;
-        if (sb.rs_frames > 0) pl.aud_list.push_back(i);
+        if (sb.rs_frames > 0) {
+            pl.aud_list.push_back(i);
+            for (int t = 0; t * audio48_tile() < sb.rs_nout; ++t) pl.w_aud.push_back(make_int2(i, t));
+        }
     }
     pl.tot_comp = comp;
     pl.tot_audio = audio;
@@ -760,6 +769,13 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         f.wk_cap = cap;
         r->graph_rebuilds++;
     }
+    if (pl.tot_pcm > f.rs_cap) {
+        cudaFree(f.d_rs);
+        f.d_rs = nullptr;
+        int64_t cap = std::max<int64_t>(pl.tot_pcm * 5 / 4, 1 << 14);
+        CK(dalloc(&f.d_rs, (size_t)cap));
+        f.rs_cap = cap;
+    }
     size_t res = align256(pl.sbs.size() * sizeof(DevResult));
     size_t need = res + align256((size_t)pl.tot_pcm * 2) + align256((size_t)pl.tot_audio * 4) +
                   align256((size_t)pl.tot_rds * 8) + align256((size_t)pl.tot_ext * 8);
@@ -777,7 +793,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
-          pl.w_rds.size();
+          pl.w_rds.size() + pl.w_aud.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
@@ -871,7 +887,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         return at;
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
-           o_out = put(pl.w_out), o_rds = put(pl.w_rds);
+           o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
@@ -969,9 +985,9 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     }
     if (!pl.aud_list.empty()) {
         prof_mark(r, f, "audio48k");
-        CK(launch_audio48((int)pl.aud_list.size(), f.s, d_aud_list, d_sb, r->d_prm, r->d_banks, r->d_aud, d_audio,
-                          d_pcm));
-        nl++;
+        CK(launch_audio48((int)pl.w_aud.size(), (int)pl.aud_list.size(), f.s, d_w + o_waud, d_aud_list, d_sb,
+                          r->d_prm, r->d_banks, r->d_aud, d_audio, f.d_rs, d_pcm));
+        nl += pl.w_aud.empty() ? 1 : 2;
     }
     if (!pl.sbs.empty()) {
         prof_mark(r, f, "post_back");
@@ -1237,6 +1253,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_out);
         cudaFree(f.d_wk);
         cudaFree(f.d_block);
+        cudaFree(f.d_rs);
         if (f.h_desc) cudaFreeHost(f.h_desc);
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);

@@ -1339,25 +1339,63 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
 // ===========================================================================
 // 48 kHz audio back end (recorder/streamer.go:1408-1470, 569-575)
 // ===========================================================================
-// One CTA per channel.  Output o of the block sits at the resampler's phase
-// position t0 + o*M: it is produced after consuming c = floor((t0+o*M)/L)
-// inputs, at arm (t0+o*M) - c*L, over the last K consumed samples (earlier
-// blocks' samples from the carried delay line) -- the closed form of
+// Resampling: output o of the block sits at the resampler's phase position
+// t0 + o*M: it is produced after consuming c = floor((t0+o*M)/L) inputs, at
+// arm (t0+o*M) - c*L, over the last K consumed samples (earlier blocks'
+// samples from the carried delay line) -- the closed form of
 // Resampler.Process (dsp/resample.go:105-153); the host mirrors the phase
-// counter, including that method's exits, so every output is independent.
-// The float64 dot products are the reference's (separate multiply and add).
-// De-emphasis y = a*y + (1-a)*x (float64) is a first-order recurrence: each
-// thread runs a contiguous run of outputs, the runs' affine maps are scanned
-// across the CTA, and each run is replayed from its exact start.  Then the
-// WFM gain 0.35 and s16le: int16(clip(s * 32767)), truncating.
+// counter, including that method's exits, so every output is independent and
+// k_audio48_rs computes one per thread over the whole grid.  The float64 dot
+// products keep the reference's separate multiply and add.
+// k_audio48_out, one CTA per channel: de-emphasis y = a*y + (1-a)*x (float64),
+// a first-order recurrence -- each thread takes a contiguous run of outputs,
+// the runs' affine maps are scanned across the CTA and each run is replayed
+// from its start -- then the WFM gain 0.35 and s16le: int16(clip(s * 32767)),
+// truncating; it also carries the delay lines and the de-emphasis state.
 constexpr int kAudThreads = 256;
+constexpr int kAudOT = 256;  // resampled frames per CTA in k_audio48_rs
 
 __global__ void __launch_bounds__(kAudThreads)
-k_audio48(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
-          const RsBank *__restrict__ banks, AudState *__restrict__ aud, const float *__restrict__ audio,
-          int16_t *__restrict__ pcm) {
+k_audio48_rs(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+             const RsBank *__restrict__ banks, const AudState *__restrict__ aud, const float *__restrict__ audio,
+             float *__restrict__ rs_out) {
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int o = w.y * kAudOT + (int)threadIdx.x;
+    if (o >= sb.rs_nout) return;
+    const ChanParams &cp = prm[sb.slot];
+    const AudState &as = aud[sb.slot];
+    const RsBank &bk = banks[cp.rs_bank];
+    const int C = cp.aud_ch, L = bk.L, M = bk.M, K = bk.K;
+    const float *in = audio + sb.audio_off;
+    float *dst = rs_out + sb.pcm_off + o * C;
+    if (L == M) {
+        for (int c = 0; c < C; ++c) dst[c] = in[o * C + c];
+        return;
+    }
+    const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
+    const int64_t cc = T / L;  // T >= 0
+    const double *arm = bk.arm + (int)(T - cc * L) * K;
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const int64_t i = cc - 1 - k;
+        const double h = arm[k];
+        const float v0 = i >= 0 ? in[i * C] : as.dl[0][-1 - i];
+        acc0 = __dadd_rn(acc0, __dmul_rn((double)v0, h));
+        if (C == 2) {
+            const float v1 = i >= 0 ? in[i * 2 + 1] : as.dl[1][-1 - i];
+            acc1 = __dadd_rn(acc1, __dmul_rn((double)v1, h));
+        }
+    }
+    dst[0] = (float)acc0;
+    if (C == 2) dst[1] = (float)acc1;
+}
+
+__global__ void __launch_bounds__(kAudThreads)
+k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+              const RsBank *__restrict__ banks, AudState *__restrict__ aud, const float *__restrict__ audio,
+              const float *__restrict__ rs_out, int16_t *__restrict__ pcm) {
     __shared__ double s_a[kAudThreads], s_b[2][kAudThreads];
-    __shared__ float s_dl[2][kRsTaps];
     const SlotBlock sb = sbt[list[blockIdx.x]];
     const ChanParams &cp = prm[sb.slot];
     AudState &as = aud[sb.slot];
@@ -1365,50 +1403,36 @@ k_audio48(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const
     const int n = sb.rs_frames, nout = sb.rs_nout;
     if (n <= 0) return;
     const RsBank &bk = banks[cp.rs_bank];
-    const int L = bk.L, M = bk.M, K = bk.K;
-    const float *in = audio + sb.audio_off;
-    if (threadIdx.x < 2 * kRsTaps) s_dl[threadIdx.x / kRsTaps][threadIdx.x % kRsTaps] = as.dl[threadIdx.x / kRsTaps][threadIdx.x % kRsTaps];
-    __syncthreads();
+    const float *r = rs_out + sb.pcm_off;
     const int per = (nout + kAudThreads - 1) / kAudThreads;
     const int o0 = min(nout, (int)threadIdx.x * per), o1 = min(nout, o0 + per);
     const bool wfm = cp.mode == 2 || cp.mode == 3;
     const double a = cp.deemph_a;
-    // pass 1: this run's de-emphasis map y_end = A*y_start + B per channel
-    double A = 1.0, B[2] = {0.0, 0.0};
-    auto sample = [&](int o, int c) -> float {
-        if (L == M) return in[o * C + c];
-        const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
-        const int64_t cc = T / L;  // T >= 0
-        const int ph = (int)(T - cc * L);
-        const double *arm = bk.arm + ph * K;
-        double acc = 0.0;
-        for (int k = 0; k < K; ++k) {
-            const int64_t i = cc - 1 - k;
-            const float v = i >= 0 ? in[i * C + c] : s_dl[c][-1 - i];
-            acc = __dadd_rn(acc, __dmul_rn((double)v, arm[k]));
-        }
-        return (float)acc;
-    };
-    if (wfm && a > 0.0) {
+    const bool de = wfm && a > 0.0;
+    double y0 = as.y[0], y1 = as.y[1];
+    if (de) {
+        // this run's map y_end = A*y_start + B, per channel
+        double A = 1.0, B0 = 0.0, B1 = 0.0;
         for (int o = o0; o < o1; ++o) {
             A = __dmul_rn(A, a);
-            for (int c = 0; c < C; ++c)
-                B[c] = __dadd_rn(__dmul_rn(a, B[c]), __dmul_rn(1.0 - a, (double)sample(o, c)));
+            B0 = __dadd_rn(__dmul_rn(a, B0), __dmul_rn(1.0 - a, (double)r[o * C]));
+            if (C == 2) B1 = __dadd_rn(__dmul_rn(a, B1), __dmul_rn(1.0 - a, (double)r[o * 2 + 1]));
         }
         s_a[threadIdx.x] = A;
-        s_b[0][threadIdx.x] = B[0];
-        s_b[1][threadIdx.x] = B[1];
+        s_b[0][threadIdx.x] = B0;
+        s_b[1][threadIdx.x] = B1;
         __syncthreads();
-        // inclusive scan of the affine maps (later o applied after earlier)
+        // inclusive scan of the maps (a later run applied after an earlier one)
         for (int d = 1; d < kAudThreads; d <<= 1) {
             double pa = 1.0, pb0 = 0.0, pb1 = 0.0;
-            if ((int)threadIdx.x >= d) {
+            const bool take = (int)threadIdx.x >= d;
+            if (take) {
                 pa = s_a[threadIdx.x - d];
                 pb0 = s_b[0][threadIdx.x - d];
                 pb1 = s_b[1][threadIdx.x - d];
             }
             __syncthreads();
-            if ((int)threadIdx.x >= d) {
+            if (take) {
                 const double ca = s_a[threadIdx.x];
                 s_b[0][threadIdx.x] = ca * pb0 + s_b[0][threadIdx.x];
                 s_b[1][threadIdx.x] = ca * pb1 + s_b[1][threadIdx.x];
@@ -1416,20 +1440,19 @@ k_audio48(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const
             }
             __syncthreads();
         }
-    }
-    // start values of this run: carried state through the runs before it
-    double y[2] = {as.y[0], as.y[1]};
-    if (wfm && a > 0.0 && threadIdx.x > 0) {
-        const double pa = s_a[threadIdx.x - 1];
-        y[0] = pa * as.y[0] + s_b[0][threadIdx.x - 1];
-        y[1] = pa * as.y[1] + s_b[1][threadIdx.x - 1];
+        if (threadIdx.x > 0) {
+            const double pa = s_a[threadIdx.x - 1];
+            y0 = pa * as.y[0] + s_b[0][threadIdx.x - 1];
+            y1 = pa * as.y[1] + s_b[1][threadIdx.x - 1];
+        }
     }
     for (int o = o0; o < o1; ++o) {
         for (int c = 0; c < C; ++c) {
-            float s = sample(o, c);
-            if (wfm && a > 0.0) {
-                y[c] = __dadd_rn(__dmul_rn(a, y[c]), __dmul_rn(1.0 - a, (double)s));
-                s = (float)y[c];
+            float s = r[o * C + c];
+            if (de) {
+                double &y = c == 0 ? y0 : y1;
+                y = __dadd_rn(__dmul_rn(a, y), __dmul_rn(1.0 - a, (double)s));
+                s = (float)y;
             }
             if (wfm) s = s * 0.35f;
             float v = s * 32767.0f;
@@ -1437,18 +1460,20 @@ k_audio48(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const
             pcm[sb.pcm_off + o * C + c] = (int16_t)v;
         }
     }
-    __syncthreads();
+    __syncthreads();  // every read of the old state is done
     // carried state: the last K consumed samples, newest first; the last y
-    if (threadIdx.x < 2 * kRsTaps && L != M) {
-        const int c = threadIdx.x / kRsTaps, k = threadIdx.x % kRsTaps;
-        if (c < C) {
-            const int i = n - 1 - k;
-            as.dl[c][k] = i >= 0 ? in[i * C + c] : s_dl[c][-1 - i];
-        }
+    const int c = threadIdx.x / kRsTaps, k = threadIdx.x % kRsTaps;
+    const bool mine = bk.L != bk.M && threadIdx.x < 2 * kRsTaps && c < C;
+    float v = 0.f;
+    if (mine) {
+        const int i = n - 1 - k;
+        v = i >= 0 ? audio[sb.audio_off + i * C + c] : as.dl[c][-1 - i];
     }
-    if (wfm && a > 0.0 && nout > 0 && o1 == nout && o0 < o1) {
-        as.y[0] = y[0];
-        as.y[1] = y[1];
+    __syncthreads();  // the shifted entries are read before any is overwritten
+    if (mine) as.dl[c][k] = v;
+    if (de && nout > 0 && o1 == nout && o0 < o1) {
+        as.y[0] = y0;
+        as.y[1] = y1;
     }
 }
 
@@ -1558,11 +1583,15 @@ cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_audio48(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                           const RsBank *banks, AudState *aud, const float *audio, int16_t *pcm) {
-    k_audio48<<<count, kAudThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, pcm);
+cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *work, const int *list,
+                           const SlotBlock *sbt, const ChanParams *prm, const RsBank *banks, AudState *aud,
+                           const float *audio, float *rs_buf, int16_t *pcm) {
+    if (grid_rs > 0) k_audio48_rs<<<grid_rs, kAudThreads, 0, sm>>>(work, sbt, prm, banks, aud, audio, rs_buf);
+    k_audio48_out<<<count, kAudThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
     return cudaGetLastError();
 }
+
+int audio48_tile() { return kAudOT; }
 
 cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res) {

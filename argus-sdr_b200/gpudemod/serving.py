@@ -22,7 +22,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import CH_RDS, E_BUDGET, E_SLOTS, GPUDError, MODE_AM, MODE_CW, MODE_LSB, MODE_NFM, MODE_USB, \
+from . import CH_AUDIO48K, CH_RDS, E_BUDGET, E_SLOTS, GPUDError, MODE_AM, MODE_CW, MODE_LSB, MODE_NFM, MODE_USB, \
     MODE_WFM_STEREO
 from .synth import MODE_TABLE
 
@@ -39,11 +39,12 @@ class Request:
     kind: str         # WFM / NFM / AM / USB / LSB / CW
 
 
-def channel_spec(req: Request):
+def channel_spec(req: Request, pcm: bool = True):
     """(signal_id, offset, bandwidth, out_rate, taps, runner mode, flags) of a
-    request: WFM as stereo with RDS; the narrow modes at their own rates."""
+    request: WFM as stereo with RDS; the narrow modes at their own rates; with
+    `pcm` the audio comes back as the 48 kHz s16le stream /ws/audio sends."""
     out_rate, taps, bw = MODE_TABLE[req.kind]
-    flags = CH_RDS if req.kind == "WFM" else 0
+    flags = (CH_RDS if req.kind == "WFM" else 0) | (CH_AUDIO48K if pcm else 0)
     return (req.rid, req.offset_hz, bw, out_rate, taps, RUNNER_MODE[req.kind], flags)
 
 

@@ -49,7 +49,8 @@ N_BLOCKS = 64
 METRIC = "aggregate channel-MS/s on 1 B200 (serving vs plain runner); p99 block latency"
 WORKLOAD = ("FM band batch: 10 MS/s cf32, 2^20-sample blocks, 40 WFM stations on a 200 kHz grid "
             "(10-40 dB SNR), 256-tap FIR, decimate by 32 to 312.5 kS/s, FM discriminator, stereo "
-            "decode with 19 kHz pilot PLL, RDS baseband")
+            "decode with 19 kHz pilot PLL, RDS baseband; audio returned as the streaming path delivers "
+            "it: 48 kHz stereo s16le (polyphase resample, 50 us de-emphasis, x0.35)")
 
 
 def parse():
@@ -156,7 +157,7 @@ def make_scene(device, rank=0, n_blocks=N_BLOCKS):
 
 def admit_all(runner, stations):
     import gpudemod as G
-    return [runner.admit(i, st.offset_hz, BW, OUT_RATE, TAPS, G.MODE_WFM_STEREO, G.CH_RDS)
+    return [runner.admit(i, st.offset_hz, BW, OUT_RATE, TAPS, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_AUDIO48K)
             for i, st in enumerate(stations)]
 
 
@@ -172,7 +173,7 @@ def algorithmic_work(chans, n_in=BLOCK):
     3 stereo FIRs + the L-R / mono FIR of 101 taps at 2 flop per tap, PLL ~36
     per sample; RDS 4*101 per RDS output + 2 per composite sample.  Bytes: the
     wideband block read once + outputs + per-channel taps and history."""
-    w = {k: {"flop": 0, "bytes": 0} for k in ("extract", "demod", "wfm_fir", "wfm_out", "pll", "rds")}
+    w = {k: {"flop": 0, "bytes": 0} for k in ("extract", "demod", "wfm_fir", "wfm_out", "pll", "rds", "audio48")}
     w["extract"]["bytes"] = 8 * n_in
     per_out = {"WFM": 6, "NFM": 6, "AM": 5, "USB": 3, "LSB": 3, "CW": 1}
     for c in chans:
@@ -182,6 +183,12 @@ def algorithmic_work(chans, n_in=BLOCK):
         w["extract"]["bytes"] += 8 * n_out + 4 * T + 16 * (T - 1)
         w["demod"]["flop"] += per_out[c["kind"]] * n_out
         w["demod"]["bytes"] += 12 * n_out
+        # 48 kHz back end: 33-tap arm per output frame and audio channel,
+        # de-emphasis 3 and gain 1 per sample (WFM); 2 bytes per PCM sample
+        ach = 2 if c["kind"] == "WFM" else 1
+        n48 = n_out * 48000 // c["out_rate"]
+        w["audio48"]["flop"] += ach * n48 * (2 * 33 + (4 if c["kind"] == "WFM" else 0))
+        w["audio48"]["bytes"] += ach * (n_out * 4 + n48 * 2)
         if c["kind"] == "WFM":
             dr = c["out_rate"] // 19000
             n_rds = n_out // dr
@@ -205,6 +212,8 @@ def stage_key(name):
         return "pll"
     if name in ("demod", "am"):
         return "demod"
+    if name == "audio48k":
+        return "audio48"
     return name
 
 
@@ -247,9 +256,23 @@ def fp32_peak_tflops():
 # ---------------------------------------------------------------------------
 # CPU path (oracle restatement of the reference's Go CPU code)
 # ---------------------------------------------------------------------------
+class CpuChannel:
+    """The reference's CPU path for one channel: the oracle chain, then the
+    48 kHz back end (resample, de-emphasis, gain, s16le) on its audio."""
+
+    def __init__(self, O, fs, off, bw, rate, taps, mode, kind, rds):
+        self.ch = O.OracleChannel(fs, off, bw, rate, taps, mode, rds=rds)
+        stereo = mode == O.MODE_WFM_STEREO
+        self.back = O.Audio48(rate, 2 if stereo else 1, wfm=kind == "WFM", deemph_us=50.0)
+
+    def process(self, x):
+        out = self.ch.process(x)
+        self.back.process(out["audio"])
+
+
 def cpu_run(blocks_np, stations, n_blocks, threads):
     from oracle import oracle as O
-    chans = [O.OracleChannel(FS, st.offset_hz, BW, OUT_RATE, TAPS, O.MODE_WFM_STEREO, rds=True) for st in stations]
+    chans = [CpuChannel(O, FS, st.offset_hz, BW, OUT_RATE, TAPS, O.MODE_WFM_STEREO, "WFM", True) for st in stations]
 
     def work(c):
         for b in range(n_blocks):
@@ -284,7 +307,7 @@ def run_reference(args):
     # each step: every channel processes one 2^18-sample chunk (a bounded sample
     # of the 2^20 block) through the full chain, state carried across steps
     from oracle import oracle as O
-    chans = [O.OracleChannel(FS, st.offset_hz, BW, OUT_RATE, TAPS, O.MODE_WFM_STEREO, rds=True) for st in stations]
+    chans = [CpuChannel(O, FS, st.offset_hz, BW, OUT_RATE, TAPS, O.MODE_WFM_STEREO, "WFM", True) for st in stations]
     chunk = 1 << 18
     pos = [0]
 
@@ -537,12 +560,12 @@ def run_mixed(args, world, rank, local):
     def make_runner():
         r = G.ChannelRunner(FS, BLOCK, max_channels=128, max_taps=1024)
         for i, c in enumerate(chans):
-            r.admit(i, c["off"], c["bw"], c["out_rate"], c["T"], mode[c["kind"]], 0)
+            r.admit(i, c["off"], c["bw"], c["out_rate"], c["T"], mode[c["kind"]], G.CH_AUDIO48K)
         return r
 
     def cpu_baseline(blocks):
         omode = {"NFM": O.MODE_NFM, "AM": O.MODE_AM, "USB": O.MODE_USB, "LSB": O.MODE_LSB, "CW": O.MODE_CW}
-        oc = [O.OracleChannel(FS, c["off"], c["bw"], c["out_rate"], c["T"], omode[c["kind"]], rds=False)
+        oc = [CpuChannel(O, FS, c["off"], c["bw"], c["out_rate"], c["T"], omode[c["kind"]], c["kind"], False)
               for c in chans]
         nb = args.cpu_blocks
         bnp = [blocks[b].cpu().numpy() for b in range(nb)]

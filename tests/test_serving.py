@@ -82,5 +82,6 @@ def test_channel_spec_per_mode():
         spec = SV.channel_spec(SV.Request(7, 0.0, 1.0, 12345.0, kind))
         assert spec[:5] == (7, 12345.0, bw, rate, taps)
         assert spec[5] == SV.RUNNER_MODE[kind]
-        assert spec[6] == (G.CH_RDS if kind == "WFM" else 0)
+        assert spec[6] == (G.CH_RDS if kind == "WFM" else 0) | G.CH_AUDIO48K
+        assert SV.channel_spec(SV.Request(7, 0.0, 1.0, 0.0, kind), pcm=False)[6] & G.CH_AUDIO48K == 0
         assert 10_000_000 % rate == 0
