@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import ChannelResult, ChannelSpec, RunnerStats, StageTime, lib
+from ._lib import ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
 
 # DemodType (gpudemod.go:69-76) -> runner modes
 DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
@@ -336,3 +336,42 @@ def NewBatchRunner(max_samples: int, sample_rate: int) -> BatchRunner:
 
 def kernel_launch_count() -> int:
     return int(lib.gpud_kernel_launch_count())
+
+
+class StereoPilotDetector:
+    """classifier.StereoPilotPresent / estimateWFMPilot (internal/classifier/
+    pll.go:75-131) for a batch of FM-multiplex basebands on the device
+    (gpud_pilot_*).  Inputs are CUDA tensors (complex64) or host arrays, which
+    are copied to the device first."""
+
+    def __init__(self, max_jobs: int = 64, max_samples: int = 1 << 20):
+        self._p = C.c_void_p()
+        rc = lib.gpud_pilot_create(int(max_jobs), int(max_samples), C.byref(self._p))
+        if rc != 0:
+            raise GPUDError(rc, "gpud_pilot_create failed")
+
+    def close(self):
+        if self._p:
+            lib.gpud_pilot_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, iqs, sample_rates, window: bool = True, threshold: float = 4.0):
+        import torch
+        keep = []
+        jobs = (PilotJob * max(1, len(iqs)))()
+        for i, (x, fs) in enumerate(zip(iqs, sample_rates)):
+            t = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(x, np.complex64))
+            t = t.to(device="cuda", dtype=torch.complex64).contiguous()
+            keep.append(t)
+            jobs[i] = PilotJob(t.data_ptr(), t.numel(), int(fs), 1 if window else 0, 0)
+        res = (PilotResult * max(1, len(iqs)))()
+        torch.cuda.synchronize()
+        _check(None, lib.gpud_pilot_run(self._p, jobs, len(iqs), float(threshold), None, res))
+        return [{"present": bool(r.present), "ratio": r.ratio, "best_hz": r.best_hz, "median": r.median,
+                 "best_bin": r.best_bin} for r in res[: len(iqs)]]

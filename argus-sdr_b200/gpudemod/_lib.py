@@ -60,6 +60,16 @@ class ChannelResult(C.Structure):
     ]
 
 
+class PilotJob(C.Structure):
+    _fields_ = [("iq", C.c_void_p), ("n", C.c_int32), ("sample_rate", C.c_int32), ("window", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class PilotResult(C.Structure):
+    _fields_ = [("present", C.c_int32), ("best_bin", C.c_int32), ("ratio", C.c_double), ("best_hz", C.c_double),
+                ("median", C.c_double)]
+
+
 class StageTime(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("ms", C.c_double)]
 
@@ -135,6 +145,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_reset_all_signals": (i, [P]),
         "gpud_streaming_config_hash": (C.c_uint64, [C.c_int64, i, i, i]),
         "gpud_kernel_launch_count": (C.c_uint64, []),
+        "gpud_pilot_create": (i, [i, i, C.POINTER(P)]),
+        "gpud_pilot_destroy": (i, [P]),
+        "gpud_pilot_run": (i, [P, C.POINTER(PilotJob), i, d, P, C.POINTER(PilotResult)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -346,6 +346,41 @@ GPUD_API int GPUD_CALL gpud_runner_reset_all_signals(gpud_runner *r);
 GPUD_API uint64_t GPUD_CALL gpud_streaming_config_hash(int64_t signal_id, int out_rate, int num_taps,
                                                        int sample_rate);
 
+/* ------------------------------------------------------------------------
+ * Part 3: long-window stereo pilot detector
+ * classifier.StereoPilotPresent / estimateWFMPilot (internal/classifier/
+ * pll.go:75-131, 170-196) for a batch of FM-multiplex basebands (complex,
+ * carrier at DC), each analysed on the device: float64 discriminator,
+ * spectrum magnitude at 19 kHz +- 1 kHz in 10 Hz steps (201 bins), pilot
+ * present when max / median > threshold.
+ * ------------------------------------------------------------------------ */
+typedef struct gpud_pilot gpud_pilot;
+
+typedef struct {
+    const gpud_float2 *iq; /* device pointer to n samples */
+    int32_t n;
+    int32_t sample_rate;   /* below 40000: no decision (not present) */
+    int32_t window;        /* 1: the last sample_rate/2 samples (StereoPilotPresent); 0: all of them */
+    int32_t pad;
+} gpud_pilot_job;
+
+typedef struct {
+    int32_t present;  /* stereo pilot: median > 0 and ratio > threshold */
+    int32_t best_bin; /* 0..200, frequency 18000 + 10 * best_bin Hz (the first maximum) */
+    double ratio;     /* largest magnitude / median magnitude */
+    double best_hz;
+    double median;
+} gpud_pilot_result;
+
+/* max_samples bounds n (after the window) of every job. */
+GPUD_API int GPUD_CALL gpud_pilot_create(int max_jobs, int max_samples, gpud_pilot **out);
+GPUD_API int GPUD_CALL gpud_pilot_destroy(gpud_pilot *p);
+/* threshold <= 0 selects the reference's 4.0.  Runs on `stream` (NULL: the
+ * legacy default stream) and returns once results (host, count entries) are
+ * written. */
+GPUD_API int GPUD_CALL gpud_pilot_run(gpud_pilot *p, const gpud_pilot_job *jobs, int count, double threshold,
+                                      gpud_stream_handle stream, gpud_pilot_result *results);
+
 /* Number of kernels this library has launched in the process (all entry
  * points). */
 GPUD_API uint64_t GPUD_CALL gpud_kernel_launch_count(void);

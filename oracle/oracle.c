@@ -1335,3 +1335,71 @@ int or_audio48_process(or_audio48 *a, const float *in, int frames, float *out_f,
     free(audio);
     return nf * C;
 }
+
+/* ------------------------------------------------------------------------ */
+/* internal/classifier/pll.go:35-42, 75-131, 170-196  StereoPilotPresent /    */
+/* estimateWFMPilot: float64 FM discriminator, 201 Goertzel magnitudes at      */
+/* 19 kHz +-1 kHz in 10 Hz steps, locked when max / median > threshold.        */
+/* ------------------------------------------------------------------------ */
+
+static int or_cmp_double(const void *a, const void *b) {
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+/* window != 0: StereoPilotPresent (the last sample_rate/2 samples); else the
+ * whole vector (estimateWFMPilot as EstimateExactFrequency calls it).
+ * Returns the lock decision; *ratio, *best_hz, *median and mags[201] (may be
+ * NULL) receive the intermediate values. */
+int or_stereo_pilot(const cf32 *iq, int n, int sample_rate, int window, double threshold, double *ratio,
+                    double *best_hz, double *median, double *mags) {
+    *ratio = 0;
+    *best_hz = 19000.0;
+    *median = 0;
+    if (window) {
+        int mx = sample_rate / 2;
+        if (mx > 0 && n > mx) {
+            iq += n - mx;
+            n = mx;
+        }
+    }
+    if (sample_rate < 40000 || n < 2) return 0;
+    int nd = n - 1;
+    double *d = (double *)malloc(sizeof(double) * (size_t)nd);
+    for (int i = 1; i < n; i++) {
+        cf32 p = iq[i - 1], c = iq[i];
+        double num = (double)p.re * (double)c.im - (double)p.im * (double)c.re;
+        double den = (double)p.re * (double)c.re + (double)p.im * (double)c.im;
+        d[i - 1] = atan2(num, den);
+    }
+    double m[201], best = 0.0, bestf = 19000.0;
+    int cnt = 0;
+    for (double off = -1000.0; off <= 1000.0; off += 10.0) {
+        double f = 19000.0 + off;
+        double k = f / ((double)sample_rate / (double)nd);
+        double w = 2.0 * OR_PI * k / (double)nd;
+        double coeff = 2.0 * cos(w);
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = 0; i < nd; i++) {
+            double s0 = d[i] + coeff * s1 - s2;
+            s2 = s1;
+            s1 = s0;
+        }
+        double mag = sqrt(s1 * s1 + s2 * s2 - coeff * s1 * s2);
+        m[cnt++] = mag;
+        if (mag > best) {
+            best = mag;
+            bestf = f;
+        }
+    }
+    free(d);
+    if (mags) memcpy(mags, m, sizeof m);
+    double c[201];
+    memcpy(c, m, sizeof m);
+    qsort(c, 201, sizeof(double), or_cmp_double);
+    double med = c[201 / 2];
+    *median = med;
+    *best_hz = bestf;
+    if (med > 0) *ratio = best / med;
+    return med > 0 && *ratio > threshold;
+}

@@ -78,6 +78,7 @@ def _load() -> C.CDLL:
         "or_audio48_size": (C.c_size_t, []),
         "or_audio48_init": (i, [P, i, i, i, d]),
         "or_audio48_process": (i, [P, P, i, P, P]),
+        "or_stereo_pilot": (i, [P, i, i, i, d, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -478,3 +479,15 @@ class Audio48:
         pcm = np.zeros(cap, np.int16)
         n = _lib.or_audio48_process(self._buf, _p(a), frames, _p(f), _p(pcm))
         return f[:n].copy(), pcm[:n].copy()
+
+
+def stereo_pilot(iq, sample_rate: int, window: bool = True, threshold: float = 4.0):
+    """classifier.StereoPilotPresent (window=True) / estimateWFMPilot over the
+    whole vector (window=False), internal/classifier/pll.go:75-131.  Returns
+    (locked, ratio, best_hz, median, 201 magnitudes)."""
+    x = _c64(iq)
+    ratio, best, med = C.c_double(), C.c_double(), C.c_double()
+    mags = np.zeros(201, np.float64)
+    lk = _lib.or_stereo_pilot(_p(x), x.size, int(sample_rate), 1 if window else 0, float(threshold),
+                              C.byref(ratio), C.byref(best), C.byref(med), _p(mags))
+    return bool(lk), ratio.value, best.value, med.value, mags

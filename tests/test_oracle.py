@@ -361,3 +361,20 @@ def test_resampler_closed_form_counts(in_rate):
         want, t_next = _rs_advance(L, M, t, int(n))
         t = r.ratio()[3]
         assert (got, t) == (want, t_next), (n, got, want, t, t_next)
+
+
+def test_wfm_pilot_detection_kat():
+    """TestWFMPilotDetection (classifier/hard_rules_test.go:39-58): 2 s at
+    192 kS/s of an FM carrier modulated by a 19 kHz pilot at 10 % of 75 kHz
+    locks within 5 Hz; noise alone does not lock."""
+    fs = 192_000
+    i = np.arange(2 * fs)
+    dev = 0.1 * np.sin(2 * np.pi * 19000 * i / fs) * 75000 / fs
+    ph = np.cumsum(2 * np.pi * dev)
+    iq = (np.cos(ph) + 1j * np.sin(ph)).astype(np.complex64)
+    lk, ratio, best, _, _ = O.stereo_pilot(iq, fs, window=False)
+    assert lk and abs(best - 19000.0) <= 5
+    rng = np.random.default_rng(3)
+    noise = (rng.standard_normal(fs) + 1j * rng.standard_normal(fs)).astype(np.complex64)
+    assert not O.stereo_pilot(noise, fs)[0]
+    assert not O.stereo_pilot(iq, 32_000)[0]  # below 40 kS/s: no decision
