@@ -68,6 +68,7 @@ cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *
                            const float *audio, float *rs_buf, int16_t *pcm);
 int audio48_tile();
 int rds_smem_bytes(int dr);
+int rds_tile();
 int dense_smem_bytes_host(int P, int L);
 int wide_smem_bytes_host(int T);
 
@@ -753,7 +754,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         if ((mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO) && sb.n_disc > 0)
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_out.push_back(make_int2(i, t));
         if (sb.n_rds > 0) {
-            for (int t = 0; t * 64 < sb.n_rds; ++t) pl.w_rds.push_back(make_int2(i, t));
+            for (int t = 0; t * rds_tile() < sb.n_rds; ++t) pl.w_rds.push_back(make_int2(i, t));
             pl.rds_smem = std::max(pl.rds_smem, rds_smem_bytes(std::max(1, s.spec.out_rate / 19000)));
         }
     }

@@ -1169,9 +1169,28 @@ k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
 // float64 FreqShift phase, a 101-tap lowpass accumulated in float64 in the
 // reference's order (separate multiply and add, as Go's amd64 code does), and
 // every Dr-th stream sample kept.
-constexpr int kRdsOT = 64;
+constexpr int kRdsOT = 128;     // RDS outputs per CTA (one per thread)
+constexpr int kRdsThreads = 128;
 
-__global__ void __launch_bounds__(128)
+// Index of the binade entry covering stream index k.
+__device__ __forceinline__ int binade_find(const BinadeTable &t, int64_t k) {
+    int lo = 0, hi = t.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.e[mid].k_start <= k) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// RDS baseband (demod/fm.go:143-163, 234-271): the composite shifted by the
+// reference's float64 FreqShift phase (exact values from the binade table),
+// 101-tap float64 low-pass evaluated at the kept outputs only.  Staging: each
+// thread takes a contiguous run of composite samples, evaluates sin/cos of
+// the exact phase once at the run start (and at any binade start inside it)
+// and advances by the exact in-binade step with a float64 rotation
+// (relative error < 1e-14 over a run, far below the float32 the shifted
+// samples are stored in).
+__global__ void __launch_bounds__(kRdsThreads)
 k_rds(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
       const ChanState *__restrict__ st, const WfmTaps *__restrict__ taps, const BinadeTable *__restrict__ tabs,
       const float *__restrict__ wk, const float2 *__restrict__ rds_dl, float2 *__restrict__ rds_out) {
@@ -1191,14 +1210,28 @@ k_rds(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const Ch
     const BinadeTable &tab = tabs[cp.rds_tab];
     const float *comp = wk + sb.comp_off;
     const float2 *dl = rds_dl + cp.wfm_idx * kWfmHist;
-    for (int i = threadIdx.x; i < span; i += blockDim.x) {
-        int q = qlo + i;
+    const int per = (span + kRdsThreads - 1) / kRdsThreads;
+    const int i0 = min(span, (int)threadIdx.x * per), i1 = min(span, i0 + per);
+    int ent = -1;
+    int64_t next_k = 0;
+    double cs = 0.0, sn = 0.0, wc = 1.0, ws = 0.0;
+    for (int i = i0; i < i1; ++i) {
+        const int q = qlo + i;
         float2 v = make_float2(0.f, 0.f);
         if (q >= 0) {
-            double ph = binade_value(tab, c0 + q + 1);
-            double sn, cs;
-            sincos(ph, &sn, &cs);
-            double b = (double)comp[q];
+            const int64_t k = c0 + q + 1;  // phase index: incremented before use (freqshift.go:13-15)
+            if (ent < 0 || k >= next_k) {
+                ent = binade_find(tab, k);
+                const BinadeEntry &be = tab.e[ent];
+                next_k = ent + 1 < tab.count ? tab.e[ent + 1].k_start : INT64_MAX;
+                sincos(be.x_start + (double)(k - be.k_start) * be.q, &sn, &cs);
+                sincos(be.q, &ws, &wc);
+            } else {
+                const double c1 = cs * wc - sn * ws;
+                sn = sn * wc + cs * ws;
+                cs = c1;
+            }
+            const double b = (double)comp[q];
             v = make_float2((float)(b * cs), (float)(b * sn));
         } else if (q >= -s.rds_hist_len) {
             v = dl[kWfmHist + q];
@@ -1207,7 +1240,7 @@ k_rds(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const Ch
     }
     __syncthreads();
     const WfmTaps &tb = taps[cp.rds_tab];
-    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    for (int r = r0 + threadIdx.x; r < r1; r += kRdsThreads) {
         const int qr = sb.rds_first + r * dr;
         const int li = qr - qlo;
         double ar = 0.0, ai = 0.0;
@@ -1572,7 +1605,7 @@ cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const Sl
 cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                        const ChanParams *prm, const ChanState *st, const WfmTaps *taps, const BinadeTable *tabs,
                        const float *wk, const float2 *rds_dl, float2 *rds_out) {
-    k_rds<<<grid, 128, smem, sm>>>(work, sbt, prm, st, taps, tabs, wk, rds_dl, rds_out);
+    k_rds<<<grid, kRdsThreads, smem, sm>>>(work, sbt, prm, st, taps, tabs, wk, rds_dl, rds_out);
     return cudaGetLastError();
 }
 
@@ -1600,5 +1633,6 @@ cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, co
 }
 
 int rds_smem_bytes(int dr) { return (kRdsOT * dr + kWfmTaps + 8) * 8; }
+int rds_tile() { return kRdsOT; }
 
 }  // namespace gpud

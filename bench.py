@@ -220,7 +220,7 @@ def stage_key(name):
 # DRAM bytes per launch of the dominant kernel, read+write, from an ncu
 # capture (--set full) of that kernel on the same workload; None where no
 # capture exists.
-NCU_TRAFFIC = {("fm_band", "extract"): 8.58e6}
+NCU_TRAFFIC = {("fm_band", "extract"): 8.58e6, ("mixed", "extract"): 8.91e6}
 
 
 def measured_peaks():
