@@ -70,6 +70,7 @@ int audio48_tile();
 int rds_smem_bytes(int dr);
 int rds_tile();
 int dense_smem_bytes_host(int P, int L);
+int dense_tile();
 int wide_smem_bytes_host(int T);
 
 constexpr int kWfmTapsPadH = 104;
@@ -735,7 +736,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         Slot &s = r->slots[(size_t)sb.slot];
         if (sb.n_out > 0) {
             if (s.ext_kind == 0) {
-                for (int t = 0; t * 256 < sb.n_out; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
+                for (int t = 0; t * dense_tile() < sb.n_out; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
                 pl.dense_smem[s.L] = std::max(pl.dense_smem[s.L], dense_smem_bytes_host(s.P, s.L));
             } else {
                 for (int t = 0; t * 32 < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));

@@ -74,6 +74,7 @@ __host__ __device__ inline int dense_smem_bytes(int P, int L) {
 }
 
 int dense_smem_bytes_host(int P, int L) { return dense_smem_bytes(P, L); }
+int dense_tile() { return kDenseOT; }
 
 template <int L>
 __global__ void __launch_bounds__(kDenseThreads, 2)
@@ -172,11 +173,14 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
 #pragma unroll
     for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
     for (int p = warp; p < P; p += 8) {
-        // lane window: columns lane*R + tt, stored at (lane*R + tt) + (lane*R + tt)/8
-        const float2 *zrow = Z + p * Mp + lane * (R + 1);
+        // lane window: columns c = lane*R + tt, stored at c + c/8
+        const float2 *zrow = Z + p * Mp;
         float2 win[R + L - 1];
 #pragma unroll
-        for (int tt = 0; tt < R + L - 1; ++tt) win[tt] = zrow[tt + (tt >> 3)];
+        for (int tt = 0; tt < R + L - 1; ++tt) {
+            const int c = lane * R + tt;
+            win[tt] = zrow[c + (c >> 3)];
+        }
         float h[L];
 #pragma unroll
         for (int u = 0; u < L; ++u) h[u] = tsm[p * L + u];
@@ -192,12 +196,14 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     }
     __syncthreads();
     constexpr int RS = kDenseOT + kDenseOT / 8;
-    float2 *red = Z + warp * RS + lane * (R + 1);
+    float2 *red = Z + warp * RS;
 #pragma unroll
-    for (int r = 0; r < R; ++r) red[r] = make_float2(ar[r], ai[r]);
+    for (int r = 0; r < R; ++r) {
+        const int o = lane * R + r;
+        red[o + (o >> 3)] = make_float2(ar[r], ai[r]);
+    }
     __syncthreads();
-    {
-        const int o = threadIdx.x;
+    for (int o = threadIdx.x; o < kDenseOT; o += kDenseThreads) {
         float2 sum = make_float2(0.f, 0.f);
 #pragma unroll
         for (int wv = 0; wv < 8; ++wv) {
@@ -1236,16 +1242,19 @@ k_rds(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const Ch
         } else if (q >= -s.rds_hist_len) {
             v = dl[kWfmHist + q];
         }
-        cpl[i] = v;
+        cpl[i + (i >> 4)] = v;
     }
     __syncthreads();
+    // outputs dr samples apart read through one pad slot every 16: the lanes'
+    // addresses fall in distinct banks
     const WfmTaps &tb = taps[cp.rds_tab];
     for (int r = r0 + threadIdx.x; r < r1; r += kRdsThreads) {
         const int qr = sb.rds_first + r * dr;
         const int li = qr - qlo;
         double ar = 0.0, ai = 0.0;
         for (int k = 0; k < kWfmTaps; ++k) {
-            const float2 v = cpl[li - k];
+            const int c = li - k;
+            const float2 v = cpl[c + (c >> 4)];
             ar = __dadd_rn(ar, __dmul_rn((double)v.x, tb.rds[k]));
             ai = __dadd_rn(ai, __dmul_rn((double)v.y, tb.rds[k]));
         }
@@ -1632,7 +1641,10 @@ cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, co
     return cudaGetLastError();
 }
 
-int rds_smem_bytes(int dr) { return (kRdsOT * dr + kWfmTaps + 8) * 8; }
+int rds_smem_bytes(int dr) {
+    const int span = kRdsOT * dr + kWfmTaps + 8;
+    return (span + span / 16 + 1) * 8;
+}
 int rds_tile() { return kRdsOT; }
 
 }  // namespace gpud
