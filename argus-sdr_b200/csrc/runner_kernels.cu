@@ -1397,47 +1397,83 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
 constexpr int kAudThreads = 256;
 constexpr int kAudOT = 256;  // resampled frames per CTA in k_audio48_rs
 
+constexpr int kAudWin = 4096;     // staged input frames per channel and CTA
+constexpr int kAudBank = 4096;    // staged bank coefficients (doubles)
+
 __global__ void __launch_bounds__(kAudThreads)
 k_audio48_rs(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
              const RsBank *__restrict__ banks, const AudState *__restrict__ aud, const float *__restrict__ audio,
              float *__restrict__ rs_out) {
+    extern __shared__ double s_aud[];  // bank (L*K doubles) | inputs 2 x kAudWin floats
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
-    const int o = w.y * kAudOT + (int)threadIdx.x;
-    if (o >= sb.rs_nout) return;
+    const int oa = w.y * kAudOT, ob = min(sb.rs_nout, oa + kAudOT);  // this CTA's outputs
+    if (oa >= ob) return;
     const ChanParams &cp = prm[sb.slot];
     const AudState &as = aud[sb.slot];
     const RsBank &bk = banks[cp.rs_bank];
     const int C = cp.aud_ch, L = bk.L, M = bk.M, K = bk.K;
     const float *in = audio + sb.audio_off;
-    float *dst = rs_out + sb.pcm_off + o * C;
+    const int o = oa + (int)threadIdx.x;
     if (L == M) {
-        for (int c = 0; c < C; ++c) dst[c] = in[o * C + c];
+        if (o < ob)
+            for (int c = 0; c < C; ++c) rs_out[sb.pcm_off + o * C + c] = in[o * C + c];
         return;
     }
+    // consumed-input window of the tile: [lo, hi]
+    const int64_t lo = ((int64_t)sb.rs_t0 + (int64_t)oa * M) / L - K;
+    const int64_t hi = ((int64_t)sb.rs_t0 + (int64_t)(ob - 1) * M) / L - 1;
+    const int win = (int)(hi - lo + 1);
+    const bool staged = win <= kAudWin && L * K <= kAudBank;
+    double *s_bank = s_aud;
+    float *s_in = reinterpret_cast<float *>(s_aud + kAudBank);
+    if (staged) {
+        for (int i = threadIdx.x; i < L * K; i += kAudThreads) s_bank[i] = bk.arm[i];
+        for (int i = threadIdx.x; i < win; i += kAudThreads) {
+            const int64_t g = lo + i;
+            for (int c = 0; c < C; ++c)
+                s_in[c * kAudWin + i] = g >= 0 ? in[g * C + c] : as.dl[c][-1 - g];
+        }
+        __syncthreads();
+    }
+    if (o >= ob) return;
     const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
     const int64_t cc = T / L;  // T >= 0
-    const double *arm = bk.arm + (int)(T - cc * L) * K;
+    const int ph = (int)(T - cc * L);
     double acc0 = 0.0, acc1 = 0.0;
-    for (int k = 0; k < K; ++k) {
-        const int64_t i = cc - 1 - k;
-        const double h = arm[k];
-        const float v0 = i >= 0 ? in[i * C] : as.dl[0][-1 - i];
-        acc0 = __dadd_rn(acc0, __dmul_rn((double)v0, h));
-        if (C == 2) {
-            const float v1 = i >= 0 ? in[i * 2 + 1] : as.dl[1][-1 - i];
-            acc1 = __dadd_rn(acc1, __dmul_rn((double)v1, h));
+    if (staged) {
+        const double *arm = s_bank + ph * K;
+        const float *x0 = s_in + (cc - 1 - lo), *x1 = s_in + kAudWin + (cc - 1 - lo);
+        for (int k = 0; k < K; ++k) {
+            const double h = arm[k];
+            acc0 = __dadd_rn(acc0, __dmul_rn((double)x0[-k], h));
+            if (C == 2) acc1 = __dadd_rn(acc1, __dmul_rn((double)x1[-k], h));
+        }
+    } else {
+        const double *arm = bk.arm + ph * K;
+        for (int k = 0; k < K; ++k) {
+            const int64_t i = cc - 1 - k;
+            const double h = arm[k];
+            const float v0 = i >= 0 ? in[i * C] : as.dl[0][-1 - i];
+            acc0 = __dadd_rn(acc0, __dmul_rn((double)v0, h));
+            if (C == 2) {
+                const float v1 = i >= 0 ? in[i * 2 + 1] : as.dl[1][-1 - i];
+                acc1 = __dadd_rn(acc1, __dmul_rn((double)v1, h));
+            }
         }
     }
+    float *dst = rs_out + sb.pcm_off + o * C;
     dst[0] = (float)acc0;
     if (C == 2) dst[1] = (float)acc1;
 }
 
-__global__ void __launch_bounds__(kAudThreads)
+constexpr int kAudOutThreads = 1024;  // one CTA per channel: short serial runs
+
+__global__ void __launch_bounds__(kAudOutThreads)
 k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
               const RsBank *__restrict__ banks, AudState *__restrict__ aud, const float *__restrict__ audio,
               const float *__restrict__ rs_out, int16_t *__restrict__ pcm) {
-    __shared__ double s_a[kAudThreads], s_b[2][kAudThreads];
+    __shared__ double s_a[kAudOutThreads], s_b[2][kAudOutThreads];
     const SlotBlock sb = sbt[list[blockIdx.x]];
     const ChanParams &cp = prm[sb.slot];
     AudState &as = aud[sb.slot];
@@ -1446,7 +1482,7 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
     if (n <= 0) return;
     const RsBank &bk = banks[cp.rs_bank];
     const float *r = rs_out + sb.pcm_off;
-    const int per = (nout + kAudThreads - 1) / kAudThreads;
+    const int per = (nout + kAudOutThreads - 1) / kAudOutThreads;
     const int o0 = min(nout, (int)threadIdx.x * per), o1 = min(nout, o0 + per);
     const bool wfm = cp.mode == 2 || cp.mode == 3;
     const double a = cp.deemph_a;
@@ -1465,7 +1501,7 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
         s_b[1][threadIdx.x] = B1;
         __syncthreads();
         // inclusive scan of the maps (a later run applied after an earlier one)
-        for (int d = 1; d < kAudThreads; d <<= 1) {
+        for (int d = 1; d < kAudOutThreads; d <<= 1) {
             double pa = 1.0, pb0 = 0.0, pb1 = 0.0;
             const bool take = (int)threadIdx.x >= d;
             if (take) {
@@ -1628,8 +1664,15 @@ cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, c
 cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *work, const int *list,
                            const SlotBlock *sbt, const ChanParams *prm, const RsBank *banks, AudState *aud,
                            const float *audio, float *rs_buf, int16_t *pcm) {
-    if (grid_rs > 0) k_audio48_rs<<<grid_rs, kAudThreads, 0, sm>>>(work, sbt, prm, banks, aud, audio, rs_buf);
-    k_audio48_out<<<count, kAudThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
+    const int smem = kAudBank * 8 + 2 * kAudWin * 4;
+    static bool attr_set = false;  // 64 KiB of dynamic shared memory needs the opt-in
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_audio48_rs, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (grid_rs > 0) k_audio48_rs<<<grid_rs, kAudThreads, smem, sm>>>(work, sbt, prm, banks, aud, audio, rs_buf);
+    k_audio48_out<<<count, kAudOutThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
     return cudaGetLastError();
 }
 
