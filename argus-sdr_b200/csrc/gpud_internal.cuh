@@ -85,6 +85,8 @@ struct ChanParams {
     double rds_inc;                        // 2*pi*57000/out_rate
     int32_t rds_tab;                       // binade table id for the RDS phase
     int32_t aud_ch;                        // audio channels (2 for WFM_STEREO, else 1)
+    int32_t d1;                            // pre-demod decimation (1: none)
+    int32_t pad2;
     double deemph_a;                       // de-emphasis coefficient exp(-1/(48000 tau)), 0: none
 };
 
@@ -128,6 +130,12 @@ struct SlotBlock {
     int32_t rs_nout;   // 48 kHz frames produced this block
     int32_t pcm_off;   // int16 offset into the PCM output region
     int32_t rs_frames; // demod-rate frames consumed this block
+    // demodulator input: the extraction output, or with a pre-demod
+    // decimation stage its output (streamer.go:1098-1146)
+    int32_t dem_off;   // float2 offset of the demod input in the IQ region
+    int32_t n_dem;     // demod input samples this block
+    int32_t d1_phase;  // pre-demod decimator phase before the block
+    int32_t pad_sb;
 };
 
 // Rational polyphase resampler bank (dsp/resample.go:45-93) for one input rate.
@@ -184,6 +192,7 @@ __device__ __forceinline__ double binade_value(const BinadeTable &t, int64_t k) 
 
 constexpr int kWfmTaps = 101;      // stereo / RDS filter length (streamer.go:1531-1545, fm.go:155)
 constexpr int kWfmHist = 100;
+constexpr int kD1Taps = 101;       // pre-demod decimating FIR (streamer.go:1124)
 
 }  // namespace gpud
 

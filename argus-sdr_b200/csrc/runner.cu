@@ -60,7 +60,10 @@ cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, co
                        const float *wk, const float2 *rds_dl, float2 *rds_out);
 cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                               const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
-                              float2 *rds_dl, const BinadeTable *tabs, DevResult *res);
+                              float2 *rds_dl, const BinadeTable *tabs, float2 *d1hist, DevResult *res);
+cudaError_t launch_decim2(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                          const double *d1taps, const float2 *d1hist, float2 *ext);
+int decim2_tile();
 cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res);
 cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *work, const int *list,
@@ -177,6 +180,7 @@ struct Slot {
     bool has_last = false;
     int64_t rds_count = 0;
     int64_t rs_t = 0;  // 48 kHz resampler phase counter (outTime)
+    int d1 = 1, d1_phase = 0;  // pre-demod decimation and its phase counter
     int rs_class = -1, rs_L = 1, rs_M = 1, aud_ch = 1;
     uint64_t footprint = 0;
 };
@@ -194,6 +198,7 @@ struct BlockPlan {
     std::vector<int> pll_list;
     std::vector<int> aud_list;  // entries with a 48 kHz back end and input this block
     std::vector<int2> w_aud;    // (entry, tile) of the 48 kHz resampler
+    std::vector<int2> w_dec;    // (entry, tile) of the pre-demod decimator
     int64_t tot_ext = 0, tot_emit_ext = 0, tot_comp = 0, tot_audio = 0, tot_audio_host = 0, tot_rds = 0,
             tot_pcm = 0;
 };
@@ -264,6 +269,8 @@ struct gpud_runner {
     BinadeTable *d_tabs = nullptr;
     std::vector<int> class_rate;  // rate of each WFM rate class
     AudState *d_aud = nullptr;    // per slot
+    double *d_d1taps = nullptr;   // per slot: pre-demod decimator taps
+    float2 *d_d1hist = nullptr;   // per slot: its 100-sample history
     RsBank *d_banks = nullptr;
     std::vector<int> rs_rate;     // input rate of each resampler bank
     std::vector<int3> rs_lmk;     // (L, M, K) of each bank
@@ -357,7 +364,7 @@ static uint64_t slot_block_bytes(const gpud_runner *r, int D, int mode, int flag
 
 static uint64_t slot_state_bytes(const gpud_runner *r) {
     return sizeof(ChanParams) + sizeof(ChanState) + (uint64_t)r->tapcap * 2 * 4 + (uint64_t)2 * r->max_taps * 8 +
-           (kWfmHist * 3 + kAudioDlStrideH) * 8 + sizeof(AudState);
+           (kWfmHist * 3 + kAudioDlStrideH) * 8 + sizeof(AudState) + kD1Taps * 8 + kWfmHist * 8;
 }
 
 // NewResampler (dsp/resample.go:45-93, 256-295): L/M from the gcd, odd
@@ -500,6 +507,9 @@ static void design_taps(gpud_runner *r, const Slot &s, double bandwidth, std::ve
     *cutoff_out = cutoff;
 }
 
+// Rate of the demodulator and everything after it.
+static int demod_rate(const Slot &s) { return s.spec.out_rate / std::max(1, s.d1); }
+
 static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     Slot &s = r->slots[(size_t)slot];
     std::memset(p, 0, sizeof *p);
@@ -512,13 +522,13 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     p->plen = s.L;
     p->mode = s.spec.mode;
     p->flags = s.spec.flags;
-    p->out_rate = s.spec.out_rate;
+    p->out_rate = demod_rate(s);
     p->taps_off = s.taps_off;
     p->dtaps_off = s.dtaps_off;
     p->hist_off = s.hist_off;
     p->hcap = s.hcap;
     p->wfm_idx = s.wfm_idx;
-    int rate = s.spec.out_rate;
+    int rate = demod_rate(s);
     p->rds_dr = std::max(1, rate / 19000);
     double bfo = s.spec.mode == GPUD_MODE_LSB ? -700.0 : 700.0;
     p->ssb_inc = 2 * GPUD_PI * bfo / (double)rate;
@@ -535,6 +545,7 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     double tau_us = (s.spec.flags & GPUD_CH_DEEMPH75) ? 75.0 : 50.0;
     if (s.spec.flags & GPUD_CH_NO_DEEMPH) tau_us = 0.0;
     p->deemph_a = (wfm && tau_us > 0) ? std::exp(-1.0 / (48000.0 * tau_us * 1e-6)) : 0.0;
+    p->d1 = s.d1;
 }
 
 static void queue_write(gpud_runner *r, int slot, void *dst, const void *src, size_t bytes) {
@@ -561,6 +572,9 @@ static int validate_spec(gpud_runner *r, const gpud_channel_spec *spec, int *D, 
     if (*T > r->max_taps) return set_err(r, GPUD_E_TAPS, "num_taps above the runner's max_taps");
     int P = std::min(*D, *T), L = (*T + *D - 1) / *D;
     if ((int64_t)P * L > r->tapcap || *T > r->tapcap) return set_err(r, GPUD_E_TAPS, "tap layout too large");
+    if (spec->demod_decim < 0 || spec->demod_decim > 64 ||
+        (spec->demod_decim > 1 && spec->out_rate / spec->demod_decim < 1000))
+        return set_err(r, GPUD_E_DECIM, "demod_decim out of range");
     return 0;
 }
 
@@ -630,14 +644,19 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
     sb.n_out = (s.pc + n) / s.D;
     sb.hist_len = s.hist_len;
     sb.hist_sel = s.hist_sel;
+    // demodulator input: the extraction output, or the samples the pre-demod
+    // decimator emits (those with phase counter 0: d1_phase + j*d1)
+    sb.d1_phase = s.d1_phase;
+    sb.n_dem = sb.n_out;
+    if (s.d1 > 1) sb.n_dem = sb.n_out > s.d1_phase ? (sb.n_out - 1 - s.d1_phase) / s.d1 + 1 : 0;
     int mode = s.spec.mode;
     bool fm = mode == GPUD_MODE_NFM || mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO;
     bool wfm = mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO;
     sb.n_disc = 0;
     sb.bridge = 0;
-    if (fm && sb.n_out > 0) {
+    if (fm && sb.n_dem > 0) {
         sb.bridge = s.has_last ? 1 : 0;
-        sb.n_disc = s.has_last ? sb.n_out : sb.n_out - 1;
+        sb.n_disc = s.has_last ? sb.n_dem : sb.n_dem - 1;
     }
     switch (mode) {
     case GPUD_MODE_NFM:
@@ -646,14 +665,14 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
     case GPUD_MODE_AM:
     case GPUD_MODE_USB:
     case GPUD_MODE_LSB:
-    case GPUD_MODE_CW: sb.n_audio = sb.n_out; break;
+    case GPUD_MODE_CW: sb.n_audio = sb.n_dem; break;
     default: sb.n_audio = 0;
     }
     sb.comp_hist_len = s.comp_hist_len;
     sb.n_rds = 0;
     sb.rds_first = -1;
     if (wfm && (s.spec.flags & GPUD_CH_RDS) && sb.n_disc > 0) {
-        int dr = std::max(1, s.spec.out_rate / 19000);
+        int dr = std::max(1, demod_rate(s) / 19000);
         int64_t c0 = s.rds_count;
         int qf = (int)((dr - c0 % dr) % dr);
         if (qf < sb.n_disc) {
@@ -685,6 +704,15 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             ext += (sb.n_out + 3) & ~3;
             if (pass == 0) pl.tot_emit_ext = ext;
         }
+    // pre-demod decimator outputs after every extraction output
+    for (auto &sb : pl.sbs) {
+        if (r->slots[(size_t)sb.slot].d1 > 1) {
+            sb.dem_off = (int)ext;
+            ext += (sb.n_dem + 3) & ~3;
+        } else {
+            sb.dem_off = sb.ext_off;
+        }
+    }
     pl.tot_ext = ext;
     int64_t comp = 0, audio = 0, rds = 0, pcm = 0;
     // demod-rate audio: channels that return it to the host first, then those
@@ -700,6 +728,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         }
     pl.aud_list.clear();
     pl.w_aud.clear();
+    pl.w_dec.clear();
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         SlotBlock &sb = pl.sbs[(size_t)i];
         Slot &s = r->slots[(size_t)sb.slot];
@@ -744,10 +773,12 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             }
         }
         int mode = s.spec.mode;
-        int nd = (mode == GPUD_MODE_USB || mode == GPUD_MODE_LSB || mode == GPUD_MODE_CW) ? sb.n_out : sb.n_disc;
+        int nd = (mode == GPUD_MODE_USB || mode == GPUD_MODE_LSB || mode == GPUD_MODE_CW) ? sb.n_dem : sb.n_disc;
         if ((mode >= GPUD_MODE_NFM && mode <= GPUD_MODE_WFM_STEREO) || mode >= GPUD_MODE_USB)
             for (int t = 0; t * 1024 < nd; ++t) pl.w_demod.push_back(make_int2(i, t));
-        if (mode == GPUD_MODE_AM && sb.n_out > 0) pl.w_am.push_back(make_int2(i, 0));
+        if (mode == GPUD_MODE_AM && sb.n_dem > 0) pl.w_am.push_back(make_int2(i, 0));
+        if (s.d1 > 1)
+            for (int t = 0; t * decim2_tile() < sb.n_dem; ++t) pl.w_dec.push_back(make_int2(i, t));
         if (mode == GPUD_MODE_WFM_STEREO && sb.n_disc > 0) {
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_fir.push_back(make_int2(i, t));
             pl.pll_list.push_back(i);
@@ -756,7 +787,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_out.push_back(make_int2(i, t));
         if (sb.n_rds > 0) {
             for (int t = 0; t * rds_tile() < sb.n_rds; ++t) pl.w_rds.push_back(make_int2(i, t));
-            pl.rds_smem = std::max(pl.rds_smem, rds_smem_bytes(std::max(1, s.spec.out_rate / 19000)));
+            pl.rds_smem = std::max(pl.rds_smem, rds_smem_bytes(std::max(1, demod_rate(s) / 19000)));
         }
     }
 }
@@ -795,7 +826,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
-          pl.w_rds.size() + pl.w_aud.size();
+          pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
@@ -828,7 +859,8 @@ static void advance_mirrors(gpud_runner *r, const BlockPlan &pl, int n, std::vec
         s.pc = (s.pc + n) % s.D;
         s.hist_len = std::min(s.T - 1, s.hist_len + n);
         s.hist_sel = 1 - s.hist_sel;
-        if (sb.n_out > 0) s.has_last = true;
+        if (sb.n_dem > 0) s.has_last = true;
+        if (s.d1 > 1) s.d1_phase = ((s.d1_phase - sb.n_out) % s.d1 + s.d1) % s.d1;
         if (s.wfm_idx >= 0) {
             s.comp_hist_len = std::min(kWfmHist, s.comp_hist_len + sb.n_disc);
             s.rds_count += sb.n_disc;
@@ -889,7 +921,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         return at;
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
-           o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud);
+           o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
@@ -931,6 +963,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                                n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
+    if (!pl.w_dec.empty()) {
+        prof_mark(r, f, "decim2");
+        CK(launch_decim2((int)pl.w_dec.size(), f.s, d_w + o_wdec, d_sb, r->d_prm, r->d_d1taps, r->d_d1hist, d_ext));
+        nl++;
+    }
     if (!pl.w_demod.empty()) {
         prof_mark(r, f, "demod");
         CK(launch_demod((int)pl.w_demod.size(), f.s, d_w + o_dem, d_sb, r->d_prm, r->d_st, d_ext, f.d_wk, d_audio));
@@ -955,7 +992,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     if (!pl.sbs.empty()) {
         prof_mark(r, f, "post_front");
         CK(launch_post_front((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_ext, f.d_wk,
-                             r->d_comp_dl, r->d_rds_dl, r->d_tabs, d_res));
+                             r->d_comp_dl, r->d_rds_dl, r->d_tabs, r->d_d1hist, d_res));
         nl++;
     }
     CK(cudaEventRecord(f.ev_front, f.s));
@@ -1236,6 +1273,8 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     CKC(dalloc(&r->d_wtaps, (size_t)kMaxWfmClasses));
     CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses));
     CKC(dalloc(&r->d_aud, M));
+    CKC(dalloc(&r->d_d1taps, M * kD1Taps));
+    CKC(dalloc(&r->d_d1hist, M * kWfmHist));
     CKC(dalloc(&r->d_banks, (size_t)kMaxRsClasses));
 #undef CKC
     r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 8 * kFrames + sizeof(RsBank) * kMaxRsClasses;
@@ -1276,6 +1315,8 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     cudaFree(r->d_wtaps);
     cudaFree(r->d_tabs);
     cudaFree(r->d_aud);
+    cudaFree(r->d_d1taps);
+    cudaFree(r->d_d1hist);
     cudaFree(r->d_banks);
     if (r->stream) cudaStreamDestroy(r->stream);
     if (r->admin) cudaStreamDestroy(r->admin);
@@ -1338,13 +1379,15 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     if (slot < 0) return set_err(r, GPUD_E_SLOTS, "channel cap reached");
     bool wfm = spec->mode == GPUD_MODE_WFM || spec->mode == GPUD_MODE_WFM_STEREO;
     int rclass = -1;
+    int d1 = std::max(1, spec->demod_decim);
+    int drate = spec->out_rate / d1;  // actualDemodRate (streamer.go:1113)
     if (wfm) {
-        rclass = rate_class_for(r, spec->out_rate);
+        rclass = rate_class_for(r, drate);
         if (rclass < 0) return set_err(r, GPUD_E_CUDA, "WFM rate classes exhausted");
     }
     int rsclass = -1;
     if ((spec->flags & GPUD_CH_AUDIO48K) && spec->mode != GPUD_MODE_IQ) {
-        rsclass = rs_class_for(r, spec->out_rate);
+        rsclass = rs_class_for(r, drate);
         if (rsclass < 0) return set_err(r, GPUD_E_ARG, "no 48 kHz resampler for this output rate");
     }
     drop_pending(r, slot);
@@ -1364,6 +1407,8 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     s.rate_class = rclass;
     s.rs_class = rsclass;
     s.aud_ch = spec->mode == GPUD_MODE_WFM_STEREO ? 2 : 1;
+    s.d1 = d1;
+    s.d1_phase = 0;
     if (rsclass >= 0) {
         s.rs_L = r->rs_lmk[(size_t)rsclass].x;
         s.rs_M = r->rs_lmk[(size_t)rsclass].y;
@@ -1377,12 +1422,22 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     ChanParams p;
     fill_params(r, slot, &p);
     ChanState st{};
-    st.pll_freq = 2 * GPUD_PI * 19000 / (double)s.spec.out_rate;  // stereoDecodeStateful init (streamer.go:1546-1555)
+    st.pll_freq = 2 * GPUD_PI * 19000 / (double)demod_rate(s);  // stereoDecodeStateful init (streamer.go:1546-1555)
     CK(cudaMemcpyAsync(r->d_taps + s.taps_off, pm.data(), pm.size() * 4, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemcpyAsync(r->d_taps + s.dtaps_off, h.data(), h.size() * 4, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemcpyAsync(r->d_prm + slot, &p, sizeof p, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemcpyAsync(r->d_st + slot, &st, sizeof st, cudaMemcpyHostToDevice, r->admin));
     CK(cudaMemsetAsync(r->d_aud + slot, 0, sizeof(AudState), r->admin));
+    if (d1 > 1) {
+        // streamer.go:1117-1124: 101 taps of LowpassFIR(cutoff, snip rate),
+        // 90 kHz for WFM, else 0.8 x the demod Nyquist
+        double cut = wfm ? 90000.0 : (double)drate / 2.0 * 0.8;
+        auto h1 = lowpass_fir(cut, spec->out_rate, kD1Taps);
+        h1.resize(kD1Taps, 0.0);
+        CK(cudaMemcpyAsync(r->d_d1taps + (size_t)slot * kD1Taps, h1.data(), kD1Taps * 8, cudaMemcpyHostToDevice,
+                           r->admin));
+        CK(cudaMemsetAsync(r->d_d1hist + (size_t)slot * kWfmHist, 0, kWfmHist * sizeof(float2), r->admin));
+    }
     if (s.wfm_idx >= 0) {
         CK(cudaMemsetAsync(r->d_comp_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
         CK(cudaMemsetAsync(r->d_lr_dl + (size_t)s.wfm_idx * kWfmHist, 0, kWfmHist * 4, r->admin));
@@ -1505,7 +1560,7 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     out->signal_id = s.spec.signal_id;
     out->rate = s.spec.out_rate;
     out->audio_channels = s.spec.mode == GPUD_MODE_WFM_STEREO ? 2 : (s.spec.mode == GPUD_MODE_IQ ? 0 : 1);
-    out->rds_rate = s.spec.out_rate / std::max(1, s.spec.out_rate / 19000);
+    out->rds_rate = demod_rate(s) / std::max(1, demod_rate(s) / 19000);
     out->phase_count = s.pc;
     out->history_len = s.hist_len;
     if (r->done_frame < 0) {
@@ -1588,11 +1643,13 @@ struct SnapHeader {
     int64_t rds_count;
     double cutoff;
     int64_t rs_t;  // 48 kHz resampler phase counter
+    int32_t d1, d1_phase;  // pre-demod decimation and its phase counter
 };
 
 static uint64_t snap_bytes(const Slot &s) {
     uint64_t b = sizeof(SnapHeader) + sizeof(ChanState) + (uint64_t)s.hcap * 8 + sizeof(AudState);
     if (s.wfm_idx >= 0) b += kWfmHist * 4 * 2 + kAudioDlStrideH * 4 + kWfmHist * 8;
+    if (s.d1 > 1) b += kWfmHist * 8;
     return b;
 }
 
@@ -1610,8 +1667,8 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
     int rc = drain(r);
     if (rc) return rc;
     char *p = (char *)blob;
-    SnapHeader h{0x47505544u, 2, s.D, s.T, s.spec.mode, s.wfm_idx >= 0, s.pc, s.hist_len, s.hist_sel,
-                 s.comp_hist_len, s.has_last ? 1 : 0, 0, s.rds_count, s.cutoff, s.rs_t};
+    SnapHeader h{0x47505544u, 3, s.D, s.T, s.spec.mode, s.wfm_idx >= 0, s.pc, s.hist_len, s.hist_sel,
+                 s.comp_hist_len, s.has_last ? 1 : 0, 0, s.rds_count, s.cutoff, s.rs_t, s.d1, s.d1_phase};
     std::memcpy(p, &h, sizeof h);
     p += sizeof h;
     CK(cudaMemcpy(p, r->d_st + slot, sizeof(ChanState), cudaMemcpyDeviceToHost));
@@ -1632,6 +1689,10 @@ GPUD_API int GPUD_CALL gpud_runner_snapshot(gpud_runner *r, int slot, void *blob
         CK(cudaMemcpy(p, r->d_rds_dl + w * kWfmHist, kWfmHist * 8, cudaMemcpyDeviceToHost));
         p += kWfmHist * 8;
     }
+    if (s.d1 > 1) {
+        CK(cudaMemcpy(p, r->d_d1hist + (size_t)slot * kWfmHist, kWfmHist * 8, cudaMemcpyDeviceToHost));
+        p += kWfmHist * 8;
+    }
     *bytes = need;
     return 0;
 }
@@ -1646,7 +1707,8 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     SnapHeader h;
     std::memcpy(&h, p, sizeof h);
     p += sizeof h;
-    if (h.magic != 0x47505544u || h.version != 2 || h.D != s.D || h.T != s.T || h.mode != s.spec.mode || h.wfm != (s.wfm_idx >= 0))
+    if (h.magic != 0x47505544u || h.version != 3 || h.D != s.D || h.T != s.T || h.mode != s.spec.mode ||
+        h.wfm != (s.wfm_idx >= 0) || h.d1 != s.d1)
         return set_err(r, GPUD_E_STATE, "snapshot geometry mismatch");
     int rc = drain(r);
     if (rc) return rc;
@@ -1669,6 +1731,11 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
         CK(cudaMemcpy(r->d_rds_dl + w * kWfmHist, p, kWfmHist * 8, cudaMemcpyHostToDevice));
         p += kWfmHist * 8;
     }
+    if (s.d1 > 1) {
+        CK(cudaMemcpy(r->d_d1hist + (size_t)slot * kWfmHist, p, kWfmHist * 8, cudaMemcpyHostToDevice));
+        p += kWfmHist * 8;
+    }
+    s.d1_phase = h.d1_phase;
     s.pc = h.pc;
     s.hist_len = h.hist_len;
     s.comp_hist_len = h.comp_hist_len;

@@ -305,6 +305,38 @@ k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
 }
 
 // ===========================================================================
+// Pre-demod decimation (recorder/streamer.go:1098-1146 with
+// dsp/decimating_fir.go:56-95): 101-tap float64 low-pass, one output each
+// time the decimator's phase counter is 0 -- stream samples d1_phase + j*d1
+// of this block -- over the newest 101 extraction outputs (earlier blocks'
+// from the carried 100-sample history), float64 accumulate in the
+// reference's order, complex64 output.
+// ===========================================================================
+constexpr int kDecOT = 256;
+
+__global__ void __launch_bounds__(kDecOT)
+k_decim2(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+         const double *__restrict__ d1taps, const float2 *__restrict__ d1hist, float2 *__restrict__ ext) {
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int j = w.y * kDecOT + (int)threadIdx.x;
+    if (j >= sb.n_dem) return;
+    const ChanParams &cp = prm[sb.slot];
+    const double *h = d1taps + (int64_t)sb.slot * kD1Taps;
+    const float2 *hist = d1hist + (int64_t)sb.slot * kWfmHist;  // oldest first
+    const float2 *x = ext + sb.ext_off;
+    const int i = sb.d1_phase + j * cp.d1;
+    double ar = 0.0, ai = 0.0;
+    for (int k = 0; k < kD1Taps; ++k) {
+        const int q = i - k;
+        const float2 v = q >= 0 ? x[q] : hist[kWfmHist + q];
+        ar = __dadd_rn(ar, __dmul_rn((double)v.x, h[k]));
+        ai = __dadd_rn(ai, __dmul_rn((double)v.y, h[k]));
+    }
+    ext[sb.dem_off + j] = make_float2((float)ar, (float)ai);
+}
+
+// ===========================================================================
 // Demodulators (internal/demod/*.go; bridge per recorder/streamer.go:1287-1302)
 // ===========================================================================
 constexpr int kDemodOT = 1024;
@@ -317,7 +349,7 @@ k_demod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const 
     const SlotBlock sb = sbt[w.x];
     const ChanParams &cp = prm[sb.slot];
     const int q0 = w.y * kDemodOT;
-    const float2 *iq = ext + sb.ext_off;
+    const float2 *iq = ext + sb.dem_off;
     const int mode = cp.mode;
     if (mode == 1 || mode == 2 || mode == 3) {  // NFM / WFM / WFM_STEREO: fmDiscrimInto (fm.go:179-196)
         const float2 last = st[sb.slot].last_iq;
@@ -337,7 +369,7 @@ k_demod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const 
         }
     } else if (mode == 5 || mode == 6 || mode == 7) {  // ssb.go:19-39, cw.go:11-26
         float *dst = audio + sb.audio_off;
-        for (int q = q0 + threadIdx.x; q < q0 + kDemodOT && q < sb.n_out; q += blockDim.x) {
+        for (int q = q0 + threadIdx.x; q < q0 + kDemodOT && q < sb.n_dem; q += blockDim.x) {
             double ph = (double)(q + 1) * cp.ssb_inc;
             double s, c;
             sincos(ph, &s, &c);
@@ -353,18 +385,18 @@ k_am(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const flo
      float *__restrict__ audio) {
     __shared__ double red[256];
     const SlotBlock sb = sbt[work[blockIdx.x].x];
-    const float2 *iq = ext + sb.ext_off;
+    const float2 *iq = ext + sb.dem_off;
     double acc = 0.0;
-    for (int q = threadIdx.x; q < sb.n_out; q += 256) acc += hypot((double)iq[q].x, (double)iq[q].y);
+    for (int q = threadIdx.x; q < sb.n_dem; q += 256) acc += hypot((double)iq[q].x, (double)iq[q].y);
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int s = 128; s > 0; s >>= 1) {
         if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
         __syncthreads();
     }
-    const float mean = (float)(red[0] / (double)sb.n_out);
+    const float mean = (float)(red[0] / (double)sb.n_dem);
     float *dst = audio + sb.audio_off;
-    for (int q = threadIdx.x; q < sb.n_out; q += 256) {
+    for (int q = threadIdx.x; q < sb.n_dem; q += 256) {
         float mag = (float)hypot((double)iq[q].x, (double)iq[q].y);
         dst[q] = mag - mean;
     }
@@ -1285,10 +1317,22 @@ __global__ void __launch_bounds__(128)
 k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
              const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, const float2 *__restrict__ ext,
              const float *__restrict__ wk, float *__restrict__ comp_dl, float2 *__restrict__ rds_dl,
-             const BinadeTable *__restrict__ tabs, DevResult *__restrict__ res) {
+             const BinadeTable *__restrict__ tabs, float2 *__restrict__ d1hist, DevResult *__restrict__ res) {
     const SlotBlock sb = sbt[blockIdx.x];
     const ChanParams &cp = prm[sb.slot];
     ChanState &s = st[sb.slot];
+    if (cp.d1 > 1 && sb.n_out > 0) {
+        // pre-demod decimator history: the last 100 extraction outputs
+        __shared__ float2 dtmp[kWfmHist];
+        float2 *dh = d1hist + (int64_t)sb.slot * kWfmHist;
+        for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) {
+            const int g = sb.n_out + i - kWfmHist;
+            dtmp[i] = g >= 0 ? ext[sb.ext_off + g] : dh[kWfmHist + g];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) dh[i] = dtmp[i];
+        __syncthreads();
+    }
     const uint64_t u0 = s.nco_q;
     // extraction history: last min(T-1, H+n) samples of (history ++ shifted block)
     {
@@ -1333,8 +1377,8 @@ k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ p
     }
     if (threadIdx.x == 0) {
         s.nco_q = u0 + (uint64_t)n * cp.inc_q;
-        if (sb.n_out > 0) {
-            s.last_iq = ext[sb.ext_off + sb.n_out - 1];
+        if (sb.n_dem > 0) {
+            s.last_iq = ext[sb.dem_off + sb.n_dem - 1];
             s.has_last = 1;
         }
         if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
@@ -1654,10 +1698,18 @@ cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, co
     return cudaGetLastError();
 }
 
+cudaError_t launch_decim2(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                          const double *d1taps, const float2 *d1hist, float2 *ext) {
+    k_decim2<<<grid, kDecOT, 0, sm>>>(work, sbt, prm, d1taps, d1hist, ext);
+    return cudaGetLastError();
+}
+
+int decim2_tile() { return kDecOT; }
+
 cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                               const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
-                              float2 *rds_dl, const BinadeTable *tabs, DevResult *res) {
-    k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, comp_dl, rds_dl, tabs, res);
+                              float2 *rds_dl, const BinadeTable *tabs, float2 *d1hist, DevResult *res) {
+    k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, comp_dl, rds_dl, tabs, d1hist, res);
     return cudaGetLastError();
 }
 

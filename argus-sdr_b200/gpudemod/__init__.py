@@ -107,9 +107,10 @@ def _check(r, rc: int):
         raise GPUDError(rc, msg)
 
 
-def _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash=0, mode=MODE_IQ, flags=0) -> ChannelSpec:
+def _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash=0, mode=MODE_IQ, flags=0,
+          demod_decim=1) -> ChannelSpec:
     return ChannelSpec(int(signal_id), float(offset_hz), float(bandwidth), int(out_rate), int(num_taps),
-                       int(config_hash) & ((1 << 64) - 1), int(mode), int(flags))
+                       int(config_hash) & ((1 << 64) - 1), int(mode), int(flags), int(demod_decim), 0)
 
 
 def _iq_ptr(iq):
@@ -156,15 +157,18 @@ class ChannelRunner:
             pass
 
     def admit(self, signal_id, offset_hz, bandwidth, out_rate, num_taps=101, mode=MODE_IQ, flags=0,
-              config_hash=0) -> int:
+              config_hash=0, demod_decim=1) -> int:
+        """Admits a channel.  demod_decim > 1 adds the pre-demod decimating
+        low-pass (recorder/streamer.go:1098-1146): extraction runs at
+        out_rate, the demodulator at out_rate // demod_decim."""
         slot = C.c_int()
-        spec = _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash, mode, flags)
+        spec = _spec(signal_id, offset_hz, bandwidth, out_rate, num_taps, config_hash, mode, flags, demod_decim)
         _check(self._r, lib.gpud_runner_admit(self._r, C.byref(spec), C.byref(slot)))
         return slot.value
 
-    def footprint(self, out_rate, mode=MODE_IQ, flags=0, num_taps=101) -> int:
+    def footprint(self, out_rate, mode=MODE_IQ, flags=0, num_taps=101, demod_decim=1) -> int:
         b = C.c_uint64()
-        spec = _spec(0, 0, 0, out_rate, num_taps, 0, mode, flags)
+        spec = _spec(0, 0, 0, out_rate, num_taps, 0, mode, flags, demod_decim)
         _check(self._r, lib.gpud_runner_channel_footprint(self._r, C.byref(spec), C.byref(b)))
         return b.value
 

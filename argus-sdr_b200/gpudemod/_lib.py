@@ -30,6 +30,8 @@ class ChannelSpec(C.Structure):
         ("config_hash", C.c_uint64),
         ("mode", C.c_int32),
         ("flags", C.c_int32),
+        ("demod_decim", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

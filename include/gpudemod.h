@@ -194,6 +194,13 @@ typedef struct {
     uint64_t config_hash;
     int32_t mode;  /* GPUD_MODE_* */
     int32_t flags; /* GPUD_CH_* */
+    /* pre-demod decimation (recorder/streamer.go:1098-1146): > 1 puts the
+     * stateful 101-tap decimating low-pass of dsp/decimating_fir.go (cutoff
+     * 90 kHz for WFM modes, else 0.8 x the demod Nyquist) between the
+     * extraction at out_rate and the demodulator, which then runs at
+     * out_rate / demod_decim; 0 or 1: none. */
+    int32_t demod_decim;
+    int32_t reserved;
 } gpud_channel_spec;
 
 /* Per-channel result of the last processed block.  The pointers reference

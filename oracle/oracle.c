@@ -1025,8 +1025,60 @@ enum {
     OR_MODE_CW = 7
 };
 
+/* internal/dsp/decimating_fir.go:6-95 StatefulDecimatingFIRComplex: float64
+ * delay line (delay[0] newest), emit when the phase counter is 0 (then it
+ * restarts at factor-1), float64 accumulate, complex64 output. */
+typedef struct {
+    int n, factor, phase;
+    double taps[128];
+    double dr[128], di[128];
+} or_decim_fir;
+
+static void decim_fir_init(or_decim_fir *f, const double *taps, int n, int factor) {
+    memset(f, 0, sizeof *f);
+    f->n = n;
+    f->factor = factor < 1 ? 1 : factor;
+    memcpy(f->taps, taps, sizeof(double) * (size_t)n);
+}
+
+static int decim_fir_process(or_decim_fir *f, const cf32 *iq, int len, cf32 *out) {
+    int n = f->n, nout = 0;
+    if (len == 0 || n == 0) return 0;
+    for (int i = 0; i < len; i++) {
+        memmove(f->dr + 1, f->dr, sizeof(double) * (size_t)(n - 1));
+        memmove(f->di + 1, f->di, sizeof(double) * (size_t)(n - 1));
+        f->dr[0] = (double)iq[i].re;
+        f->di[0] = (double)iq[i].im;
+        if (f->factor <= 1 || f->phase == 0) {
+            double ar = 0, ai = 0;
+            for (int k = 0; k < n; k++) {
+                ar += f->dr[k] * f->taps[k];
+                ai += f->di[k] * f->taps[k];
+            }
+            out[nout].re = (float)ar;
+            out[nout].im = (float)ai;
+            nout++;
+            if (f->factor > 1) f->phase = f->factor - 1;
+        } else {
+            f->phase--;
+        }
+    }
+    return nout;
+}
+
+size_t or_decim_fir_size(void) { return sizeof(or_decim_fir); }
+int or_decim_fir_init(or_decim_fir *f, const double *taps, int n, int factor) {
+    if (n < 1 || n > 128) return -1;
+    decim_fir_init(f, taps, n, factor);
+    return 0;
+}
+int or_decim_fir_process(or_decim_fir *f, const cf32 *iq, int len, cf32 *out) { return decim_fir_process(f, iq, len, out); }
+int or_decim_fir_phase(const or_decim_fir *f) { return f->phase; }
+
 typedef struct {
     int sample_rate, out_rate, num_taps, decim, mode, rds_on;
+    int demod_decim, demod_rate;
+    or_decim_fir pre;
     double offset_hz;
     double nco_phase;
     int phase_count;
@@ -1067,6 +1119,26 @@ int or_channel_init(or_channel *ch, int sample_rate, double offset_hz, double ba
     ch->poly_len = or_build_polyphase(basef, blen, D, ch->poly);
     or_stereo_init(&ch->st);
     or_rds_init(&ch->rds, out_rate);
+    ch->demod_decim = 1;
+    ch->demod_rate = out_rate;
+    return 0;
+}
+
+/* recorder/streamer.go:1098-1146: the stateful anti-alias FIR + decimation
+ * by decim1 ahead of the demodulator: 101 taps of LowpassFIR(cutoff, snip
+ * rate), cutoff 90 kHz for WFM modes, else 0.8 x the demod Nyquist.  The demod
+ * stages then run at out_rate / decim1. */
+int or_channel_set_demod_decim(or_channel *ch, int decim1) {
+    if (decim1 <= 1) return 0;
+    int drate = ch->out_rate / decim1;
+    int wfm = ch->mode == OR_MODE_WFM || ch->mode == OR_MODE_WFM_STEREO;
+    double cutoff = wfm ? 90000.0 : (double)drate / 2.0 * 0.8;
+    double taps[128];
+    int n = or_lowpass_fir(cutoff, ch->out_rate, 101, taps);
+    decim_fir_init(&ch->pre, taps, n, decim1);
+    ch->demod_decim = decim1;
+    ch->demod_rate = drate;
+    or_rds_init(&ch->rds, drate);
     return 0;
 }
 
@@ -1082,7 +1154,15 @@ int or_channel_process(or_channel *ch, const cf32 *in, int n, cf32 *iq_out, int 
     *n_audio = 0;
     *n_rds = 0;
     *flags = 0;
-    int rate = ch->out_rate;
+    int rate = ch->demod_rate;
+    cf32 *dec = NULL;
+    if (ch->demod_decim > 1) {
+        /* the demodulator sees the decimated stream; iq_out keeps the extraction output */
+        dec = (cf32 *)malloc(sizeof(cf32) * (size_t)(nout + 2));
+        int nd = decim_fir_process(&ch->pre, iq_out, nout, dec);
+        nout = nd;
+    }
+    const cf32 *dq = dec ? dec : iq_out;
     switch (ch->mode) {
     case OR_MODE_NFM:
     case OR_MODE_WFM:
@@ -1092,14 +1172,14 @@ int or_channel_process(or_channel *ch, const cf32 *in, int n, cf32 *iq_out, int 
         if (ch->has_last && nout > 0) {
             cf32 *br = (cf32 *)malloc(sizeof(cf32) * (size_t)(nout + 1));
             br[0] = ch->last_iq;
-            memcpy(br + 1, iq_out, sizeof(cf32) * (size_t)nout);
+            memcpy(br + 1, dq, sizeof(cf32) * (size_t)nout);
             nd = or_fm_discrim(br, nout + 1, disc);
             free(br);
         } else {
-            nd = or_fm_discrim(iq_out, nout, disc);
+            nd = or_fm_discrim(dq, nout, disc);
         }
         if (nout > 0) {
-            ch->last_iq = iq_out[nout - 1];
+            ch->last_iq = dq[nout - 1];
             ch->has_last = 1;
         }
         if (nd > 0) {
@@ -1120,20 +1200,21 @@ int or_channel_process(or_channel *ch, const cf32 *in, int n, cf32 *iq_out, int 
         break;
     }
     case OR_MODE_AM:
-        *n_audio = or_am_demod(iq_out, nout, audio);
+        *n_audio = or_am_demod(dq, nout, audio);
         break;
     case OR_MODE_USB:
-        *n_audio = or_ssb_demod(iq_out, nout, rate, 1, audio);
+        *n_audio = or_ssb_demod(dq, nout, rate, 1, audio);
         break;
     case OR_MODE_LSB:
-        *n_audio = or_ssb_demod(iq_out, nout, rate, 0, audio);
+        *n_audio = or_ssb_demod(dq, nout, rate, 0, audio);
         break;
     case OR_MODE_CW:
-        *n_audio = or_cw_demod(iq_out, nout, rate, audio);
+        *n_audio = or_cw_demod(dq, nout, rate, audio);
         break;
     default:
         break;
     }
+    free(dec);
     return 0;
 }
 

@@ -70,6 +70,11 @@ def _load() -> C.CDLL:
         "or_channel_state": (None, [P, P, P, P]),
         "or_channel_stereo_margins": (None, [P, P, P, P]),
         "or_channel_set_offset": (None, [P, d]),
+        "or_channel_set_demod_decim": (i, [P, i]),
+        "or_decim_fir_size": (C.c_size_t, []),
+        "or_decim_fir_init": (i, [P, P, i, i]),
+        "or_decim_fir_process": (i, [P, P, i, P]),
+        "or_decim_fir_phase": (i, [P]),
         "or_resampler_size": (C.c_size_t, []),
         "or_resampler_init": (i, [P, i, i, i]),
         "or_resampler_ratio": (None, [P, P, P, P, P]),
@@ -387,18 +392,41 @@ class RDSDecoder:
 # per-channel block pipeline
 # --------------------------------------------------------------------------
 
+class DecimatingFIR:
+    """StatefulDecimatingFIRComplex (dsp/decimating_fir.go:6-95): float64
+    delay line and accumulation, one output whenever the phase counter is 0."""
+
+    def __init__(self, taps, factor):
+        t = np.ascontiguousarray(taps, dtype=np.float64)
+        self._buf = C.create_string_buffer(_lib.or_decim_fir_size())
+        if _lib.or_decim_fir_init(self._buf, t.ctypes.data, t.size, int(factor)) != 0:
+            raise ValueError("1..128 taps")
+        self.factor = max(1, int(factor))
+
+    @property
+    def phase(self):
+        return _lib.or_decim_fir_phase(self._buf)
+
+    def process(self, iq):
+        x = _c64(iq)
+        out = np.zeros(x.size + 1, np.complex64)
+        n = _lib.or_decim_fir_process(self._buf, x.ctypes.data, x.size, out.ctypes.data)
+        return out[:n]
+
+
 class OracleChannel:
     """One channel's block-by-block chain (extract -> demod -> stereo -> RDS),
     see or_channel_process in oracle.c."""
 
-    def __init__(self, sample_rate, offset_hz, bandwidth, out_rate, num_taps, mode, rds=True):
+    def __init__(self, sample_rate, offset_hz, bandwidth, out_rate, num_taps, mode, rds=True, demod_decim=1):
         self._buf = C.create_string_buffer(_lib.or_channel_size())
         rc = _lib.or_channel_init(self._buf, int(sample_rate), float(offset_hz), float(bandwidth),
                                   int(out_rate), int(num_taps), int(mode), 1 if rds else 0)
         if rc != 0:
             raise ValueError("non-integer decimation")
+        _lib.or_channel_set_demod_decim(self._buf, int(demod_decim))
         self.decim = sample_rate // out_rate
-        self.out_rate = out_rate
+        self.out_rate = out_rate // max(1, int(demod_decim))
 
     def process(self, block):
         x = _c64(block)

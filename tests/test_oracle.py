@@ -378,3 +378,65 @@ def test_wfm_pilot_detection_kat():
     noise = (rng.standard_normal(fs) + 1j * rng.standard_normal(fs)).astype(np.complex64)
     assert not O.stereo_pilot(noise, fs)[0]
     assert not O.stereo_pilot(iq, 32_000)[0]  # below 40 kS/s: no decision
+
+
+def _decim_input(n, a, b):
+    i = np.arange(n)
+    return (((i % a) - (a // 2)) / 8.0 + 1j * ((i % b) - (b // 2)) / 8.0).astype(np.complex64)
+
+
+def test_decimating_fir_stream_continuity():
+    """dsp/decimating_fir_test.go:8-38: chunks of 733 equal one call."""
+    taps = O.lowpass_fir(90000, 512000, 101)
+    x = _decim_input(8192, 17, 11)
+    whole = O.DecimatingFIR(taps, 2).process(x)
+    d = O.DecimatingFIR(taps, 2)
+    chunked = np.concatenate([d.process(x[i:i + 733]) for i in range(0, x.size, 733)])
+    assert whole.size == chunked.size == 4096
+    assert np.array_equal(whole, chunked)
+
+
+def test_decimating_fir_equals_filter_then_decimate():
+    """dsp/decimating_fir_test.go:40-58: length of ApplyFIR + Decimate; with a
+    zero start the stateful stage is that pipeline sample for sample."""
+    taps = O.lowpass_fir(90000, 512000, 101)
+    x = _decim_input(48640, 13, 7)
+    for factor in (2, 3):
+        out = O.DecimatingFIR(taps, factor).process(x)
+        xr, xi = x.real.astype(np.float64), x.imag.astype(np.float64)
+        fr = np.convolve(xr, taps)[: x.size]
+        fi = np.convolve(xi, taps)[: x.size]
+        want = (fr[::factor].astype(np.float32) + 1j * fi[::factor].astype(np.float32)).astype(np.complex64)
+        assert out.size == len(range(0, x.size, factor))
+        # numpy's convolution sums in another order: a float32 rounding apart
+        assert np.max(np.abs(out - want)) <= 1e-6
+
+
+def test_decimating_fir_phase_carry():
+    """The phase counter carried across calls: after n inputs from phase p the
+    emitted count is ceil((n - p) / factor) and the new phase (p - n) mod factor."""
+    taps = O.lowpass_fir(90000, 512000, 101)
+    d = O.DecimatingFIR(taps, 3)
+    p = 0
+    for n in (1, 2, 5, 7, 100, 3, 4):
+        out = d.process(_decim_input(n, 5, 3))
+        want = (n - 1 - p) // 3 + 1 if n > p else 0
+        assert out.size == want
+        p = (p - n) % 3
+        assert d.phase == p
+
+
+def test_channel_demod_decim_halves_the_demod_rate():
+    """recorder/streamer.go:1098-1146: WFM at 512 kS/s extraction, decim1 2,
+    demodulator and stereo decoder at 256 kS/s."""
+    fs, rate = 2_048_000, 512_000
+    t = np.arange(1 << 16) / fs
+    x = np.exp(2j * np.pi * 300e3 * t).astype(np.complex64)
+    a = O.OracleChannel(fs, 300e3, 250e3, rate, 64, O.MODE_WFM_STEREO, rds=False, demod_decim=2)
+    b = O.OracleChannel(fs, 300e3, 250e3, rate, 64, O.MODE_WFM_STEREO, rds=False)
+    ra, rb = a.process(x), b.process(x)
+    assert ra["iq"].size == rb["iq"].size == x.size // 4
+    # first block: no discriminator bridge, one sample fewer at each rate
+    assert ra["audio"].size == 2 * (ra["iq"].size // 2 - 1)
+    assert rb["audio"].size == 2 * (rb["iq"].size - 1)
+    assert a.out_rate == 256_000
