@@ -86,7 +86,7 @@ struct ChanParams {
     int32_t rds_tab;                       // binade table id for the RDS phase
     int32_t aud_ch;                        // audio channels (2 for WFM_STEREO, else 1)
     int32_t d1;                            // pre-demod decimation (1: none)
-    int32_t pad2;
+    int32_t precise_sum;                   // 1: extraction rows summed in float32, rows added in float64
     double deemph_a;                       // de-emphasis coefficient exp(-1/(48000 tau)), 0: none
 };
 
@@ -135,6 +135,11 @@ struct SlotBlock {
     int32_t dem_off;   // float2 offset of the demod input in the IQ region
     int32_t n_dem;     // demod input samples this block
     int32_t d1_phase;  // pre-demod decimator phase before the block
+    // phase-grouped extraction: ng groups of pg phases; partial sums at
+    // part_off (float2) when ng > 1
+    int32_t ng;
+    int32_t pg;
+    int32_t part_off;
     int32_t pad_sb;
 };
 

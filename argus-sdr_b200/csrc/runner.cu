@@ -75,6 +75,16 @@ int rds_tile();
 int dense_smem_bytes_host(int P, int L);
 int dense_tile();
 int wide_smem_bytes_host(int T);
+int group_smem_bytes_host(int Pc, int L);
+int mod_smem_bytes_host(int Pc, int L);
+cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                 const float2 *hist, const float *taps, float2 *ext, void *part);
+cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                               const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                               const float2 *hist, const float *taps, float2 *ext, void *part);
+cudaError_t launch_group_sum(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                             const ChanParams *prm, const void *part, float2 *ext);
 
 constexpr int kWfmTapsPadH = 104;
 struct WfmTapsHost {
@@ -85,6 +95,9 @@ constexpr int kAudioDlStrideH = kWfmHist + 4;
 constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
+constexpr int kGroupSmemTarget = 100 * 1024;  // two CTAs per SM
+constexpr int kModSmemTarget = 72 * 1024;     // three CTAs per SM
+constexpr int kModMaxL = 4;
 constexpr int kPllMaxIters = 64;
 constexpr int kFrames = 3;  // blocks in flight
 constexpr int kMaxRsClasses = 16;  // 48 kHz resampler banks (one per demod rate)
@@ -172,7 +185,8 @@ struct Slot {
     uint64_t reusable_after = 0;  // a retired slot is reused once this ticket completed
     gpud_channel_spec spec{};
     int D = 1, T = 1, P = 1, L = 1, hcap = 0;
-    int ext_kind = 0;  // 0 dense, 1 wide
+    int ext_kind = 0;  // 0 dense (all D phases of a tile), 1 wide, 2 phase groups, 3 modulated short arms
+    int pg = 0, ng = 1;  // phase groups: ng groups of at most pg phases
     int taps_off = 0, dtaps_off = 0, hist_off = 0, wfm_idx = -1, rate_class = -1;
     double cutoff = 0;
     // host mirrors of device integer state (as of the last submitted block)
@@ -193,6 +207,11 @@ struct BlockPlan {
     int dense_smem[kDenseMaxL + 1] = {};
     std::vector<int2> w_wide;
     int wide_smem = 0;
+    std::vector<int2> w_group, w_gsum;  // (entry, tile*ng + group), (entry, 256-output tile)
+    int group_smem = 0;
+    std::vector<int2> w_mod;            // (entry, tile*ng + group) of the modulated short-arm form
+    int mod_smem = 0;
+    int64_t tot_part = 0;               // double2 slots of partial sums of multi-group channels
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
@@ -230,6 +249,8 @@ struct Frame {
     float2 *h_in = nullptr;
     float *d_rs = nullptr;  // resampled 48 kHz audio before de-emphasis
     int64_t rs_cap = 0;
+    double2 *d_part = nullptr;  // phase-group partial sums (double2 slots)
+    int64_t part_cap = 0;
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
@@ -510,6 +531,15 @@ static void design_taps(gpud_runner *r, const Slot &s, double bandwidth, std::ve
 // Rate of the demodulator and everything after it.
 static int demod_rate(const Slot &s) { return s.spec.out_rate / std::max(1, s.d1); }
 
+// FM discriminators on an oversampled channel (output rate well above the
+// signal bandwidth) see consecutive samples that differ little, and magnify
+// the white rounding error of each extraction output; such channels add the
+// float32 sums of the polyphase rows in float64.
+static bool precise_sum(const gpud_channel_spec &sp) {
+    bool fm = sp.mode == GPUD_MODE_NFM || sp.mode == GPUD_MODE_WFM || sp.mode == GPUD_MODE_WFM_STEREO;
+    return fm && (double)sp.out_rate >= 4.0 * std::max(sp.bandwidth, 400.0);
+}
+
 static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     Slot &s = r->slots[(size_t)slot];
     std::memset(p, 0, sizeof *p);
@@ -522,6 +552,7 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     p->plen = s.L;
     p->mode = s.spec.mode;
     p->flags = s.spec.flags;
+    p->precise_sum = precise_sum(s.spec) ? 1 : 0;
     p->out_rate = demod_rate(s);
     p->taps_off = s.taps_off;
     p->dtaps_off = s.dtaps_off;
@@ -647,6 +678,8 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
     // demodulator input: the extraction output, or the samples the pre-demod
     // decimator emits (those with phase counter 0: d1_phase + j*d1)
     sb.d1_phase = s.d1_phase;
+    sb.ng = s.ng;
+    sb.pg = s.pg;
     sb.n_dem = sb.n_out;
     if (s.d1 > 1) sb.n_dem = sb.n_out > s.d1_phase ? (sb.n_out - 1 - s.d1_phase) / s.d1 + 1 : 0;
     int mode = s.spec.mode;
@@ -753,6 +786,12 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     }
     pl.w_wide.clear();
     pl.wide_smem = 0;
+    pl.w_group.clear();
+    pl.w_gsum.clear();
+    pl.group_smem = 0;
+    pl.w_mod.clear();
+    pl.mod_smem = 0;
+    pl.tot_part = 0;
     pl.w_demod.clear();
     pl.w_am.clear();
     pl.w_fir.clear();
@@ -767,6 +806,19 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             if (s.ext_kind == 0) {
                 for (int t = 0; t * dense_tile() < sb.n_out; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
                 pl.dense_smem[s.L] = std::max(pl.dense_smem[s.L], dense_smem_bytes_host(s.P, s.L));
+            } else if (s.ext_kind == 2 || s.ext_kind == 3) {
+                auto &wl = s.ext_kind == 2 ? pl.w_group : pl.w_mod;
+                for (int t = 0; t * dense_tile() < sb.n_out; ++t)
+                    for (int g = 0; g < s.ng; ++g) wl.push_back(make_int2(i, t * s.ng + g));
+                if (s.ext_kind == 2)
+                    pl.group_smem = std::max(pl.group_smem, group_smem_bytes_host(s.pg, s.L));
+                else
+                    pl.mod_smem = std::max(pl.mod_smem, mod_smem_bytes_host(s.pg, s.L));
+                if (s.ng > 1) {
+                    pl.sbs[(size_t)i].part_off = (int)pl.tot_part;
+                    pl.tot_part += ((int64_t)s.ng * sb.n_out + 31) & ~31;
+                    for (int t = 0; t * 256 < sb.n_out; ++t) pl.w_gsum.push_back(make_int2(i, t));
+                }
             } else {
                 for (int t = 0; t * 32 < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));
                 pl.wide_smem = std::max(pl.wide_smem, wide_smem_bytes_host(s.T));
@@ -802,6 +854,13 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         f.wk_cap = cap;
         r->graph_rebuilds++;
     }
+    if (pl.tot_part > f.part_cap) {
+        cudaFree(f.d_part);
+        f.d_part = nullptr;
+        int64_t cap = std::max<int64_t>(pl.tot_part * 5 / 4, 1 << 16);
+        CK(dalloc(&f.d_part, (size_t)cap));
+        f.part_cap = cap;
+    }
     if (pl.tot_pcm > f.rs_cap) {
         cudaFree(f.d_rs);
         f.d_rs = nullptr;
@@ -826,7 +885,8 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
-          pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size();
+          pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() + pl.w_gsum.size() +
+          pl.w_mod.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
@@ -921,7 +981,8 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         return at;
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
-           o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec);
+           o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec),
+           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
@@ -955,6 +1016,23 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                                 : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
         CK(launch_extract_dense(L, (int)pl.w_dense[L].size(), pl.dense_smem[L], f.s, d_w + w_dense_off[L], d_sb,
                                 r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
+        nl++;
+    }
+    if (!pl.w_group.empty()) {
+        prof_mark(r, f, "extract_group");
+        CK(launch_extract_group((int)pl.w_group.size(), pl.group_smem, f.s, d_w + o_grp, d_sb, r->d_prm, r->d_st,
+                                x_dev, n, r->d_hist, r->d_taps, d_ext, f.d_part));
+        nl++;
+    }
+    if (!pl.w_mod.empty()) {
+        prof_mark(r, f, "extract_mod");
+        CK(launch_extract_mod((int)pl.w_mod.size(), pl.mod_smem, f.s, d_w + o_mod, d_sb, r->d_prm, r->d_st, x_dev,
+                              n, r->d_hist, r->d_taps, d_ext, f.d_part));
+        nl++;
+    }
+    if (!pl.w_gsum.empty()) {
+        prof_mark(r, f, "group_sum");
+        CK(launch_group_sum((int)pl.w_gsum.size(), f.s, d_w + o_gsum, d_sb, r->d_prm, f.d_part, d_ext));
         nl++;
     }
     if (!pl.w_wide.empty()) {
@@ -1295,6 +1373,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_wk);
         cudaFree(f.d_block);
         cudaFree(f.d_rs);
+        cudaFree(f.d_part);
         if (f.h_desc) cudaFreeHost(f.h_desc);
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);
@@ -1348,6 +1427,38 @@ GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_
     if (rc) return rc;
     *bytes = slot_block_bytes(r, D, spec->mode, spec->flags);
     return 0;
+}
+
+// Extraction form of a channel: arms of at most 4 taps in the modulated-taps
+// form (phase groups of raw samples); else the dense kernel when all D phases
+// of a 256-output tile fit in shared memory (L <= 16); else phase groups of
+// at most pg phases each (large D, long arms); else the wide kernel.
+static void choose_extraction(Slot &s) {
+    s.ng = 1;
+    s.pg = s.P;
+    const bool mod = s.L <= kModMaxL;
+    if (!mod && s.L <= kDenseMaxL && dense_smem_bytes_host(s.P, s.L) <= kDenseSmemLimit) {
+        s.ext_kind = 0;
+        return;
+    }
+    int pmax = 0;
+    for (int lo = 1, hi = s.P; lo <= hi;) {  // largest group within the shared-memory target
+        int mid = (lo + hi) / 2;
+        if (mod ? mod_smem_bytes_host(mid, s.L) <= kModSmemTarget
+                : group_smem_bytes_host(mid, s.L) <= kGroupSmemTarget) {
+            pmax = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    if (pmax == 0) {
+        s.ext_kind = 1;
+        return;
+    }
+    s.ext_kind = mod ? 3 : 2;
+    s.ng = (s.P + pmax - 1) / pmax;
+    s.pg = (s.P + s.ng - 1) / s.ng;
 }
 
 GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out) {
@@ -1413,8 +1524,7 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
         s.rs_L = r->rs_lmk[(size_t)rsclass].x;
         s.rs_M = r->rs_lmk[(size_t)rsclass].y;
     }
-    int smem = dense_smem_bytes_host(s.P, s.L);
-    s.ext_kind = (s.L >= 2 && s.L <= kDenseMaxL && smem <= kDenseSmemLimit) ? 0 : 1;
+    choose_extraction(s);
     s.footprint = fp;
     // The slot's memory is unused by every block in flight: write it now.
     std::vector<float> pm, h;
@@ -1486,8 +1596,9 @@ GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offse
         queue_write(r, slot, r->d_taps + s.taps_off, pm.data(), pm.size() * 4);
         queue_write(r, slot, r->d_taps + s.dtaps_off, h.data(), h.size() * 4);
     }
+    bool was_precise = precise_sum(s.spec);
     s.spec.bandwidth = bandwidth;
-    if (offset_hz != s.spec.offset_hz) {
+    if (offset_hz != s.spec.offset_hz || precise_sum(s.spec) != was_precise) {
         s.spec.offset_hz = offset_hz;
         ChanParams p;
         fill_params(r, slot, &p);

@@ -49,32 +49,219 @@ __host__ __device__ inline int dense_row_stride(int L) {
     return (M + (M >> 3) + 1) | 1;
 }
 
-__device__ __forceinline__ float2 shifted_sample(int i, int n, const float2 *__restrict__ x, uint64_t u0,
-                                                 uint64_t inc, const float2 *__restrict__ hist, int H) {
-    if (i >= 0) {
-        if (i >= n) return make_float2(0.f, 0.f);
-        return cmulf(__ldg(x + i), q64_phasor(u0 + (uint64_t)i * inc));
-    }
-    int hi = H + i;
-    return hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
-}
-
 // Rotation table entries: one per 256-sample staging round.
 __host__ __device__ inline int dense_rounds(int P, int L) { return (P * (kDenseOT + L - 1) + kDenseThreads - 1) / kDenseThreads; }
 
-// Shared memory: Z (reused for the cross-warp reduction) | taps | rotation table.
+// Shared memory: Z (reused for the cross-warp reduction) | taps | rotation
+// table.
 __host__ __device__ inline int dense_zbytes(int P, int L) {
-    int z = P * dense_row_stride(L) * 8;
-    int red = 8 * (kDenseOT + kDenseOT / 8) * 8;
+    int z = (P * dense_row_stride(L) * 8 + 15) & ~15;
+    int red = 8 * (kDenseOT + kDenseOT / 8) * 16;  // float64 reduction of precise channels
     return z > red ? z : red;
 }
 
 __host__ __device__ inline int dense_smem_bytes(int P, int L) {
-    return dense_zbytes(P, L) + ((P * L + 1) & ~1) * 4 + dense_rounds(P, L) * 8 + 16;
+    return dense_zbytes(P, L) + ((P * L + 3) & ~3) * 4 + dense_rounds(P, L) * 8 + 16;
+}
+
+// Rotation of tile sample i' = t + 256k: exp(j phi(ibase + t)) * exp(j 256 k inc).
+struct RotPair {
+    float2 a;
+    const float2 *tab;
+    __device__ __forceinline__ float2 operator()(int k) const { return cmulf(a, tab[k]); }
+};
+
+__device__ __forceinline__ void dense_stage(float2 *Z, int Mp, int D, int total, int nk, int ibase, int n,
+                                            const float2 *__restrict__ x, const float2 *__restrict__ hist, int H,
+                                            const RotPair &rp) {
+    const int t = (int)threadIdx.x;
+    int mr = t / D, q = t - (t / D) * D;
+    const int dm = kDenseThreads / D, dq = kDenseThreads - dm * D;
+    const int nfull = total / kDenseThreads;  // rounds in which every thread has a sample
+    const bool interior = ibase >= 0 && ibase + total <= n;
+    constexpr int U = 4;
+    int k = 0;
+    if (interior) {
+        const float2 *xp = x + ibase + t;
+        for (; k + U <= nfull; k += U) {
+            float2 xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = __ldg(xp + (k + u) * kDenseThreads);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const float2 rot = rp(k + u);
+                Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = cmulf(xv[u], rot);
+                q += dq;
+                mr += dm;
+                if (q >= D) {
+                    q -= D;
+                    ++mr;
+                }
+            }
+        }
+    }
+    // remaining rounds, and every round of tiles at the block edges
+    for (; k < nk; ++k) {
+        const int ip = t + k * kDenseThreads;
+        if (ip < total) {
+            const int i = ibase + ip;
+            float2 v;
+            if (i >= 0) {
+                v = i < n ? cmulf(__ldg(x + i), rp(k)) : make_float2(0.f, 0.f);
+            } else {
+                const int hi = H + i;
+                v = hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
+            }
+            Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = v;
+        }
+        q += dq;
+        mr += dm;
+        if (q >= D) {
+            q -= D;
+            ++mr;
+        }
+    }
 }
 
 int dense_smem_bytes_host(int P, int L) { return dense_smem_bytes(P, L); }
 int dense_tile() { return kDenseOT; }
+
+// One phase row, L <= 16 taps: lane's R outputs from a window of R+L-1.
+template <int L>
+__device__ __forceinline__ void group_row(const float2 *zrow, const float *hrow, int lane, float *ar, float *ai) {
+    constexpr int R = kDenseR;
+    float2 win[R + L - 1];
+#pragma unroll
+    for (int tt = 0; tt < R + L - 1; ++tt) {
+        const int c = lane * R + tt;
+        win[tt] = zrow[c + (c >> 3)];
+    }
+    float h[L];
+#pragma unroll
+    for (int u = 0; u < L; ++u) h[u] = hrow[u];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+        for (int u = 0; u < L; ++u) {
+            const float2 z = win[r + L - 1 - u];
+            ar[r] = fmaf(h[u], z.x, ar[r]);
+            ai[r] = fmaf(h[u], z.y, ai[r]);
+        }
+    }
+}
+
+// One phase row, long arm (Le a multiple of 8 > 16): chunks of 8 taps with a
+// window of R+7 samples that slides 8 columns per chunk (8 new loads).
+__device__ __forceinline__ void group_row_long(const float2 *zrow, const float *hrow, int Le, int lane, float *ar,
+                                               float *ai) {
+    constexpr int R = kDenseR;
+    constexpr int W = R + 7;
+    float2 win[W];
+    int base = lane * R + Le - 8;  // chunk c: columns base - 8c + t
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+        const int c = base + t;
+        win[t] = zrow[c + (c >> 3)];
+    }
+    const int nc = Le >> 3;
+    for (int ch = 0; ch < nc; ++ch) {
+        const float4 h0 = *reinterpret_cast<const float4 *>(hrow + 8 * ch);
+        const float4 h1 = *reinterpret_cast<const float4 *>(hrow + 8 * ch + 4);
+        const float h[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                const float2 z = win[r + 7 - v];
+                ar[r] = fmaf(h[v], z.x, ar[r]);
+                ai[r] = fmaf(h[v], z.y, ai[r]);
+            }
+        }
+        if (ch + 1 < nc) {
+#pragma unroll
+            for (int t = W - 1; t >= 8; --t) win[t] = win[t - 8];
+            base -= 8;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int c = base + t;
+                win[t] = zrow[c + (c >> 3)];
+            }
+        }
+    }
+}
+
+// Sum of a tile: the rows pp = warp, warp+8, ... < rows accumulate into each
+// lane's R outputs, then the 8 warps' partial sums are reduced through shared
+// memory (Z reused) and out(o, sum) receives tile output o.  With PREC each
+// row is summed in float32 on its own and the rows are added in float64
+// (channels whose demodulator magnifies white output error: the float32
+// rounding then no longer grows with the running sum of the whole tile).
+constexpr int kRedStride = kDenseOT + kDenseOT / 8;
+constexpr int kRedBytes = 8 * kRedStride * 16;
+
+template <bool PREC, class Row, class Out>
+__device__ __forceinline__ void tile_sum(int rows, const Row &row, float2 *Z, const Out &out) {
+    constexpr int R = kDenseR;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if constexpr (!PREC) {
+        float ar[R], ai[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
+        for (int pp = warp; pp < rows; pp += 8) row(pp, lane, ar, ai);
+        __syncthreads();
+        float2 *red = Z + warp * kRedStride;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int o = lane * R + r;
+            red[o + (o >> 3)] = make_float2(ar[r], ai[r]);
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < kDenseOT; o += kDenseThreads) {
+            float2 sum = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int wv = 0; wv < 8; ++wv) {
+                const float2 v = Z[wv * kRedStride + o + (o >> 3)];
+                sum.x += v.x;
+                sum.y += v.y;
+            }
+            out(o, sum);
+        }
+    } else {
+        double dr[R], di[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) dr[r] = di[r] = 0.0;
+        for (int pp = warp; pp < rows; pp += 8) {
+            float ar[R], ai[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
+            row(pp, lane, ar, ai);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                dr[r] += (double)ar[r];
+                di[r] += (double)ai[r];
+            }
+        }
+        __syncthreads();
+        double2 *Z64 = reinterpret_cast<double2 *>(Z);
+        double2 *red = Z64 + warp * kRedStride;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int o = lane * R + r;
+            red[o + (o >> 3)] = make_double2(dr[r], di[r]);
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < kDenseOT; o += kDenseThreads) {
+            double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int wv = 0; wv < 8; ++wv) {
+                const double2 v = Z64[wv * kRedStride + o + (o >> 3)];
+                sum.x += v.x;
+                sum.y += v.y;
+            }
+            out(o, sum);
+        }
+    }
+}
 
 template <int L>
 __global__ void __launch_bounds__(kDenseThreads, 2)
@@ -82,7 +269,6 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
                 const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
                 const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
                 float2 *__restrict__ ext) {
-    constexpr int R = kDenseR;
     extern __shared__ float4 smem4[];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
@@ -95,7 +281,7 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     const int Mp = dense_row_stride(L);
     float2 *Z = reinterpret_cast<float2 *>(smem4);
     float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smem4) + dense_zbytes(P, L));
-    float2 *wtab = reinterpret_cast<float2 *>(tsm + ((P * L + 1) & ~1));
+    void *wtab = tsm + ((P * L + 3) & ~3);
 
     const int s0 = D - sb.pc - 1;
     const int m_base = j0 - (L - 1);
@@ -115,105 +301,28 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     const int nk = dense_rounds(P, L);
     const float *tg = taps_arena + cp.taps_off;
     for (int i = threadIdx.x; i < P * L; i += kDenseThreads) tsm[i] = tg[i];
-    for (int k = threadIdx.x; k < nk; k += kDenseThreads)
-        wtab[k] = q64_phasor((uint64_t)k * (uint64_t)kDenseThreads * inc);
     const int t = (int)threadIdx.x;
-    int mr = t / D, q = t - (t / D) * D;
-    const int dm = kDenseThreads / D, dq = kDenseThreads - dm * D;
-    const float2 a_t = q64_phasor(u0 + (uint64_t)(int64_t)(ibase + t) * inc);
-    __syncthreads();
-    const int nfull = total / kDenseThreads;  // rounds in which every thread has a sample
-    const bool interior = ibase >= 0 && ibase + total <= n;
-    constexpr int U = 4;
-    int k = 0;
-    if (interior) {
-        const float2 *xp = x + ibase + t;
-        for (; k + U <= nfull; k += U) {
-            float2 xv[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) xv[u] = __ldg(xp + (k + u) * kDenseThreads);
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const float2 rot = cmulf(a_t, wtab[k + u]);
-                Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = cmulf(xv[u], rot);
-                q += dq;
-                mr += dm;
-                if (q >= D) {
-                    q -= D;
-                    ++mr;
-                }
-            }
-        }
-    }
-    // remaining rounds, and every round of tiles at the block edges
-    for (; k < nk; ++k) {
-        const int ip = t + k * kDenseThreads;
-        if (ip < total) {
-            const int i = ibase + ip;
-            float2 v;
-            if (i >= 0) {
-                v = i < n ? cmulf(__ldg(x + i), cmulf(a_t, wtab[k])) : make_float2(0.f, 0.f);
-            } else {
-                const int hi = H + i;
-                v = hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
-            }
-            Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = v;
-        }
-        q += dq;
-        mr += dm;
-        if (q >= D) {
-            q -= D;
-            ++mr;
-        }
+    {
+        float2 *w32 = reinterpret_cast<float2 *>(wtab);
+        for (int k = threadIdx.x; k < nk; k += kDenseThreads)
+            w32[k] = q64_phasor((uint64_t)k * (uint64_t)kDenseThreads * inc);
+        const RotPair rp{q64_phasor(u0 + (uint64_t)(int64_t)(ibase + t) * inc), w32};
+        __syncthreads();
+        dense_stage(Z, Mp, D, total, nk, ibase, n, x, hist, H, rp);
     }
     __syncthreads();
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float ar[R], ai[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
-    for (int p = warp; p < P; p += 8) {
-        // lane window: columns c = lane*R + tt, stored at c + c/8
-        const float2 *zrow = Z + p * Mp;
-        float2 win[R + L - 1];
-#pragma unroll
-        for (int tt = 0; tt < R + L - 1; ++tt) {
-            const int c = lane * R + tt;
-            win[tt] = zrow[c + (c >> 3)];
-        }
-        float h[L];
-#pragma unroll
-        for (int u = 0; u < L; ++u) h[u] = tsm[p * L + u];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-#pragma unroll
-            for (int u = 0; u < L; ++u) {
-                float2 z = win[r + L - 1 - u];
-                ar[r] = fmaf(h[u], z.x, ar[r]);
-                ai[r] = fmaf(h[u], z.y, ai[r]);
-            }
-        }
-    }
-    __syncthreads();
-    constexpr int RS = kDenseOT + kDenseOT / 8;
-    float2 *red = Z + warp * RS;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int o = lane * R + r;
-        red[o + (o >> 3)] = make_float2(ar[r], ai[r]);
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < kDenseOT; o += kDenseThreads) {
-        float2 sum = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int wv = 0; wv < 8; ++wv) {
-            const float2 v = Z[wv * RS + o + (o >> 3)];
-            sum.x += v.x;
-            sum.y += v.y;
-        }
-        const int j = j0 + o;
-        if (j < sb.n_out) ext[sb.ext_off + j] = sum;
-    }
+    auto row = [&](int p, int lane, float *ar, float *ai) { group_row<L>(Z + p * Mp, tsm + p * L, lane, ar, ai); };
+    float2 *dst = ext + sb.ext_off + j0;
+    const int nv = sb.n_out - j0;
+    if (cp.precise_sum)
+        tile_sum<true>(P, row, Z, [&](int o, double2 v) {
+            if (o < nv) dst[o] = make_float2((float)v.x, (float)v.y);
+        });
+    else
+        tile_sum<false>(P, row, Z, [&](int o, float2 v) {
+            if (o < nv) dst[o] = v;
+        });
 }
 
 // Wide form (short polyphase arms, or tiles too large for shared memory): one
@@ -301,6 +410,362 @@ k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
                 ext[sb.ext_off + jw + o] = make_float2(y.x + br[o], y.y + bi[o]);
             }
         }
+    }
+}
+
+// ===========================================================================
+// Phase-grouped polyphase form: channels whose D phases of a 256-output tile
+// do not fit in shared memory (large D), channels with one tap per phase
+// (T <= D), and long arms (L > 16).  A work item is (tile, phase group g):
+// the CTA stages the rotated samples of phases p_lo .. p_lo+Pc-1 only,
+//     Z[pp][m] = s(s0 + (m_base + m)*D - (p_lo + pp)),
+// -- for each column m a contiguous run of Pc samples -- and computes the
+// group's share of the 256 outputs with the same warp/lane layout as the dense
+// form.  With one group the sums go to the extraction output; with several,
+// each group writes its partial sums and k_group_sum adds them in group order
+// (deterministic: the grouping depends on the channel only).
+// The rotation of sample cb(m) + r is A[m] * B[r], A[m] = exp(j phi(cb(m))),
+// B[r] = exp(j r inc), both exact from the Q0.64 phase.
+// ===========================================================================
+__host__ __device__ inline int group_Le(int L) { return L > 16 ? (L + 7) & ~7 : L; }
+
+__host__ __device__ inline int group_smem_bytes(int Pc, int L) {
+    const int Le = group_Le(L);
+    const int M = kDenseOT + Le - 1;
+    int z = (Pc * dense_row_stride(Le) * 8 + 15) & ~15;  // the taps after Z are read as float4
+    const int red = 8 * (kDenseOT + kDenseOT / 8) * 16;
+    if (z < red) z = red;
+    return z + ((Pc * Le + 3) & ~3) * 4 + (M + Pc) * 8 + 16;
+}
+
+int group_smem_bytes_host(int Pc, int L) { return group_smem_bytes(Pc, L); }
+
+struct GroupTile {
+    int j0, g, p_lo, Pc, Le, M, Mp;
+};
+
+__device__ __forceinline__ void group_stage_samples(const GroupTile &gt, int D, int cb0, int n, int H,
+                                                    const float2 *__restrict__ x, const float2 *__restrict__ hist,
+                                                    float2 *Z, const float2 *A, const float2 *B) {
+    const int Pc = gt.Pc;
+    const int total = Pc * gt.M;
+    const int t = (int)threadIdx.x;
+    int m = t / Pc, r = t - m * Pc;
+    const int dm = kDenseThreads / Pc, dr = kDenseThreads - dm * Pc;
+    // every sample of the tile inside the block: no history, no zero fill
+    const bool interior = cb0 >= 0 && cb0 + (gt.M - 1) * D + Pc <= n;
+    // U samples per thread in flight: the loads are issued before any is used
+    constexpr int U = 8;
+    for (int f0 = t; f0 < total; f0 += U * kDenseThreads) {
+        int mu[U], ru[U];
+        float2 xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            mu[u] = m;
+            ru[u] = r;
+            r += dr;
+            m += dm;
+            if (r >= Pc) {
+                r -= Pc;
+                ++m;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = cb0 + mu[u] * D + ru[u];
+            const bool in = f0 + u * kDenseThreads < total;
+            if (interior) {
+                xv[u] = in ? __ldg(x + i) : make_float2(0.f, 0.f);
+            } else {
+                const int hi = H + i;
+                xv[u] = !in ? make_float2(0.f, 0.f)
+                            : (i >= 0 ? (i < n ? __ldg(x + i) : make_float2(0.f, 0.f))
+                                      : (hi >= 0 ? hist[hi] : make_float2(0.f, 0.f)));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (f0 + u * kDenseThreads < total) {
+                const int i = cb0 + mu[u] * D + ru[u];
+                // history samples are already shifted; zero fill stays zero
+                const float2 v = (interior || i >= 0) ? cmulf(xv[u], cmulf(A[mu[u]], B[ru[u]])) : xv[u];
+                Z[(Pc - 1 - ru[u]) * gt.Mp + mu[u] + (mu[u] >> 3)] = v;
+            }
+        }
+    }
+}
+
+// Stage Z (row stride Mp, column c stored at c + c/8), the taps of the
+// group's phases (padded with zeros to Le per phase) and the rotation tables
+// (tabs: M + Pc float2 entries).
+__device__ __forceinline__ void group_stage(const GroupTile &gt, const SlotBlock &sb, const ChanParams &cp,
+                                            uint64_t u0, const float2 *__restrict__ x, int n,
+                                            const float2 *__restrict__ hist, const float *__restrict__ tg,
+                                            float2 *Z, float *tsm, void *tabs) {
+    const int D = cp.decim, L = cp.plen;
+    const uint64_t inc = cp.inc_q;
+    const int s0 = D - sb.pc - 1;
+    const int m_base = gt.j0 - (gt.Le - 1);
+    const int Pc = gt.Pc;
+    // cb(m): first sample of column m's run
+    const int cb0 = s0 + m_base * D - gt.p_lo - Pc + 1;
+    for (int i = threadIdx.x; i < Pc * gt.Le; i += kDenseThreads) {
+        const int pp = i / gt.Le, u = i - pp * gt.Le;
+        tsm[i] = u < L ? tg[(gt.p_lo + pp) * L + u] : 0.f;
+    }
+    {
+        float2 *A = reinterpret_cast<float2 *>(tabs), *B = A + gt.M;
+        for (int m = threadIdx.x; m < gt.M; m += kDenseThreads)
+            A[m] = q64_phasor(u0 + (uint64_t)(int64_t)(cb0 + m * D) * inc);
+        for (int r = threadIdx.x; r < Pc; r += kDenseThreads) B[r] = q64_phasor((uint64_t)r * inc);
+        __syncthreads();
+        group_stage_samples(gt, D, cb0, n, sb.hist_len, x, hist, Z, A, B);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kDenseThreads, 2)
+k_extract_group(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+                const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+                const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
+                float2 *__restrict__ ext, void *__restrict__ part) {
+    extern __shared__ float4 smemg4[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const int ng = sb.ng;
+    const int tile = w.y / ng;
+    GroupTile gt;
+    gt.g = w.y - tile * ng;
+    gt.j0 = tile * kDenseOT;
+    if (gt.j0 >= sb.n_out) return;
+    const int L = cp.plen;
+    gt.p_lo = gt.g * sb.pg;
+    gt.Pc = min(sb.pg, cp.nphase - gt.p_lo);
+    gt.Le = group_Le(L);
+    gt.M = kDenseOT + gt.Le - 1;
+    gt.Mp = dense_row_stride(gt.Le);
+    int zb = (sb.pg * gt.Mp * 8 + 15) & ~15;
+    const int red_b = kRedBytes;
+    if (zb < red_b) zb = red_b;
+    float2 *Z = reinterpret_cast<float2 *>(smemg4);
+    float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smemg4) + zb);
+    void *tabs = tsm + ((sb.pg * gt.Le + 3) & ~3);
+    const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+    group_stage(gt, sb, cp, st[sb.slot].nco_q, x, n, hist, taps_arena + cp.taps_off, Z, tsm, tabs);
+
+    auto row = [&](int pp, int lane, float *ar, float *ai) {
+        const float2 *zrow = Z + pp * gt.Mp;
+        const float *hrow = tsm + pp * gt.Le;
+        switch (L) {
+#define GPUD_ROW(LL) \
+    case LL: group_row<LL>(zrow, hrow, lane, ar, ai); break;
+            GPUD_ROW(1) GPUD_ROW(2) GPUD_ROW(3) GPUD_ROW(4) GPUD_ROW(5) GPUD_ROW(6) GPUD_ROW(7) GPUD_ROW(8)
+            GPUD_ROW(9) GPUD_ROW(10) GPUD_ROW(11) GPUD_ROW(12) GPUD_ROW(13) GPUD_ROW(14) GPUD_ROW(15) GPUD_ROW(16)
+#undef GPUD_ROW
+        default: group_row_long(zrow, hrow, gt.Le, lane, ar, ai); break;
+        }
+    };
+    const int nv = sb.n_out - gt.j0;
+    // one group: the extraction output; several: this group's partial sums
+    // (double2 slots from part_off; float2 view for non-precise channels)
+    const int64_t pbase = (int64_t)sb.part_off * 2 + (int64_t)gt.g * sb.n_out + gt.j0;
+    if (cp.precise_sum) {
+        double2 *p64 = reinterpret_cast<double2 *>(part) + (int64_t)sb.part_off + (int64_t)gt.g * sb.n_out + gt.j0;
+        float2 *e = ext + sb.ext_off + gt.j0;
+        tile_sum<true>(gt.Pc, row, Z, [&](int o, double2 v) {
+            if (o >= nv) return;
+            if (ng == 1) e[o] = make_float2((float)v.x, (float)v.y);
+            else p64[o] = v;
+        });
+    } else {
+        float2 *dst = ng == 1 ? ext + sb.ext_off + gt.j0 : reinterpret_cast<float2 *>(part) + pbase;
+        tile_sum<false>(gt.Pc, row, Z, [&](int o, float2 v) {
+            if (o < nv) dst[o] = v;
+        });
+    }
+}
+
+// Short arms (L <= 4) in phase groups with the NCO folded into the taps: with
+// few taps per staged sample, rotating every sample costs more than the
+// multiply-adds it feeds.  The tile stages raw samples (history samples, kept
+// shifted, are turned back by exp(-j phi(i))), each CTA builds the modulated
+// taps hc[p + uD] = h[p + uD] exp(-j (p + uD) inc) of its phases, and every
+// output takes one rotation exp(j phi(n_j)) at the end:
+//     y_j = exp(j phi(n_j)) * sum_k hc[k] x(n_j - k).
+
+__host__ __device__ inline int mod_smem_bytes(int Pc, int L) {
+    int z = (Pc * dense_row_stride(L) * 8 + 15) & ~15;
+    if (z < kRedBytes) z = kRedBytes;
+    return z + Pc * L * 8 + 16;
+}
+
+int mod_smem_bytes_host(int Pc, int L) { return mod_smem_bytes(Pc, L); }
+
+template <int L>
+__device__ __forceinline__ void mod_row(const float2 *zrow, const float2 *hrow, int lane, float *ar, float *ai) {
+    constexpr int R = kDenseR;
+    float2 win[R + L - 1];
+#pragma unroll
+    for (int tt = 0; tt < R + L - 1; ++tt) {
+        const int c = lane * R + tt;
+        win[tt] = zrow[c + (c >> 3)];
+    }
+    float2 h[L];
+#pragma unroll
+    for (int u = 0; u < L; ++u) h[u] = hrow[u];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+        for (int u = 0; u < L; ++u) {
+            const float2 z = win[r + L - 1 - u];
+            ar[r] = fmaf(h[u].x, z.x, fmaf(-h[u].y, z.y, ar[r]));
+            ai[r] = fmaf(h[u].x, z.y, fmaf(h[u].y, z.x, ai[r]));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kDenseThreads, 3)
+k_extract_mod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+              const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+              const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
+              float2 *__restrict__ ext, void *__restrict__ part) {
+    extern __shared__ float4 smemm4[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const int ng = sb.ng;
+    const int tile = w.y / ng;
+    const int g = w.y - tile * ng;
+    const int j0 = tile * kDenseOT;
+    if (j0 >= sb.n_out) return;
+    const int L = cp.plen, D = cp.decim;
+    const int p_lo = g * sb.pg;
+    const int Pc = min(sb.pg, cp.nphase - p_lo);
+    const int M = kDenseOT + L - 1;
+    const int Mp = dense_row_stride(L);
+    int zb = (sb.pg * Mp * 8 + 15) & ~15;
+    if (zb < kRedBytes) zb = kRedBytes;
+    float2 *Z = reinterpret_cast<float2 *>(smemm4);
+    float2 *hc = reinterpret_cast<float2 *>(reinterpret_cast<char *>(smemm4) + zb);
+    const uint64_t u0 = st[sb.slot].nco_q;
+    const uint64_t inc = cp.inc_q;
+    const float *tg = taps_arena + cp.taps_off;
+    for (int i = threadIdx.x; i < Pc * L; i += kDenseThreads) {
+        const int pp = i / L, u = i - pp * L;
+        const int k = p_lo + pp + u * D;
+        const float h = tg[(p_lo + pp) * L + u];
+        const float2 ph = q64_phasor((uint64_t)0 - (uint64_t)k * inc);
+        hc[i] = make_float2(h * ph.x, h * ph.y);
+    }
+    // raw samples: Z[pp][m] = x(cb0 + m*D + r), pp = Pc-1-r
+    const int s0 = D - sb.pc - 1;
+    const int cb0 = s0 + (j0 - (L - 1)) * D - p_lo - Pc + 1;
+    const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+    const int H = sb.hist_len;
+    const int total = Pc * M;
+    const bool interior = cb0 >= 0 && cb0 + (M - 1) * D + Pc <= n;
+    {
+        const int t = (int)threadIdx.x;
+        int m = t / Pc, r = t - m * Pc;
+        const int dm = kDenseThreads / Pc, dr = kDenseThreads - dm * Pc;
+        constexpr int U = 8;
+        for (int f0 = t; f0 < total; f0 += U * kDenseThreads) {
+            int mu[U], ru[U];
+            float2 xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                mu[u] = m;
+                ru[u] = r;
+                r += dr;
+                m += dm;
+                if (r >= Pc) {
+                    r -= Pc;
+                    ++m;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = cb0 + mu[u] * D + ru[u];
+                const bool in = f0 + u * kDenseThreads < total;
+                if (interior) {
+                    xv[u] = in ? __ldg(x + i) : make_float2(0.f, 0.f);
+                } else if (!in || i >= n) {
+                    xv[u] = make_float2(0.f, 0.f);
+                } else if (i >= 0) {
+                    xv[u] = __ldg(x + i);
+                } else {
+                    const int hi = H + i;
+                    // a carried sample is shifted already: undo its rotation
+                    xv[u] = hi >= 0 ? cmulf(hist[hi], q64_phasor((uint64_t)0 - (u0 + (uint64_t)(int64_t)i * inc)))
+                                    : make_float2(0.f, 0.f);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (f0 + u * kDenseThreads < total) Z[(Pc - 1 - ru[u]) * Mp + mu[u] + (mu[u] >> 3)] = xv[u];
+        }
+    }
+    __syncthreads();
+    auto row = [&](int pp, int lane, float *ar, float *ai) {
+        const float2 *zrow = Z + pp * Mp;
+        const float2 *hrow = hc + pp * L;
+        switch (L) {
+        case 1: mod_row<1>(zrow, hrow, lane, ar, ai); break;
+        case 2: mod_row<2>(zrow, hrow, lane, ar, ai); break;
+        case 3: mod_row<3>(zrow, hrow, lane, ar, ai); break;
+        default: mod_row<4>(zrow, hrow, lane, ar, ai); break;
+        }
+    };
+    const int nv = sb.n_out - j0;
+    auto phase_out = [&](int o) { return q64_phasor(u0 + (uint64_t)(int64_t)(s0 + (j0 + o) * D) * inc); };
+    if (cp.precise_sum) {
+        double2 *p64 = reinterpret_cast<double2 *>(part) + (int64_t)sb.part_off + (int64_t)g * sb.n_out + j0;
+        float2 *e = ext + sb.ext_off + j0;
+        tile_sum<true>(Pc, row, Z, [&](int o, double2 v) {
+            if (o >= nv) return;
+            const float2 ph = phase_out(o);
+            const double yr = v.x * (double)ph.x - v.y * (double)ph.y;
+            const double yi = v.x * (double)ph.y + v.y * (double)ph.x;
+            if (ng == 1) e[o] = make_float2((float)yr, (float)yi);
+            else p64[o] = make_double2(yr, yi);
+        });
+    } else {
+        float2 *dst = ng == 1 ? ext + sb.ext_off + j0
+                              : reinterpret_cast<float2 *>(part) + (int64_t)sb.part_off * 2 + (int64_t)g * sb.n_out + j0;
+        tile_sum<false>(Pc, row, Z, [&](int o, float2 v) {
+            if (o < nv) dst[o] = cmulf(v, phase_out(o));
+        });
+    }
+}
+
+// Sum of the phase groups' partial outputs, in group order (float64 for
+// precise channels, rounded once).
+__global__ void __launch_bounds__(256)
+k_group_sum(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+            const void *__restrict__ part, float2 *__restrict__ ext) {
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const int j = w.y * 256 + (int)threadIdx.x;
+    if (j >= sb.n_out) return;
+    if (prm[sb.slot].precise_sum) {
+        const double2 *p = reinterpret_cast<const double2 *>(part) + sb.part_off + j;
+        double2 sum = make_double2(0.0, 0.0);
+        for (int g = 0; g < sb.ng; ++g) {
+            const double2 v = p[(int64_t)g * sb.n_out];
+            sum.x += v.x;
+            sum.y += v.y;
+        }
+        ext[sb.ext_off + j] = make_float2((float)sum.x, (float)sum.y);
+    } else {
+        const float2 *p = reinterpret_cast<const float2 *>(part) + (int64_t)sb.part_off * 2 + j;
+        float2 sum = make_float2(0.f, 0.f);
+        for (int g = 0; g < sb.ng; ++g) {
+            const float2 v = p[(int64_t)g * sb.n_out];
+            sum.x += v.x;
+            sum.y += v.y;
+        }
+        ext[sb.ext_off + j] = sum;
     }
 }
 
@@ -1638,6 +2103,38 @@ cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 
         attr_set = true;
     }
     k_extract_wide<<<grid, 256, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                 const float2 *hist, const float *taps, float2 *ext, void *part) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_extract_group, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_extract_group<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                               const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                               const float2 *hist, const float *taps, float2 *ext, void *part) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_extract_mod, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_extract_mod<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_sum(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                             const ChanParams *prm, const void *part, float2 *ext) {
+    k_group_sum<<<grid, 256, 0, sm>>>(work, sbt, prm, part, ext);
     return cudaGetLastError();
 }
 

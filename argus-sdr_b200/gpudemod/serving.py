@@ -24,7 +24,7 @@ import numpy as np
 
 from . import CH_AUDIO48K, CH_RDS, E_BUDGET, E_SLOTS, GPUDError, MODE_AM, MODE_CW, MODE_LSB, MODE_NFM, MODE_USB, \
     MODE_WFM_STEREO
-from .synth import MODE_TABLE
+from .synth import HEADROOM_FS, MODE_TABLE
 
 RUNNER_MODE = {"WFM": MODE_WFM_STEREO, "NFM": MODE_NFM, "AM": MODE_AM, "USB": MODE_USB, "LSB": MODE_LSB,
                "CW": MODE_CW}
@@ -37,6 +37,9 @@ class Request:
     t_end: float
     offset_hz: float
     kind: str         # WFM / NFM / AM / USB / LSB / CW
+    out_rate: int = 0  # 0: the mode's rate (MODE_TABLE)
+    taps: int = 0      # 0: the mode's tap count
+    pcm: bool = True   # audio as 48 kHz s16le
 
 
 def channel_spec(req: Request, pcm: bool = True):
@@ -44,7 +47,9 @@ def channel_spec(req: Request, pcm: bool = True):
     request: WFM as stereo with RDS; the narrow modes at their own rates; with
     `pcm` the audio comes back as the 48 kHz s16le stream /ws/audio sends."""
     out_rate, taps, bw = MODE_TABLE[req.kind]
-    flags = (CH_RDS if req.kind == "WFM" else 0) | (CH_AUDIO48K if pcm else 0)
+    out_rate = req.out_rate or out_rate
+    taps = req.taps or taps
+    flags = (CH_RDS if req.kind == "WFM" else 0) | (CH_AUDIO48K if (pcm and req.pcm) else 0)
     return (req.rid, req.offset_hz, bw, out_rate, taps, RUNNER_MODE[req.kind], flags)
 
 
@@ -75,6 +80,63 @@ def poisson_requests(seed: int, seconds: float, rate_hz: float = 50.0, band_hz: 
             out.append(Request(rid, max(t, 0.0), t + life, off, kind))
         rid += 1
     return out
+
+
+def exact_divisors(n: int, lo: int, hi: int) -> list[int]:
+    """Divisors of n in [lo, hi] (exact integer decimation ratios)."""
+    return [d for d in range(lo, hi + 1) if n % d == 0]
+
+
+# Headroom stress mix: the mixed batch's non-WFM ratios (NFM 40 : AM 30 :
+# SSB 30 : CW 20) over 70 % of the channels and WFM (stereo + RDS) over 30 %,
+# the serving stream's WFM share.
+HEADROOM_MIX = (("WFM", 0.30), ("NFM", 0.70 * 40 / 120), ("AM", 0.70 * 30 / 120), ("SSB", 0.70 * 30 / 120),
+                ("CW", 0.70 * 20 / 120))
+
+
+class HeadroomMix:
+    """Channel draws of the headroom stress: FIR lengths uniform over
+    64..1024 taps, decimation log-uniform over the exact divisors of the
+    sample rate in [16, 2400] (WFM at D = 192, 320 kS/s), WFM channels on a
+    broadcast station (80 %) or anywhere, narrow channels on a narrow station
+    (50 %) or anywhere.  Audio stays at the demod rate: several of these rates
+    have no 48 kHz resampler of at most 128 arms."""
+
+    def __init__(self, seed: int, wfm_offsets, narrow_stations, fs: int = HEADROOM_FS, t_lo: int = 64,
+                 t_hi: int = 1024, d_lo: int = 16, d_hi: int = 2400, wfm_decim: int = 192):
+        self.rng = np.random.default_rng(seed)
+        self.fs = fs
+        self.wfm = list(wfm_offsets)
+        self.narrow = list(narrow_stations)
+        self.divs = np.array(exact_divisors(fs, d_lo, d_hi), dtype=np.float64)
+        self.t_lo, self.t_hi, self.wfm_decim = t_lo, t_hi, wfm_decim
+        self.kinds = [k for k, _ in HEADROOM_MIX]
+        p = np.array([q for _, q in HEADROOM_MIX])
+        self.p = p / p.sum()
+        self.rid = 0
+
+    def decim(self) -> int:
+        u = self.rng.uniform(math.log(self.divs[0]), math.log(self.divs[-1]))
+        return int(self.divs[int(np.argmin(np.abs(np.log(self.divs) - u)))])
+
+    def draw(self, t: float = 0.0) -> Request:
+        rng = self.rng
+        kind = self.kinds[rng.choice(len(self.kinds), p=self.p)]
+        if kind == "SSB":
+            kind = "USB" if rng.random() < 0.5 else "LSB"
+        taps = int(rng.integers(self.t_lo, self.t_hi + 1))
+        bw = MODE_TABLE[kind][2]
+        edge = self.fs / 2 - bw
+        if kind == "WFM":
+            D = self.wfm_decim
+            off = float(rng.choice(self.wfm)) if rng.random() < 0.8 else float(rng.uniform(-edge, edge))
+        else:
+            D = self.decim()
+            near = [s for s in self.narrow if s.kind == kind]
+            off = float(near[rng.integers(len(near))].offset_hz) if near and rng.random() < 0.5 \
+                else float(rng.uniform(-edge, edge))
+        self.rid += 1
+        return Request(self.rid, t, math.inf, off, kind, out_rate=self.fs // D, taps=taps, pcm=False)
 
 
 class ServingLoop:

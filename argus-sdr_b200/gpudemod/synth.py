@@ -354,3 +354,35 @@ def serving_scene(device="cpu", block=262144, seconds=10.0, seed=CONFIG_SEEDS[3]
         stations.append(make_narrow_station(rng, kind, float(off), amp))
     sigma = noise_sigma_for_snr(0.01, 0.0, 200_000.0, fs)
     return WidebandScene(fs, block, stations, sigma, seed, device), stations
+
+
+HEADROOM_FS = 61_440_000
+
+
+def headroom_scene(device="cpu", block=1 << 20, seconds=4.0, seed=CONFIG_SEEDS[4]):
+    """Headroom stress source: a continuous 61.44 MS/s band with 48 WFM
+    stations (stereo + RDS) on a 400 kHz grid and 160 narrow stations (NFM /
+    AM / SSB / CW) at random non-overlapping positions, SNR 5-35 dB, plus
+    AWGN.  Returns the scene, the WFM offsets and the narrow stations."""
+    rng = np.random.default_rng(seed)
+    fs = HEADROOM_FS
+    wfm_grid = np.arange(-30_000_000.0, 30_000_001.0, 400_000.0)
+    wfm_offs = np.sort(rng.choice(wfm_grid, size=48, replace=False))
+    narrow_grid = np.array([f for f in np.arange(-30_400_000.0, 30_400_001.0, 25_000.0)
+                            if np.min(np.abs(wfm_offs - f)) > 150_000.0])
+    narrow_offs = rng.choice(narrow_grid, size=160, replace=False)
+    kinds = ["NFM"] * 54 + ["AM"] * 40 + ["USB"] * 20 + ["LSB"] * 20 + ["CW"] * 26
+    stations = []
+    for off in wfm_offs:
+        amp = math.sqrt(10 ** (rng.uniform(5.0, 35.0) / 10)) * 0.01
+        stations.append(make_wfm_station(rng, float(off), amp, seconds=seconds + 1))
+    narrow = []
+    for kind, off in zip(kinds, narrow_offs):
+        bw = MODE_TABLE[kind][2]
+        amp = math.sqrt(10 ** (rng.uniform(5.0, 35.0) / 10)) * 0.01 * math.sqrt(bw / 12_500.0)
+        st = make_narrow_station(rng, kind, float(off), amp)
+        stations.append(st)
+        narrow.append(st)
+    sigma = noise_sigma_for_snr(0.01, 0.0, 200_000.0, fs)
+    return WidebandScene(fs, block, stations, sigma, seed, device), [float(o) for o in wfm_offs], narrow
+

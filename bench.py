@@ -63,9 +63,10 @@ def parse():
     ap.add_argument("--cpu-blocks", type=int, default=2, help="cpu_baseline sample: blocks of 2^20 per channel")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu (no baselines)")
-    ap.add_argument("--workload", default="fm_band", choices=["fm_band", "mixed", "serving"],
+    ap.add_argument("--workload", default="fm_band", choices=["fm_band", "mixed", "serving", "headroom"],
                     help="fm_band: the FM band batch (headline); mixed: the mixed-mode uneven batch; "
-                         "serving: the serving request stream")
+                         "serving: the serving request stream; headroom: 2048 channels at 61.44 MS/s with churn")
+    ap.add_argument("--headroom-channels", type=int, default=2048)
     ap.add_argument("--serve-seconds", type=float, default=8.0, help="serving: seconds of stream per phase")
     return ap.parse_args()
 
@@ -186,9 +187,10 @@ def algorithmic_work(chans, n_in=BLOCK):
         # 48 kHz back end: 33-tap arm per output frame and audio channel,
         # de-emphasis 3 and gain 1 per sample (WFM); 2 bytes per PCM sample
         ach = 2 if c["kind"] == "WFM" else 1
-        n48 = n_out * 48000 // c["out_rate"]
-        w["audio48"]["flop"] += ach * n48 * (2 * 33 + (4 if c["kind"] == "WFM" else 0))
-        w["audio48"]["bytes"] += ach * (n_out * 4 + n48 * 2)
+        if c.get("pcm", True):
+            n48 = n_out * 48000 // c["out_rate"]
+            w["audio48"]["flop"] += ach * n48 * (2 * 33 + (4 if c["kind"] == "WFM" else 0))
+            w["audio48"]["bytes"] += ach * (n_out * 4 + n48 * 2)
         if c["kind"] == "WFM":
             dr = c["out_rate"] // 19000
             n_rds = n_out // dr
@@ -710,6 +712,188 @@ def run_serving(args, world, rank, local):
     return line
 
 
+HEADROOM_BLOCK = 1 << 20
+HEADROOM_WORKLOAD = ("Headroom stress: continuous seeded 61.44 MS/s cf32 (48 WFM + 160 narrow stations, AWGN) in "
+                     "2^20-sample blocks, 2048 concurrent channels (WFM 30 % with stereo + RDS at D 192; NFM / AM / "
+                     "SSB / CW at the mixed batch's 40:30:30:20 ratios), FIR lengths uniform 64-1024 taps, "
+                     "decimation log-uniform over the exact divisors of 61,440,000 in [16, 2400], churn: Poisson "
+                     "200/s channel replacements at block boundaries; audio at the demod rate")
+
+
+def run_headroom(args, world, rank, local):
+    """Headroom stress in serving mode: the population held at 2048 channels,
+    each block boundary retires a Poisson(200/s x period) number of random
+    channels and admits as many new draws.  value: blocks resident in HBM,
+    three in flight, outputs on the device; e2e: each block from pinned host
+    memory to outputs in host memory, p50/p99 of the runner's block time."""
+    import torch
+
+    import gpudemod as G
+    from gpudemod import serving as SV
+    from gpudemod import synth
+    dev = torch.device("cuda", local)
+    fs, blk, n_live = synth.HEADROOM_FS, HEADROOM_BLOCK, args.headroom_channels
+    period = blk / fs
+    n_val = args.warmup + args.steps
+    n_blocks = 2 * n_val
+    scene, wfm_offs, narrow = synth.headroom_scene(device=dev, block=blk, seconds=n_blocks * period + 1,
+                                                   seed=synth.CONFIG_SEEDS[4] + rank)
+    blocks = torch.empty((n_blocks, blk), dtype=torch.complex64, device=dev)
+    for b in range(n_blocks):
+        blocks[b] = scene.next_block()
+    torch.cuda.synchronize()
+    mix = SV.HeadroomMix(synth.CONFIG_SEEDS[4] + 101 * rank, wfm_offs, narrow)
+    churn = np.random.default_rng(synth.CONFIG_SEEDS[4] + 7 + rank)
+    # spare slots: a retired slot is reused only after the blocks in flight that
+    # still read it have completed
+    runner = G.ChannelRunner(fs, blk, max_channels=n_live + 64, max_taps=1024, device_mem_budget=48 << 30)
+    live = {}
+
+    def admit(req):
+        live[req.rid] = (runner.admit(*SV.channel_spec(req)), req)
+
+    def boundary():
+        k = int(churn.poisson(200.0 * period))
+        for rid in churn.choice(sorted(live), size=min(k, len(live)), replace=False):
+            slot, _ = live.pop(int(rid))
+            runner.retire(slot)
+        while len(live) < n_live:
+            admit(mix.draw())
+        return k
+
+    def chan_dicts():
+        return [dict(kind=q.kind, T=q.taps, D=fs // q.out_rate, out_rate=q.out_rate, pcm=False)
+                for _, q in live.values()]
+
+    for _ in range(n_live):
+        admit(mix.draw())
+    stream = torch.cuda.ExternalStream(runner.stream_handle(), device=dev)
+
+    # ---- value: blocks in HBM, three in flight, outputs on the device -------
+    runner.set_host_outputs(False)
+    runner.set_profiling(True)
+    clk = ClockSampler(local).__enter__()
+    pipelined(runner, [blocks[b] for b in range(args.warmup)])
+    runner.reset_stats()
+    l0 = G.kernel_launch_count()
+    stage_acc, flop, ch_samples, churned = {}, 0.0, 0, 0
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tickets = []
+    for s in range(args.steps):
+        churned += boundary()
+        w = algorithmic_work(chan_dicts(), n_in=blk)
+        flop += w["per_block_flop"]
+        ch_samples += len(live) * blk
+        tickets.append(runner.submit(blocks[args.warmup + s]))
+        if len(tickets) >= 3:
+            runner.wait(tickets[-3])
+            for name, ms in runner.stage_times():
+                stage_acc.setdefault(name, []).append(ms)
+    runner.wait(tickets[-1])
+    for name, ms in runner.stage_times():
+        stage_acc.setdefault(name, []).append(ms)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = G.kernel_launch_count() - l0
+    t_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    value = world * ch_samples / (t_ms * 1e-3) / 1e6
+    st_value = runner.stats()
+
+    # ---- e2e: pinned host memory in, outputs in host memory, per block ------
+    runner.set_profiling(False)
+    runner.set_host_outputs(True)
+    pinned = [blocks[n_val + b].cpu().pin_memory() for b in range(n_val)]
+    for b in range(args.warmup):
+        boundary()
+        runner.process_block(pinned[b])
+    lat, d2h, used, e2e_samples = [], [], [], 0
+    barrier(world)
+    for s in range(args.steps):
+        boundary()
+        runner.process_block(pinned[args.warmup + s])
+        st = runner.stats()
+        lat.append(st["last_block_ms"])
+        d2h.append(st["last_d2h_bytes"])
+        used.append(st["device_bytes_used"])
+        e2e_samples += len(live) * blk
+    clk.__exit__(None, None, None)
+    L = np.array(lat)
+    busy_ms = max_over_ranks(world, float(L.sum()))
+    e2e = world * e2e_samples / (busy_ms * 1e-3) / 1e6
+    hist = {}
+    for _, q in live.values():
+        hist[q.kind] = hist.get(q.kind, 0) + 1
+    runner.close()
+    if rank != 0:
+        return None
+
+    # ---- roofline: the whole block, and the dominant kernel ------------------
+    hbm_peak, peak_kind = measured_peaks()
+    fp32 = fp32_peak_tflops()
+    kern = {k: statistics.mean(v) for k, v in stage_acc.items()
+            if k not in ("h2d", "d2h") and not k.startswith("wait")}
+    block_ms = t_ms / args.steps
+    work = algorithmic_work(chan_dicts(), n_in=blk)
+    b_min = sum(v["bytes"] for k, v in work.items() if isinstance(v, dict))
+    t_roof = max(flop / args.steps / (fp32 * 1e12), b_min / (hbm_peak * 1e9)) * 1e3
+    dom = max(kern, key=kern.get)
+    dk = stage_key(dom)
+    ach = work[dk]["flop"] / (kern[dom] * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
+            "peak_source": "cuBLAS SGEMM (TF32 off), measured in this run", "kernel": dom,
+            "ms_per_launch": kern[dom], "algorithmic_flop": work[dk]["flop"], "traffic": None,
+            "block": {"gflop": flop / args.steps / 1e9, "min_bytes": b_min, "roofline_ms": t_roof,
+                      "measured_ms": block_ms, "frac": t_roof / block_ms,
+                      "hbm_peak_gbs": hbm_peak, "hbm_peak_source": peak_kind}}
+    cpu = None
+    if not args.no_cpu and not args.profile_only:
+        from oracle import oracle as O
+        omode = {"WFM": O.MODE_WFM_STEREO, "NFM": O.MODE_NFM, "AM": O.MODE_AM, "USB": O.MODE_USB,
+                 "LSB": O.MODE_LSB, "CW": O.MODE_CW}
+        sample = [q for _, q in list(live.values())[:128]]
+        x = blocks[0].cpu().numpy()
+
+        def work1(q):
+            out_rate, taps, bw = synth.MODE_TABLE[q.kind]
+            O.OracleChannel(fs, q.offset_hz, bw, q.out_rate, q.taps, omode[q.kind], rds=q.kind == "WFM").process(x)
+
+        threads = host_threads()
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(work1, sample))
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sample) * blk / dt / 1e6, "unit": "channel-MS/s", "cores": threads, "kind": "port",
+               "sample": f"{len(sample)} channels of the mix x 1 block of 2^20 through the oracle chain "
+                         f"({dt:.1f} s wall)"}
+    return {
+        "metric": "headroom stress: aggregate channel-MS/s at 2048 channels with churn; fraction of the "
+                  "FP32/HBM roofline", "unit": "channel-MS/s",
+        "value": value, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": block_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 NCO/PLL state)", "data": "synthetic (seeded stream and channel draws)",
+        "config": {"workload": HEADROOM_WORKLOAD, "channels": n_live, "block": blk, "sample_rate": fs,
+                   "mix_at_end": hist, "churned_per_pass": churned,
+                   "inputs": f"{n_blocks} consecutive 8 MiB blocks resident in HBM ({n_blocks * 8} MiB > L2)",
+                   "parallelism": f"channel shards, {world} GPU(s), no data-path collective"},
+        "e2e": {"value": e2e, "unit": "channel-MS/s", "h2d_bytes_per_step": blk * 8,
+                "d2h_bytes_per_step": float(np.mean(d2h)), "p50_block_ms": float(np.percentile(L, 50)),
+                "p99_block_ms": float(np.percentile(L, 99)), "max_block_ms": float(L.max())},
+        "latency_ms": {"p50": st_value["p50_block_ms"], "p99": st_value["p99_block_ms"],
+                       "block_period_ms": period * 1e3},
+        "realtime": {"need_channel_msps": n_live * fs / 1e6,
+                     "met": bool(np.percentile(L, 99) < period * 1e3)},
+        "device_bytes_used_max": int(max(used)),
+        "roofline": roof,
+        "stage_ms": {k: round(v, 4) for k, v in sorted(kern.items(), key=lambda kv: -kv[1])},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -717,6 +901,8 @@ def main():
     world, rank, local = dist_setup(args.gpus)
     if args.workload == "serving":
         line = run_serving(args, world, rank, local)
+    elif args.workload == "headroom":
+        line = run_headroom(args, world, rank, local)
     elif args.workload == "mixed":
         line = run_mixed(args, world, rank, local)
     else:

@@ -1,24 +1,38 @@
 """48 kHz audio back end on the GPU (GPUD_CH_AUDIO48K) against the oracle:
 the channel chain's audio through dsp.Resampler (32 taps per arm), WFM
 de-emphasis and gain, s16le encoding (recorder/streamer.go:1408-1470,
-569-575)."""
+569-575).
+
+PCM samples agree with the oracle's to one LSB (float32 rounding at the
+truncation edge).  At a sample where the channel is weak the discriminator
+magnifies the float32 rounding of the extraction, and the reference's own CPU
+path can be several LSB from the PCM of the float64 truth; there the GPU's
+sample must be no further from the truth's PCM than the oracle's, plus one
+LSB."""
 import numpy as np
 import pytest
 
 import gpudemod as G
 from gpudemod import synth
 from oracle import oracle as O
+from oracle.truth64 import Truth64Channel
 from signals import rel_l2
 
 pytestmark = pytest.mark.gpu
 
 
-def _check(g, w_pcm, ctx):
+def _check(g, w_pcm, ctx, t_pcm=None):
     assert g["pcm_rate"] == 48000, ctx
     assert g["pcm"].size == w_pcm.size, (ctx, g["pcm"].size, w_pcm.size)
     if w_pcm.size:
-        d = np.abs(g["pcm"].astype(np.int32) - w_pcm.astype(np.int32))
-        assert d.max() <= 1, (ctx, int(d.max()))  # one LSB: float32 rounding at the truncation edge
+        gp, wp = g["pcm"].astype(np.int32), w_pcm.astype(np.int32)
+        d = np.abs(gp - wp)
+        if d.max() > 1:
+            assert t_pcm is not None, (ctx, int(d.max()))
+            tp = t_pcm.astype(np.int32)
+            bad = d > 1
+            assert np.all(np.abs(gp - tp)[bad] <= np.abs(wp - tp)[bad] + 1), (ctx, int(d.max()))
+            assert bad.sum() <= 4, (ctx, int(bad.sum()))
         assert rel_l2(g["pcm"].astype(np.float64), w_pcm.astype(np.float64)) <= 1e-4, ctx
 
 
@@ -59,8 +73,11 @@ def test_narrow_and_wfm_pcm_matches_oracle(cuda, mode, kind, flags):
     r = G.ChannelRunner(fs, block, max_channels=2)
     slot = r.admit(2, off, bw, rate, taps, mode, flags | G.CH_AUDIO48K)
     oc = O.OracleChannel(fs, off, bw, rate, taps, mode, rds=False)
+    tc = Truth64Channel(fs, off, bw, rate, taps, mode, rds=False)
     tau = 0.0 if flags & G.CH_NO_DEEMPH else (75.0 if flags & G.CH_DEEMPH75 else 50.0)
-    back = O.Audio48(rate, 2 if mode == G.MODE_WFM_STEREO else 1, wfm=(kind == "WFM"), deemph_us=tau)
+    ach = 2 if mode == G.MODE_WFM_STEREO else 1
+    back = O.Audio48(rate, ach, wfm=(kind == "WFM"), deemph_us=tau)
+    back_t = O.Audio48(rate, ach, wfm=(kind == "WFM"), deemph_us=tau)
     try:
         for b in range(3):
             x = scene.next_block().cpu().numpy()
@@ -69,7 +86,8 @@ def test_narrow_and_wfm_pcm_matches_oracle(cuda, mode, kind, flags):
             r.process_block(x)
             w = oc.process(x)
             _, w_pcm = back.process(w["audio"])
-            _check(r.result(slot), w_pcm, (kind, b))
+            _, t_pcm = back_t.process(np.asarray(tc.process(x)["audio"], np.float32))
+            _check(r.result(slot), w_pcm, (kind, b), t_pcm)
     finally:
         r.close()
 

@@ -85,3 +85,36 @@ def test_channel_spec_per_mode():
         assert spec[6] == (G.CH_RDS if kind == "WFM" else 0) | G.CH_AUDIO48K
         assert SV.channel_spec(SV.Request(7, 0.0, 1.0, 0.0, kind), pcm=False)[6] & G.CH_AUDIO48K == 0
         assert 10_000_000 % rate == 0
+
+
+def test_headroom_mix_draws():
+    """Headroom stress channel draws: exact decimation ratios in [16, 2400]
+    (WFM at 192), taps 64..1024, the 30 % WFM / mixed-batch ratio split, audio
+    at the demod rate (no 48 kHz flag), RDS on every WFM channel."""
+    from gpudemod import synth
+    wfm = [-1.2e6, 0.4e6, 8.0e6]
+    narrow = [synth.make_narrow_station(np.random.default_rng(1), k, 1e6 * i, 0.1)
+              for i, k in enumerate(["NFM", "AM", "USB", "LSB", "CW"])]
+    mix = SV.HeadroomMix(5, wfm, narrow)
+    draws = [mix.draw() for _ in range(4000)]
+    fs = synth.HEADROOM_FS
+    kinds = {}
+    for q in draws:
+        kinds[q.kind] = kinds.get(q.kind, 0) + 1
+        D = fs // q.out_rate
+        assert fs % q.out_rate == 0 and D * q.out_rate == fs
+        assert 16 <= D <= 2400
+        assert 64 <= q.taps <= 1024
+        assert abs(q.offset_hz) <= fs / 2
+        spec = SV.channel_spec(q)
+        assert spec[6] & G.CH_AUDIO48K == 0
+        if q.kind == "WFM":
+            assert D == 192 and spec[6] & G.CH_RDS
+    n = len(draws)
+    assert abs(kinds["WFM"] / n - 0.30) < 0.03
+    assert abs(kinds["NFM"] / n - 0.7 * 40 / 120) < 0.03
+    assert abs((kinds["USB"] + kinds["LSB"]) / n - 0.7 * 30 / 120) < 0.03
+    # decimation spreads over the whole log range
+    ds = np.array([fs // q.out_rate for q in draws if q.kind != "WFM"])
+    assert ds.min() <= 20 and ds.max() >= 2000
+    assert 0.3 < np.mean(np.log(ds) < np.log(196)) < 0.7
