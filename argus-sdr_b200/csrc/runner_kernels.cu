@@ -444,54 +444,47 @@ struct GroupTile {
     int j0, g, p_lo, Pc, Le, M, Mp;
 };
 
+// Sample x(cb0 + m*D + r) of column m lands in Z[Pc-1-r][m].  Warp w takes
+// the columns m = w, w+8, ...; its lanes walk the column's contiguous run
+// (coalesced loads; the stores go down one column of Z, odd row stride: no
+// bank conflicts), four columns in flight.  fetch(i) returns the tile's
+// value of block sample i.
+template <class Fetch>
+__device__ __forceinline__ void stage_columns(int Pc, int M, int Mp, int D, int cb0, float2 *Z, const Fetch &fetch) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int U = 4;
+    for (int m0 = warp; m0 < M; m0 += 8 * U) {
+        for (int r = lane; r < Pc; r += 32) {
+            float2 v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int m = m0 + 8 * u;
+                v[u] = m < M ? fetch(cb0 + m * D + r, m, r) : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int m = m0 + 8 * u;
+                if (m < M) Z[(Pc - 1 - r) * Mp + m + (m >> 3)] = v[u];
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ void group_stage_samples(const GroupTile &gt, int D, int cb0, int n, int H,
                                                     const float2 *__restrict__ x, const float2 *__restrict__ hist,
                                                     float2 *Z, const float2 *A, const float2 *B) {
-    const int Pc = gt.Pc;
-    const int total = Pc * gt.M;
-    const int t = (int)threadIdx.x;
-    int m = t / Pc, r = t - m * Pc;
-    const int dm = kDenseThreads / Pc, dr = kDenseThreads - dm * Pc;
-    // every sample of the tile inside the block: no history, no zero fill
-    const bool interior = cb0 >= 0 && cb0 + (gt.M - 1) * D + Pc <= n;
-    // U samples per thread in flight: the loads are issued before any is used
-    constexpr int U = 8;
-    for (int f0 = t; f0 < total; f0 += U * kDenseThreads) {
-        int mu[U], ru[U];
-        float2 xv[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            mu[u] = m;
-            ru[u] = r;
-            r += dr;
-            m += dm;
-            if (r >= Pc) {
-                r -= Pc;
-                ++m;
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int i = cb0 + mu[u] * D + ru[u];
-            const bool in = f0 + u * kDenseThreads < total;
-            if (interior) {
-                xv[u] = in ? __ldg(x + i) : make_float2(0.f, 0.f);
-            } else {
-                const int hi = H + i;
-                xv[u] = !in ? make_float2(0.f, 0.f)
-                            : (i >= 0 ? (i < n ? __ldg(x + i) : make_float2(0.f, 0.f))
-                                      : (hi >= 0 ? hist[hi] : make_float2(0.f, 0.f)));
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (f0 + u * kDenseThreads < total) {
-                const int i = cb0 + mu[u] * D + ru[u];
-                // history samples are already shifted; zero fill stays zero
-                const float2 v = (interior || i >= 0) ? cmulf(xv[u], cmulf(A[mu[u]], B[ru[u]])) : xv[u];
-                Z[(Pc - 1 - ru[u]) * gt.Mp + mu[u] + (mu[u] >> 3)] = v;
-            }
-        }
+    const bool interior = cb0 >= 0 && cb0 + (gt.M - 1) * D + gt.Pc <= n;
+    if (interior) {
+        stage_columns(gt.Pc, gt.M, gt.Mp, D, cb0, Z, [&](int i, int m, int r) {
+            return cmulf(__ldg(x + i), cmulf(A[m], B[r]));
+        });
+    } else {
+        stage_columns(gt.Pc, gt.M, gt.Mp, D, cb0, Z, [&](int i, int m, int r) {
+            if (i >= n) return make_float2(0.f, 0.f);
+            if (i >= 0) return cmulf(__ldg(x + i), cmulf(A[m], B[r]));
+            const int hi = H + i;  // carried history: shifted already
+            return hi >= 0 ? hist[hi] : make_float2(0.f, 0.f);
+        });
     }
 }
 
@@ -663,48 +656,18 @@ k_extract_mod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, 
     const int cb0 = s0 + (j0 - (L - 1)) * D - p_lo - Pc + 1;
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
     const int H = sb.hist_len;
-    const int total = Pc * M;
     const bool interior = cb0 >= 0 && cb0 + (M - 1) * D + Pc <= n;
-    {
-        const int t = (int)threadIdx.x;
-        int m = t / Pc, r = t - m * Pc;
-        const int dm = kDenseThreads / Pc, dr = kDenseThreads - dm * Pc;
-        constexpr int U = 8;
-        for (int f0 = t; f0 < total; f0 += U * kDenseThreads) {
-            int mu[U], ru[U];
-            float2 xv[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                mu[u] = m;
-                ru[u] = r;
-                r += dr;
-                m += dm;
-                if (r >= Pc) {
-                    r -= Pc;
-                    ++m;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = cb0 + mu[u] * D + ru[u];
-                const bool in = f0 + u * kDenseThreads < total;
-                if (interior) {
-                    xv[u] = in ? __ldg(x + i) : make_float2(0.f, 0.f);
-                } else if (!in || i >= n) {
-                    xv[u] = make_float2(0.f, 0.f);
-                } else if (i >= 0) {
-                    xv[u] = __ldg(x + i);
-                } else {
-                    const int hi = H + i;
-                    // a carried sample is shifted already: undo its rotation
-                    xv[u] = hi >= 0 ? cmulf(hist[hi], q64_phasor((uint64_t)0 - (u0 + (uint64_t)(int64_t)i * inc)))
-                                    : make_float2(0.f, 0.f);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (f0 + u * kDenseThreads < total) Z[(Pc - 1 - ru[u]) * Mp + mu[u] + (mu[u] >> 3)] = xv[u];
-        }
+    if (interior) {
+        stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) { return __ldg(x + i); });
+    } else {
+        stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) {
+            if (i >= n) return make_float2(0.f, 0.f);
+            if (i >= 0) return __ldg(x + i);
+            const int hi = H + i;
+            // a carried sample is shifted already: undo its rotation
+            return hi >= 0 ? cmulf(hist[hi], q64_phasor((uint64_t)0 - (u0 + (uint64_t)(int64_t)i * inc)))
+                           : make_float2(0.f, 0.f);
+        });
     }
     __syncthreads();
     auto row = [&](int pp, int lane, float *ar, float *ai) {
