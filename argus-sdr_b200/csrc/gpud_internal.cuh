@@ -104,7 +104,13 @@ struct ChanState {
     int64_t rds_count;   // composite samples consumed
     int32_t rds_hist_len;
     int32_t pll_iters;   // Newton iterations of the last parallel solve
+    double comp_power;   // GPUD_CH_BATCH_STEREO: sum of the block's composite squared
 };
+
+// Channel flags the kernels test (values of GPUD_CH_* in gpudemod.h).
+constexpr int kChPcmF32 = 32;
+constexpr int kChBatchStereo = 64;
+constexpr int kChFreeStereo = 128;
 
 // Per-block per-slot descriptor (host-built; all integer bookkeeping is
 // mirrored on the host, so output sizes are known before launch).
@@ -145,10 +151,9 @@ struct SlotBlock {
 
 // Rational polyphase resampler bank (dsp/resample.go:45-93) for one input rate.
 constexpr int kRsTaps = 33;     // taps per arm at 32 taps per phase (odd prototype)
-constexpr int kRsMaxL = 128;
 struct RsBank {
     int32_t L, M, K, pad;
-    double arm[kRsMaxL * kRsTaps];  // arm[p*K + t]
+    const double *arm;  // device array arm[p*K + t], L*K doubles
 };
 
 // Per-slot audio back-end state.

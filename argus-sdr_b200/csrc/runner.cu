@@ -46,6 +46,12 @@ cudaError_t launch_am(int grid, cudaStream_t sm, const int2 *work, const SlotBlo
                       float *audio);
 cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const WfmTaps *taps, float *wk, int W, const float *comp_dl);
+cudaError_t launch_free_stereo(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                               const ChanParams *prm, const BinadeTable *tabs38, float *wk, int W);
+cudaError_t launch_seg_aa(cudaStream_t sm, const float *in, int C, const double *taps, int nt, int d2, int of,
+                          float *out);
+cudaError_t launch_comp_power(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt,
+                              const ChanParams *prm, ChanState *st, const float *wk);
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
                        ChanState *st, float *wk, int W);
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
@@ -195,6 +201,7 @@ struct Slot {
     int64_t rds_count = 0;
     int64_t rs_t = 0;  // 48 kHz resampler phase counter (outTime)
     int d1 = 1, d1_phase = 0;  // pre-demod decimation and its phase counter
+    double deemph_us = -1.0;   // >= 0: de-emphasis time constant instead of the flags' choice
     int rs_class = -1, rs_L = 1, rs_M = 1, aud_ch = 1;
     uint64_t footprint = 0;
 };
@@ -215,6 +222,8 @@ struct BlockPlan {
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
+    std::vector<int2> w_free;   // (entry, 1024-sample tile) of free-running stereo channels
+    bool batch_stereo = false;  // a GPUD_CH_BATCH_STEREO channel has composite this block
     std::vector<int> aud_list;  // entries with a 48 kHz back end and input this block
     std::vector<int2> w_aud;    // (entry, tile) of the 48 kHz resampler
     std::vector<int2> w_dec;    // (entry, tile) of the pre-demod decimator
@@ -295,6 +304,7 @@ struct gpud_runner {
     RsBank *d_banks = nullptr;
     std::vector<int> rs_rate;     // input rate of each resampler bank
     std::vector<int3> rs_lmk;     // (L, M, K) of each bank
+    std::vector<double *> rs_arms;  // device arms of each bank
     bool pll_parallel = true;
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
@@ -410,14 +420,18 @@ static int rs_gcd(int a, int b) {
     return a < 0 ? -a : a;
 }
 
-static bool build_rs_bank(int in_rate, int out_rate, RsBank *bk) {
+constexpr int kRsMaxArms = 1 << 17;  // any 48 kHz ratio from an integer rate up to 6 GS/s
+
+static bool build_rs_bank(int in_rate, int out_rate, RsBank *bk, std::vector<double> &arms) {
     std::memset(bk, 0, sizeof *bk);
     const int g = rs_gcd(in_rate, out_rate);
     const int l = out_rate / g, m = in_rate / g;
+    if (l > kRsMaxArms) return false;
     int plen = l * 32;
     if (plen % 2 == 0) plen++;
     const int k = (plen + l - 1) / l;
-    if (l > kRsMaxL || k > kRsTaps) return false;
+    if (k > kRsTaps) return false;
+    arms.assign((size_t)l * k, 0.0);
     const double fc = 0.90 / (double)std::max(l, m);
     const double mid = (double)(plen - 1) / 2.0, b0 = rs_bessel0(6.0);
     for (int p = 0; p < l; ++p)
@@ -430,7 +444,7 @@ static bool build_rs_bank(int in_rate, int out_rate, RsBank *bk) {
                 const double xx = x / mid;
                 v = sn * (rs_bessel0(6.0 * std::sqrt(1 - xx * xx)) / b0) * (double)l;
             }
-            bk->arm[p * k + t] = v;
+            arms[(size_t)p * k + t] = v;
         }
     bk->L = l;
     bk->M = m;
@@ -442,15 +456,22 @@ static int rs_class_for(gpud_runner *r, int rate) {
     for (size_t i = 0; i < r->rs_rate.size(); ++i)
         if (r->rs_rate[i] == rate) return (int)i;
     if ((int)r->rs_rate.size() >= kMaxRsClasses) return -1;
-    std::vector<char> buf(sizeof(RsBank));
-    RsBank *bk = reinterpret_cast<RsBank *>(buf.data());
-    if (!build_rs_bank(rate, 48000, bk)) return -1;
+    RsBank bk;
+    std::vector<double> arms;
+    if (!build_rs_bank(rate, 48000, &bk, arms)) return -1;
     const int id = (int)r->rs_rate.size();
+    double *d_arm = nullptr;
+    if (cudaMalloc((void **)&d_arm, arms.size() * sizeof(double)) != cudaSuccess) return -1;
+    r->rs_arms.push_back(d_arm);
+    bk.arm = d_arm;
     // a new bank id is not referenced by any block in flight
-    if (cudaMemcpyAsync(r->d_banks + id, bk, sizeof(RsBank), cudaMemcpyHostToDevice, r->admin) != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(d_arm, arms.data(), arms.size() * sizeof(double), cudaMemcpyHostToDevice, r->admin) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(r->d_banks + id, &bk, sizeof(RsBank), cudaMemcpyHostToDevice, r->admin) != cudaSuccess)
+        return -1;
     if (cudaStreamSynchronize(r->admin) != cudaSuccess) return -1;
     r->rs_rate.push_back(rate);
-    r->rs_lmk.push_back(make_int3(bk->L, bk->M, bk->K));
+    r->rs_lmk.push_back(make_int3(bk.L, bk.M, bk.K));
     return id;
 }
 
@@ -498,11 +519,14 @@ static int rate_class_for(gpud_runner *r, int rate) {
             h.t[k][0] = h.t[k][1] = h.t[k][2] = h.t[k][3] = 0.f;
         }
     }
-    BinadeTable tab;
-    build_binade_table(-2 * GPUD_PI * (-57000.0) / (double)rate, &tab);
+    BinadeTable tab, tab38;
+    build_binade_table(-2 * GPUD_PI * (-57000.0) / (double)rate, &tab);  // RDS FreqShift (fm.go:152)
+    build_binade_table(2 * GPUD_PI * 38000.0 / (double)rate, &tab38);    // free-running stereo (fm.go:107)
     // a new class id is not referenced by any block in flight
     if (cudaMemcpyAsync(r->d_wtaps + id, &h, sizeof h, cudaMemcpyHostToDevice, r->admin) != cudaSuccess) return -1;
-    if (cudaMemcpyAsync(r->d_tabs + id, &tab, sizeof tab, cudaMemcpyHostToDevice, r->admin) != cudaSuccess)
+    if (cudaMemcpyAsync(r->d_tabs + id, &tab, sizeof tab, cudaMemcpyHostToDevice, r->admin) != cudaSuccess ||
+        cudaMemcpyAsync(r->d_tabs + kMaxWfmClasses + id, &tab38, sizeof tab38, cudaMemcpyHostToDevice, r->admin) !=
+            cudaSuccess)
         return -1;
     if (cudaStreamSynchronize(r->admin) != cudaSuccess) return -1;
     r->class_rate.push_back(rate);
@@ -575,6 +599,7 @@ static void fill_params(gpud_runner *r, int slot, ChanParams *p) {
     const bool wfm = s.spec.mode == GPUD_MODE_WFM || s.spec.mode == GPUD_MODE_WFM_STEREO;
     double tau_us = (s.spec.flags & GPUD_CH_DEEMPH75) ? 75.0 : 50.0;
     if (s.spec.flags & GPUD_CH_NO_DEEMPH) tau_us = 0.0;
+    if (s.deemph_us >= 0.0) tau_us = s.deemph_us;
     p->deemph_a = (wfm && tau_us > 0) ? std::exp(-1.0 / (48000.0 * tau_us * 1e-6)) : 0.0;
     p->d1 = s.d1;
 }
@@ -770,7 +795,8 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
         sb.rds_off = (int)rds;
         rds += (sb.n_rds + 1) & ~1;
         sb.pcm_off = (int)pcm;
-        pcm += ((int64_t)sb.rs_nout * s.aud_ch + 7) & ~7;
+        // int16 slots; float32 PCM takes two per sample
+        pcm += ((int64_t)sb.rs_nout * s.aud_ch * ((s.spec.flags & GPUD_CH_PCM_F32) ? 2 : 1) + 7) & ~7;
         if (sb.rs_frames > 0) {
             pl.aud_list.push_back(i);
             for (int t = 0; t * audio48_tile() < sb.rs_nout; ++t) pl.w_aud.push_back(make_int2(i, t));
@@ -798,6 +824,8 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.w_out.clear();
     pl.w_rds.clear();
     pl.pll_list.clear();
+    pl.w_free.clear();
+    pl.batch_stereo = false;
     pl.rds_smem = 0;
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
@@ -833,7 +861,12 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             for (int t = 0; t * decim2_tile() < sb.n_dem; ++t) pl.w_dec.push_back(make_int2(i, t));
         if (mode == GPUD_MODE_WFM_STEREO && sb.n_disc > 0) {
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_fir.push_back(make_int2(i, t));
-            pl.pll_list.push_back(i);
+            if (s.spec.flags & GPUD_CH_FREE_STEREO) {
+                for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_free.push_back(make_int2(i, t));
+            } else {
+                pl.pll_list.push_back(i);
+                if (s.spec.flags & GPUD_CH_BATCH_STEREO) pl.batch_stereo = true;
+            }
         }
         if ((mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO) && sb.n_disc > 0)
             for (int t = 0; t * 1024 < sb.n_disc; ++t) pl.w_out.push_back(make_int2(i, t));
@@ -886,7 +919,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() + pl.w_gsum.size() +
-          pl.w_mod.size();
+          pl.w_mod.size() + pl.w_free.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
     if (dneed > f.desc_cap) {
@@ -982,7 +1015,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
            o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec),
-           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod);
+           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod), o_free = put(pl.w_free);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
@@ -1078,6 +1111,17 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     if (prev) {
         prof_mark(r, f, "wait_prev_back");
         CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
+    }
+    if (!pl.w_free.empty()) {
+        prof_mark(r, f, "free_stereo");
+        CK(launch_free_stereo((int)pl.w_free.size(), f.s, d_w + o_free, d_sb, r->d_prm, r->d_tabs + kMaxWfmClasses,
+                              f.d_wk, W));
+        nl++;
+    }
+    if (pl.batch_stereo) {
+        prof_mark(r, f, "comp_power");
+        CK(launch_comp_power((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk));
+        nl++;
     }
     if (!pl.pll_list.empty()) {
         if (r->pll_parallel) {
@@ -1254,7 +1298,7 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
             std::memcpy(gathered.data() + a_off + (size_t)fb.audio_off * 4,
                         f.h_out + f.off_audio + (size_t)o.audio_off * 4, (size_t)o.n_audio * 4);
         std::memcpy(gathered.data() + p_off + (size_t)fb.pcm_off * 2, f.h_out + f.off_pcm + (size_t)o.pcm_off * 2,
-                    (size_t)o.rs_nout * (size_t)s.aud_ch * 2);
+                    (size_t)o.rs_nout * (size_t)s.aud_ch * ((s.spec.flags & GPUD_CH_PCM_F32) ? 4 : 2));
         std::memcpy(gathered.data() + r_off + (size_t)fb.rds_off * 8, f.h_out + f.off_rds + (size_t)o.rds_off * 8,
                     (size_t)o.n_rds * 8);
         if (s.spec.flags & GPUD_CH_EMIT_IQ)
@@ -1349,7 +1393,7 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     CKC(dalloc(&r->d_audio_dl, M * kAudioDlStrideH));
     CKC(dalloc(&r->d_rds_dl, M * kWfmHist));
     CKC(dalloc(&r->d_wtaps, (size_t)kMaxWfmClasses));
-    CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses));
+    CKC(dalloc(&r->d_tabs, (size_t)kMaxWfmClasses * 2));  // RDS 57 kHz tables, then 38 kHz tables
     CKC(dalloc(&r->d_aud, M));
     CKC(dalloc(&r->d_d1taps, M * kD1Taps));
     CKC(dalloc(&r->d_d1hist, M * kWfmHist));
@@ -1397,6 +1441,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     cudaFree(r->d_d1taps);
     cudaFree(r->d_d1hist);
     cudaFree(r->d_banks);
+    for (double *a : r->rs_arms) cudaFree(a);
     if (r->stream) cudaStreamDestroy(r->stream);
     if (r->admin) cudaStreamDestroy(r->admin);
     delete r;
@@ -1461,12 +1506,23 @@ static void choose_extraction(Slot &s) {
     s.pg = (s.P + s.ng - 1) / s.ng;
 }
 
+static int admit_core(gpud_runner *r, const gpud_channel_spec *spec, int D, int T, double deemph_us,
+                      int *slot_out);
+
 GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out) {
     if (!r || !slot_out) return GPUD_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(r->mu);
     int D, T;
     int rc = validate_spec(r, spec, &D, &T);
     if (rc) return rc;
+    return admit_core(r, spec, D, T, -1.0, slot_out);
+}
+
+// Admission after validation: decimation D and tap count T given (the batch
+// entry point passes a rounded decimation the exact-rate rule would refuse).
+static int admit_core(gpud_runner *r, const gpud_channel_spec *spec, int D, int T, double deemph_us,
+                      int *slot_out) {
+    int rc = 0;
     uint64_t fp = slot_block_bytes(r, D, spec->mode, spec->flags);
     if (r->budget && r->used + fp > r->budget) return set_err(r, GPUD_E_BUDGET, "device-memory budget exhausted");
     // a free slot no block in flight still touches; drain if only such slots are left
@@ -1518,6 +1574,7 @@ GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec
     s.rate_class = rclass;
     s.rs_class = rsclass;
     s.aud_ch = spec->mode == GPUD_MODE_WFM_STEREO ? 2 : 1;
+    s.deemph_us = deemph_us;
     s.d1 = d1;
     s.d1_phase = 0;
     if (rsclass >= 0) {
@@ -1700,7 +1757,11 @@ GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel
     const bool a48 = (s.spec.flags & GPUD_CH_AUDIO48K) != 0 && s.rs_class >= 0;
     out->audio = (a48 && f.host_outputs) ? nullptr : (const float *)(base + f.off_audio) + sb.audio_off;
     if (a48) {
-        out->pcm = (const int16_t *)(base + f.off_pcm) + sb.pcm_off;
+        const int16_t *p = (const int16_t *)(base + f.off_pcm) + sb.pcm_off;
+        if (s.spec.flags & GPUD_CH_PCM_F32)
+            out->pcm_f32 = reinterpret_cast<const float *>(p);
+        else
+            out->pcm = p;
         out->n_pcm = sb.rs_nout * s.aud_ch;
         out->pcm_rate = 48000;
     }
@@ -1957,3 +2018,163 @@ GPUD_API int GPUD_CALL gpud_runner_streaming_extract(gpud_runner *r, const gpud_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Event-recording batch path (recorder/wfm_batch_stereo.go:10-72)
+// ---------------------------------------------------------------------------
+// One capture through a one-channel runner: the channel starts fresh (zero
+// filter histories, pilot loop at 19 kHz, resampler and de-emphasis at rest),
+// its NCO at the first increment (FreqShift pre-increments from phase 0), its
+// decimation phase so that the first output is input 0 (Decimate keeps index
+// 0), the 101-tap low-pass at max(bw/2, 200) raised to 75 kHz, decimation
+// round(fs/192000), the batch stereo decoder and the 48 kHz back end in float.
+GPUD_API int GPUD_CALL gpud_wfm_batch_audio(const gpud_float2 *iq, int n, int iq_on_device, int sample_rate,
+                                            double offset_hz, double bandwidth, double deemph_us, float *out,
+                                            int out_cap, gpud_batch_audio_result *res) {
+    if (!iq || n <= 0 || sample_rate <= 0 || !out || out_cap < 0 || !res || deemph_us < 0) return GPUD_E_ARG;
+    std::memset(res, 0, sizeof *res);
+    int d1 = (int)std::llround((double)sample_rate / 192000.0);
+    if (d1 < 1) d1 = 1;
+    const int rate = sample_rate / d1;
+    res->demod_rate = rate;
+    if ((n + d1 - 1) / d1 < 2) return 0;  // fewer than two decimated samples: no audio
+    gpud_runner *r = nullptr;
+    int rc = gpud_runner_create(sample_rate, n, 1, 101, 0, &r);
+    if (rc) return rc;
+    gpud_channel_spec sp{};
+    sp.signal_id = 1;
+    sp.offset_hz = offset_hz;
+    sp.bandwidth = 2.0 * std::max(bandwidth / 2.0, 75000.0);
+    sp.out_rate = rate;
+    sp.num_taps = 101;
+    sp.mode = GPUD_MODE_WFM_STEREO;
+    sp.flags = GPUD_CH_AUDIO48K | GPUD_CH_PCM_F32 | GPUD_CH_BATCH_STEREO;
+    int slot = -1;
+    {
+        std::lock_guard<std::recursive_mutex> lk(r->mu);
+        rc = admit_core(r, &sp, d1, 101, deemph_us, &slot);
+        if (!rc && r->slots[(size_t)slot].rs_class < 0) rc = set_err(r, GPUD_E_ARG, "no 48 kHz resampler for the demod rate");
+        if (!rc) {
+            Slot &s = r->slots[(size_t)slot];
+            s.pc = d1 - 1;
+            ChanParams p;
+            fill_params(r, slot, &p);
+            const uint64_t u1 = p.inc_q;  // phase of input 0: one increment
+            if (cudaMemcpy(&r->d_st[slot].nco_q, &u1, sizeof u1, cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = set_err(r, GPUD_E_CUDA, "batch state");
+        }
+    }
+    if (!rc) rc = gpud_runner_process_block(r, iq, n, iq_on_device);
+    if (!rc) {
+        gpud_channel_result cr;
+        rc = gpud_runner_result(r, slot, &cr);
+        if (!rc) {
+            if (cr.n_pcm > out_cap) {
+                rc = GPUD_E_ARG;
+            } else {
+                if (cr.n_pcm > 0) std::memcpy(out, cr.pcm_f32, (size_t)cr.n_pcm * sizeof(float));
+                res->n_out = cr.n_pcm;
+                res->out_rate = 48000;
+                res->locked = (cr.flags & 1) ? 1 : 0;
+            }
+        }
+    }
+    gpud_runner_destroy(r);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// One-shot segment demod (recorder/cpu_audio.go:10-75, demodAudioCPU): the
+// live /api/demod path and event recordings of the other modes
+// ---------------------------------------------------------------------------
+// A fresh one-channel runner as for the batch path (FreqShift pre-increment,
+// Decimate from input 0, 101 taps at max(bw/2, 200), 75 kHz at least for the
+// 192 kS/s WFM demodulators, decimation round(fs/demodRate)); WFM is the bare
+// discriminator, WFM_STEREO the free-running stereo decoder.  Above 48 kHz the
+// audio then takes the 63-tap anti-alias filter and every round(rate/48000)-th
+// frame (stereo: whole frames only), on the device.
+GPUD_API int GPUD_CALL gpud_demod_audio_segment(int mode, const gpud_float2 *iq, int n, int iq_on_device,
+                                                int sample_rate, double offset_hz, double bandwidth, float *out,
+                                                int out_cap, gpud_segment_audio_result *res) {
+    if (!iq || n <= 0 || sample_rate <= 0 || !out || out_cap < 0 || !res) return GPUD_E_ARG;
+    if (mode < GPUD_MODE_NFM || mode > GPUD_MODE_CW) return GPUD_E_MODE;
+    std::memset(res, 0, sizeof *res);
+    const bool wide = mode == GPUD_MODE_WFM || mode == GPUD_MODE_WFM_STEREO;
+    const int C = mode == GPUD_MODE_WFM_STEREO ? 2 : 1;
+    res->channels = C;
+    const int drate = wide ? 192000 : 48000;
+    double cutoff = std::max(bandwidth / 2.0, 200.0);
+    if (cutoff < 75000.0 && drate >= 192000) cutoff = 75000.0;
+    int d1 = (int)std::llround((double)sample_rate / (double)drate);
+    if (d1 < 1) d1 = 1;
+    const int rate = sample_rate / d1;
+    res->demod_rate = rate;
+    res->out_rate = rate;
+    gpud_runner *r = nullptr;
+    int rc = gpud_runner_create(sample_rate, n, 1, 101, 0, &r);
+    if (rc) return rc;
+    gpud_channel_spec sp{};
+    sp.signal_id = 1;
+    sp.offset_hz = offset_hz;
+    sp.bandwidth = 2.0 * cutoff;
+    sp.out_rate = rate;
+    sp.num_taps = 101;
+    sp.mode = mode == GPUD_MODE_WFM ? GPUD_MODE_NFM : mode;  // WFM.Demod is the bare discriminator
+    sp.flags = mode == GPUD_MODE_WFM_STEREO ? GPUD_CH_FREE_STEREO : 0;
+    int slot = -1;
+    {
+        std::lock_guard<std::recursive_mutex> lk(r->mu);
+        rc = admit_core(r, &sp, d1, 101, -1.0, &slot);
+        if (!rc) {
+            r->slots[(size_t)slot].pc = d1 - 1;
+            ChanParams p;
+            fill_params(r, slot, &p);
+            const uint64_t u1 = p.inc_q;
+            if (cudaMemcpy(&r->d_st[slot].nco_q, &u1, sizeof u1, cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = set_err(r, GPUD_E_CUDA, "segment state");
+        }
+    }
+    if (!rc) rc = gpud_runner_set_host_outputs(r, 0);
+    if (!rc) rc = gpud_runner_process_block(r, iq, n, iq_on_device);
+    gpud_channel_result cr{};
+    if (!rc) rc = gpud_runner_result(r, slot, &cr);
+    if (!rc) {
+        const float *d_audio = cr.audio;  // device pointer (host outputs off)
+        const int na = cr.n_audio;
+        if (rate > 48000 && na > 0) {
+            auto aa = lowpass_fir(48000.0 / 2.0 * 0.9, rate, 63);
+            int d2 = (int)std::llround((double)rate / 48000.0);
+            if (d2 < 1) d2 = 1;
+            const int frames = na / C;
+            const int of = C == 2 ? frames / d2 : (frames + d2 - 1) / d2;
+            if (of * C > out_cap) {
+                rc = GPUD_E_ARG;
+            } else {
+                double *d_taps = nullptr;
+                float *d_o = nullptr;
+                if (cudaMalloc((void **)&d_taps, aa.size() * sizeof(double)) != cudaSuccess ||
+                    cudaMalloc((void **)&d_o, (size_t)std::max(1, of * C) * sizeof(float)) != cudaSuccess ||
+                    cudaMemcpy(d_taps, aa.data(), aa.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+                    launch_seg_aa(0, d_audio, C, d_taps, (int)aa.size(), d2, of, d_o) != cudaSuccess ||
+                    cudaMemcpy(out, d_o, (size_t)of * C * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    rc = GPUD_E_CUDA;
+                } else {
+                    gpud_count_launch(of * C > 0 ? 1 : 0);
+                    res->n_out = of * C;
+                    res->out_rate = rate / d2;
+                }
+                cudaFree(d_taps);
+                cudaFree(d_o);
+            }
+        } else if (na > out_cap) {
+            rc = GPUD_E_ARG;
+        } else {
+            if (na > 0 && cudaMemcpy(out, d_audio, (size_t)na * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = GPUD_E_CUDA;
+            res->n_out = na;
+        }
+    }
+    gpud_runner_destroy(r);
+    return rc;
+}
+

@@ -1029,6 +1029,19 @@ __device__ void pll_finish(ChanState &s, const ChanParams &cp, int n, double ph,
     s.pll_i = I;
     s.pll_q = Q;
     const double block_err = es / (double)n;
+    if (cp.flags & kChBatchStereo) {
+        // wfmStereoDecodeBatch (wfm_batch_stereo.go:137-142): one call, no
+        // hysteresis; locked by the pilot-band share of the composite's power
+        const double ratio = s.comp_power > 0.0 ? pp / s.comp_power : 0.0;
+        const double fhz = fr * (double)cp.out_rate / twopi;
+        const int locked = ratio > 0.003 && fabs(fhz - 19000.0) < 250.0 && block_err < 0.35;
+        s.locked = locked;
+        s.enabled = locked;
+        s.coherence = (float)ratio;
+        s.pilot_hz = (float)fhz;
+        s.last_err_avg = (float)block_err;
+        return;
+    }
     const double ea = 0.9 * s.err_avg + 0.1 * block_err;
     s.err_avg = ea;
     double coherence = 0.0;
@@ -1556,6 +1569,45 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     s.pll_iters = iters;
 }
 
+// Sum of the block's composite squared for batch-stereo channels (the
+// denominator of their lock test), one CTA per channel, fixed reduction order.
+__global__ void __launch_bounds__(256)
+k_comp_power(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+             ChanState *__restrict__ st, const float *__restrict__ wk) {
+    __shared__ double red[256];
+    const SlotBlock sb = sbt[list[blockIdx.x]];
+    const ChanParams &cp = prm[sb.slot];
+    if (!(cp.flags & kChBatchStereo)) return;
+    const float *m = wk + sb.comp_off;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < sb.n_disc; q += 256) acc += (double)m[q] * (double)m[q];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) st[sb.slot].comp_power = red[0];
+}
+
+// WFMStereo.Demod's L-R product with a free-running carrier (demod/fm.go:
+// 106-112): lr[q] = bpf[q] * float32(2 cos x_{q+1}), x_k = fl(x_{k-1} + inc),
+// inc = 2 pi 38000 / rate, the reference's sequential float64 phase evaluated
+// exactly from its binade table.
+__global__ void __launch_bounds__(256)
+k_free_stereo(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+              const BinadeTable *__restrict__ tabs38, float *__restrict__ wk, int W) {
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    const ChanParams &cp = prm[sb.slot];
+    const BinadeTable &tab = tabs38[cp.rds_tab];
+    const float *bpf = wk + 2 * W + sb.comp_off;
+    float *lr = wk + 4 * W + sb.comp_off;
+    const int q0 = w.y * 1024;
+    for (int q = q0 + threadIdx.x; q < q0 + 1024 && q < sb.n_disc; q += 256)
+        lr[q] = bpf[q] * (float)(2.0 * cos(binade_value(tab, (int64_t)q + 1)));
+}
+
 // L-R lowpass and L/R matrix when stereo is enabled; otherwise the 15 kHz mono
 // fallback filter (its own delay line, advanced only on fallback blocks) duplicated
 // to both channels.  WFM (mono) mode always takes the mono filter, one channel.
@@ -1570,7 +1622,16 @@ k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
     const ChanParams &cp = prm[sb.slot];
     const int q0 = w.y * kFirOT;
     if (q0 >= sb.n_disc) return;
-    const bool stereo = (cp.mode == 3) && st[sb.slot].enabled;
+    const bool stereo = (cp.mode == 3) && (st[sb.slot].enabled || (cp.flags & kChFreeStereo));
+    if (cp.mode == 3 && !stereo && (cp.flags & kChBatchStereo)) {
+        // batch decoder not locked: the discriminator output itself on both
+        // channels (wfm_batch_stereo.go:43-49)
+        const float *m = wk + sb.comp_off;
+        float *dst = audio + sb.audio_off;
+        for (int q = q0 + threadIdx.x; q < q0 + kFirOT && q < sb.n_disc; q += kFirThreads)
+            dst[2 * q] = dst[2 * q + 1] = m[q];
+        return;
+    }
     const WfmTaps &tb = taps[cp.rds_tab];
     for (int i = threadIdx.x; i < kWfmTapsPad; i += kFirThreads) tp[i] = tb.t[i].x;
     if (stereo) {
@@ -2005,9 +2066,13 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
                 s = (float)y;
             }
             if (wfm) s = s * 0.35f;
-            float v = s * 32767.0f;
-            v = fminf(fmaxf(v, -32768.0f), 32767.0f);
-            pcm[sb.pcm_off + o * C + c] = (int16_t)v;
+            if (cp.flags & kChPcmF32) {
+                reinterpret_cast<float *>(pcm + sb.pcm_off)[o * C + c] = s;
+            } else {
+                float v = s * 32767.0f;
+                v = fminf(fmaxf(v, -32768.0f), 32767.0f);
+                pcm[sb.pcm_off + o * C + c] = (int16_t)v;
+            }
         }
     }
     __syncthreads();  // every read of the old state is done
@@ -2098,6 +2163,44 @@ cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *
 cudaError_t launch_group_sum(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                              const ChanParams *prm, const void *part, float2 *ext) {
     k_group_sum<<<grid, 256, 0, sm>>>(work, sbt, prm, part, ext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_comp_power(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt,
+                              const ChanParams *prm, ChanState *st, const float *wk) {
+    k_comp_power<<<count, 256, 0, sm>>>(list, sbt, prm, st, wk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_free_stereo(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                               const ChanParams *prm, const BinadeTable *tabs38, float *wk, int W) {
+    k_free_stereo<<<grid, 256, 0, sm>>>(work, sbt, prm, tabs38, wk, W);
+    return cudaGetLastError();
+}
+
+// Second decimation of the one-shot segment demod (recorder/cpu_audio.go:
+// 35-72): ApplyFIRReal with the 63-tap anti-alias filter per audio channel
+// (float64 taps and sum, separate multiply and add) at frames i*d2.
+__global__ void __launch_bounds__(256)
+k_seg_aa(const float *__restrict__ in, int C, const double *__restrict__ taps, int nt, int d2, int of,
+         float *__restrict__ out) {
+    const int idx = blockIdx.x * blockDim.x + (int)threadIdx.x;
+    if (idx >= of * C) return;
+    const int i = idx / C, c = idx - i * C;
+    const int64_t src = (int64_t)i * d2;
+    double acc = 0.0;
+    for (int k = 0; k < nt; ++k) {
+        const int64_t j = src - k;
+        if (j < 0) break;
+        acc = __dadd_rn(acc, __dmul_rn((double)in[j * C + c], taps[k]));
+    }
+    out[idx] = (float)acc;
+}
+
+cudaError_t launch_seg_aa(cudaStream_t sm, const float *in, int C, const double *taps, int nt, int d2, int of,
+                          float *out) {
+    const int total = of * C;
+    if (total > 0) k_seg_aa<<<(total + 255) / 256, 256, 0, sm>>>(in, C, taps, nt, d2, of, out);
     return cudaGetLastError();
 }
 

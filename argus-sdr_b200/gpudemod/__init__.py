@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
+from ._lib import BatchAudioResult, SegmentAudioResult, ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
 
 # DemodType (gpudemod.go:69-76) -> runner modes
 DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
@@ -25,6 +25,7 @@ MODE_IQ, MODE_NFM, MODE_WFM, MODE_WFM_STEREO, MODE_AM, MODE_USB, MODE_LSB, MODE_
 MODE_BY_NAME = {"IQ": MODE_IQ, "NFM": MODE_NFM, "WFM": MODE_WFM, "WFM_STEREO": MODE_WFM_STEREO, "AM": MODE_AM,
                 "USB": MODE_USB, "LSB": MODE_LSB, "CW": MODE_CW}
 CH_EMIT_IQ, CH_RDS, CH_AUDIO48K, CH_DEEMPH75, CH_NO_DEEMPH = 1, 2, 4, 8, 16
+CH_PCM_F32, CH_BATCH_STEREO, CH_FREE_STEREO = 32, 64, 128
 SCHED_BATCHED, SCHED_PLAIN = 0, 1
 
 E_ARG, E_DECIM, E_TAPS, E_BUDGET, E_SLOTS, E_SLOT, E_BLOCK, E_TIMEOUT, E_CUDA, E_MODE, E_DEVICE_STATUS, E_STATE = \
@@ -215,6 +216,9 @@ class ChannelRunner:
         if payload and res.pcm and res.n_pcm > 0:
             buf = (C.c_int16 * res.n_pcm).from_address(C.addressof(res.pcm.contents))
             pcm = np.frombuffer(buf, dtype=np.int16).copy()
+        elif payload and res.pcm_f32 and res.n_pcm > 0:
+            buf = (C.c_float * res.n_pcm).from_address(C.addressof(res.pcm_f32.contents))
+            pcm = np.frombuffer(buf, dtype=np.float32).copy()
         return {
             "pcm": pcm,
             "pcm_rate": res.pcm_rate,
@@ -379,3 +383,33 @@ class StereoPilotDetector:
         _check(None, lib.gpud_pilot_run(self._p, jobs, len(iqs), float(threshold), None, res))
         return [{"present": bool(r.present), "ratio": r.ratio, "best_hz": r.best_hz, "median": r.median,
                  "best_bin": r.best_bin} for r in res[: len(iqs)]]
+
+
+def wfm_batch_audio(iq, sample_rate: int, offset_hz: float, bandwidth: float, deemph_us: float = 50.0):
+    """Event-recording batch WFM stereo over one capture on the GPU
+    (gpud_wfm_batch_audio; demodWFMStereoBatchAudio,
+    recorder/wfm_batch_stereo.go:10-72).  Returns (interleaved float32 L/R at
+    48 kHz, out rate, locked, demod rate)."""
+    ptr, n, dev, keep = _iq_ptr(iq)
+    cap = 2 * (int(n * 48000 / max(1, int(sample_rate))) + 256)
+    out = np.zeros(cap, np.float32)
+    res = BatchAudioResult()
+    _check(None, lib.gpud_wfm_batch_audio(ptr, n, dev, int(sample_rate), float(offset_hz), float(bandwidth),
+                                          float(deemph_us), out.ctypes.data, cap, C.byref(res)))
+    del keep
+    return out[: res.n_out].copy(), res.out_rate, bool(res.locked), res.demod_rate
+
+
+def demod_audio_segment(mode: int, iq, sample_rate: int, offset_hz: float, bandwidth: float):
+    """One-shot demod of a segment on the GPU (gpud_demod_audio_segment;
+    demodAudioCPU, recorder/cpu_audio.go:10-75).  Returns (float32 audio,
+    channels, audio rate, demod rate)."""
+    ptr, n, dev, keep = _iq_ptr(iq)
+    cap = 2 * n + 64
+    out = np.zeros(cap, np.float32)
+    res = SegmentAudioResult()
+    _check(None, lib.gpud_demod_audio_segment(int(mode), ptr, n, dev, int(sample_rate), float(offset_hz),
+                                              float(bandwidth), out.ctypes.data, cap, C.byref(res)))
+    del keep
+    return out[: res.n_out].copy(), res.channels, res.out_rate, res.demod_rate
+

@@ -59,7 +59,16 @@ class ChannelResult(C.Structure):
         ("pcm", C.POINTER(C.c_int16)),
         ("n_pcm", C.c_int32),
         ("pcm_rate", C.c_int32),
+        ("pcm_f32", C.POINTER(C.c_float)),
     ]
+
+
+class BatchAudioResult(C.Structure):
+    _fields_ = [("n_out", C.c_int32), ("out_rate", C.c_int32), ("demod_rate", C.c_int32), ("locked", C.c_int32)]
+
+
+class SegmentAudioResult(C.Structure):
+    _fields_ = [("n_out", C.c_int32), ("channels", C.c_int32), ("out_rate", C.c_int32), ("demod_rate", C.c_int32)]
 
 
 class PilotJob(C.Structure):
@@ -123,6 +132,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         # runner
         "gpud_runner_create": (i, [i, i, i, i, C.c_uint64, C.POINTER(P)]),
         "gpud_runner_destroy": (i, [P]),
+        "gpud_wfm_batch_audio": (i, [P, i, i, i, d, d, d, P, i, C.POINTER(BatchAudioResult)]),
+        "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
         "gpud_runner_admit": (i, [P, C.POINTER(ChannelSpec), pi]),
         "gpud_runner_retire": (i, [P, i]),
         "gpud_runner_update": (i, [P, i, d, d]),

@@ -179,6 +179,15 @@ enum {
 #define GPUD_CH_AUDIO48K 4
 #define GPUD_CH_DEEMPH75 8    /* 75 us de-emphasis (US/Japan) */
 #define GPUD_CH_NO_DEEMPH 16  /* no de-emphasis */
+#define GPUD_CH_PCM_F32 32    /* with GPUD_CH_AUDIO48K: float samples (pcm_f32) instead of s16le */
+/* WFM_STEREO: the event-recording batch decoder (recorder/wfm_batch_stereo.go:74-155)
+ * instead of the streaming one -- locked per block by the pilot-band share of
+ * the composite's power, no hysteresis, the discriminator output on both
+ * channels when not locked. */
+#define GPUD_CH_BATCH_STEREO 64
+/* WFM_STEREO: WFMStereo.Demod (demod/fm.go:92-123) -- a free-running 38 kHz
+ * carrier instead of the pilot loop, always stereo. */
+#define GPUD_CH_FREE_STEREO 128
 
 /* Schedules for gpud_runner_set_schedule. */
 #define GPUD_SCHED_BATCHED 0 /* one fused launch sequence for all channels (graph-captured) */
@@ -230,6 +239,7 @@ typedef struct {
     const int16_t *pcm;    /* GPUD_CH_AUDIO48K: s16le samples, interleaved per audio channel */
     int32_t n_pcm;         /* int16 samples in pcm (frames x audio_channels) */
     int32_t pcm_rate;      /* 48000 with GPUD_CH_AUDIO48K, else 0 */
+    const float *pcm_f32;  /* GPUD_CH_AUDIO48K | GPUD_CH_PCM_F32: float samples (then pcm is NULL) */
 } gpud_channel_result;
 
 /* Runner statistics. */
@@ -391,6 +401,46 @@ GPUD_API int GPUD_CALL gpud_pilot_run(gpud_pilot *p, const gpud_pilot_job *jobs,
 /* Number of kernels this library has launched in the process (all entry
  * points). */
 GPUD_API uint64_t GPUD_CALL gpud_kernel_launch_count(void);
+
+/* ======================================================================
+ * Part 4 -- event-recording batch WFM stereo (no counterpart in the
+ * reference's C ABI: it replaces the Go function demodWFMStereoBatchAudio,
+ * recorder/wfm_batch_stereo.go:10-72, called by demodWFMStereoHybrid,
+ * recorder/wfm_hybrid.go:18-19, for recorded events)
+ * ====================================================================== */
+typedef struct {
+    int32_t n_out;       /* floats written: frames x 2, interleaved L/R */
+    int32_t out_rate;    /* 48000 */
+    int32_t demod_rate;  /* sample_rate / round(sample_rate / 192000) */
+    int32_t locked;      /* the batch decoder's lock decision */
+} gpud_batch_audio_result;
+
+/* One capture, stateless: shift by offset_hz, 101-tap low-pass, decimate to
+ * ~192 kS/s, discriminator, batch stereo decode (duplicated mono when not
+ * locked), 48 kHz resample, de-emphasis (deemph_us, 0: none), x0.35.  iq is a
+ * host pointer unless iq_on_device.  Returns 0, GPUD_E_ARG (bad argument,
+ * out_cap too small) or a runner error. */
+GPUD_API int GPUD_CALL gpud_wfm_batch_audio(const gpud_float2 *iq, int n, int iq_on_device, int sample_rate,
+                                            double offset_hz, double bandwidth, double deemph_us, float *out,
+                                            int out_cap, gpud_batch_audio_result *res);
+
+typedef struct {
+    int32_t n_out;       /* floats written (frames x channels) */
+    int32_t channels;    /* 2 for WFM_STEREO, else 1 */
+    int32_t out_rate;    /* demod rate / round(demod rate / 48000) when above 48 kHz, else the demod rate */
+    int32_t demod_rate;  /* sample_rate / round(sample_rate / mode's demod rate) */
+} gpud_segment_audio_result;
+
+/* One segment, stateless, any GPUD_MODE_* but IQ (no counterpart in the
+ * reference's C ABI: it replaces the Go function demodAudioCPU,
+ * recorder/cpu_audio.go:10-75, behind the live /api/demod path,
+ * recorder/demod_live.go:40-70, and event recordings, recorder/demod.go:
+ * 21-60): shift, 101-tap low-pass, decimation to ~48 kHz (~192 kHz for WFM),
+ * the mode's demodulator (WFM_STEREO: free-running 38 kHz stereo), and above
+ * 48 kHz a 63-tap anti-alias filter and integer decimation. */
+GPUD_API int GPUD_CALL gpud_demod_audio_segment(int mode, const gpud_float2 *iq, int n, int iq_on_device,
+                                                int sample_rate, double offset_hz, double bandwidth, float *out,
+                                                int out_cap, gpud_segment_audio_result *res);
 
 #ifdef __cplusplus
 }

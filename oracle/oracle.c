@@ -1260,8 +1260,9 @@ static double or_bessel0(double x) {
 #define OR_RS_MAXK 40
 typedef struct {
     int l, m, taps; /* upsample L, downsample M, taps per arm */
-    double bank[OR_RS_MAXL * OR_RS_MAXK]; /* bank[p*taps + t] */
-    double delay[OR_RS_MAXK];             /* delay[0] newest */
+    double bank_in[OR_RS_MAXL * OR_RS_MAXK]; /* arms of small banks, bank[p*taps + t] */
+    double *bank;                            /* bank_in, or a heap bank for L > OR_RS_MAXL */
+    double delay[OR_RS_MAXK];                /* delay[0] newest */
     int out_time;
 } or_resampler;
 
@@ -1271,8 +1272,25 @@ size_t or_resampler_size(void) { return sizeof(or_resampler); }
  * L*tapsPerPhase(+1), windowed sinc fc = 0.90/max(L,M) with Kaiser beta 6 and
  * gain L, split into L arms of ceil(len/L) taps.  Returns 0, or -1 when the
  * bank does not fit. */
+static int resampler_init(or_resampler *r, int in_rate, int out_rate, int taps_per_phase, int heap_ok);
+
 int or_resampler_init(or_resampler *r, int in_rate, int out_rate, int taps_per_phase) {
+    return resampler_init(r, in_rate, out_rate, taps_per_phase, 0);
+}
+
+/* Same with any L: banks above OR_RS_MAXL arms on the heap (or_resampler_release). */
+int or_resampler_init_any(or_resampler *r, int in_rate, int out_rate, int taps_per_phase) {
+    return resampler_init(r, in_rate, out_rate, taps_per_phase, 1);
+}
+
+void or_resampler_release(or_resampler *r) {
+    if (r->bank && r->bank != r->bank_in) free(r->bank);
+    r->bank = r->bank_in;
+}
+
+static int resampler_init(or_resampler *r, int in_rate, int out_rate, int taps_per_phase, int heap_ok) {
     memset(r, 0, sizeof *r);
+    r->bank = r->bank_in;
     if (in_rate <= 0 || out_rate <= 0) in_rate = out_rate = 1;
     if (taps_per_phase < 4) taps_per_phase = 4;
     int g = or_gcd(in_rate, out_rate);
@@ -1280,7 +1298,15 @@ int or_resampler_init(or_resampler *r, int in_rate, int out_rate, int taps_per_p
     int plen = l * taps_per_phase;
     if (plen % 2 == 0) plen++;
     int k = (plen + l - 1) / l;
-    if (l > OR_RS_MAXL || k > OR_RS_MAXK) return -1;
+    if (k > OR_RS_MAXK) return -1;
+    if (l > OR_RS_MAXL) {
+        if (!heap_ok) return -1;
+        r->bank = (double *)malloc(sizeof(double) * (size_t)l * (size_t)k);
+        if (!r->bank) {
+            r->bank = r->bank_in;
+            return -1;
+        }
+    }
     double fc = 0.90 / (double)(l > m ? l : m);
     double mid = (double)(plen - 1) / 2.0;
     double b0 = or_bessel0(6.0);
@@ -1483,4 +1509,333 @@ int or_stereo_pilot(const cf32 *iq, int n, int sample_rate, int window, double t
     *best_hz = bestf;
     if (med > 0) *ratio = best / med;
     return med > 0 && *ratio > threshold;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Event-recording batch path (recorder/wfm_batch_stereo.go:10-168): one call
+ * over a whole capture, every stage stateless.                             */
+
+/* dsp.ApplyFIRReal (dsp/fir_real.go:4-20): float64 taps and accumulation from
+ * a zero history, float32 out. */
+static void apply_fir_real(const float *x, int n, const double *taps, int nt, float *out) {
+    for (int i = 0; i < n; i++) {
+        double acc = 0;
+        for (int k = 0; k < nt; k++) {
+            int idx = i - k;
+            if (idx < 0) break;
+            acc += (double)x[idx] * taps[k];
+        }
+        out[i] = (float)acc;
+    }
+}
+
+/* wfmStereoDecodeBatch (wfm_batch_stereo.go:74-155): the streaming decoder's
+ * filters and pilot loop from a fresh state over one call, locked when the
+ * pilot-band power is above 0.3 % of the composite's, the loop frequency
+ * within 250 Hz of 19 kHz and the mean |phase error| below 0.35.  out: 2n
+ * interleaved L/R (written whatever the decision).  Returns locked. */
+int or_wfm_stereo_decode_batch(const float *mono, int n, int rate, float *out, double *ratio_out,
+                               double *freq_hz_out, double *err_out) {
+    if (n <= 0 || rate <= 0) return 0;
+    double lp[101], h53[101], h23[101], h21[101], h17[101];
+    or_lowpass_fir(15000, rate, 101, lp);
+    or_lowpass_fir(53000, rate, 101, h53);
+    or_lowpass_fir(23000, rate, 101, h23);
+    or_lowpass_fir(21000, rate, 101, h21);
+    or_lowpass_fir(17000, rate, 101, h17);
+    float *lpr = (float *)malloc(sizeof(float) * (size_t)n * 6);
+    float *hi = lpr + n, *lo = lpr + 2 * (size_t)n, *pilot = lpr + 3 * (size_t)n, *bpf = lpr + 4 * (size_t)n,
+          *lr = lpr + 5 * (size_t)n;
+    apply_fir_real(mono, n, lp, 101, lpr);
+    apply_fir_real(mono, n, h53, 101, hi);
+    apply_fir_real(mono, n, h23, 101, lo);
+    for (int i = 0; i < n; i++) bpf[i] = hi[i] - lo[i];
+    apply_fir_real(mono, n, h21, 101, hi);
+    apply_fir_real(mono, n, h17, 101, lo);
+    for (int i = 0; i < n; i++) pilot[i] = hi[i] - lo[i];
+    double phase = 0.0, freq = 2 * OR_PI * 19000 / (double)rate, alpha, beta;
+    or_pll_coefficients(50, 0.707, rate, &alpha, &beta);
+    double lpa = 1 - exp(-2 * OR_PI * 200 / (double)rate);
+    double is = 0, qs = 0;
+    double fmin = 2 * OR_PI * 17000 / (double)rate, fmax = 2 * OR_PI * 21000 / (double)rate;
+    double pp = 0, tp = 0, es = 0;
+    for (int i = 0; i < n; i++) {
+        double p = (double)pilot[i];
+        double sp = sin(phase), cp = cos(phase);
+        double im = p * cp, qm = p * -sp;
+        is += lpa * (im - is);
+        qs += lpa * (qm - qs);
+        double err = atan2(qs, is);
+        freq += beta * err;
+        if (freq < fmin) freq = fmin;
+        else if (freq > fmax) freq = fmax;
+        phase += freq + alpha * err;
+        if (phase > 2 * OR_PI) phase -= 2 * OR_PI;
+        else if (phase < 0) phase += 2 * OR_PI;
+        tp += (double)mono[i] * (double)mono[i];
+        pp += p * p;
+        es += fabs(err);
+        lr[i] = bpf[i] * (float)(2 * sin(2 * phase));
+    }
+    apply_fir_real(lr, n, lp, 101, hi);  /* lr filtered */
+    double ratio = tp > 0 ? pp / tp : 0.0;
+    double fhz = freq * (double)rate / (2 * OR_PI);
+    double berr = es / (double)n;
+    int locked = ratio > 0.003 && fabs(fhz - 19000) < 250 && berr < 0.35;
+    for (int i = 0; i < n; i++) {
+        out[2 * i] = 0.5f * (lpr[i] + hi[i]);
+        out[2 * i + 1] = 0.5f * (lpr[i] - hi[i]);
+    }
+    if (ratio_out) *ratio_out = ratio;
+    if (freq_hz_out) *freq_hz_out = fhz;
+    if (err_out) *err_out = berr;
+    free(lpr);
+    return locked;
+}
+
+/* demodWFMStereoBatchAudio (wfm_batch_stereo.go:10-72): FreqShift by the
+ * offset (float64 phase accumulated from 0, product rounded once), 101-tap
+ * LowpassFIR at max(bw/2, 200) raised to 75 kHz (the WFM demodulator's
+ * 192 kS/s output), ApplyFIR over every sample, Decimate by
+ * decim1 = round(fs/192000) from index 0, the discriminator, the batch stereo
+ * decoder (duplicated mono when not locked), the stereo resampler to 48 kHz
+ * unless the demod rate is 48 kHz, de-emphasis at the output rate, x0.35.
+ * Writes interleaved float L/R to out (capacity out_cap floats); returns the
+ * float count, or -1 (capacity, resampler). */
+int or_wfm_batch_audio(const cf32 *iq, int n, int fs, double offset, double bw, double deemph_us, float *out,
+                       int out_cap, int *out_rate, int *locked_out, int *demod_rate_out) {
+    *out_rate = 0;
+    *locked_out = 0;
+    if (n <= 0 || fs <= 0) return 0;
+    double cutoff = bw / 2;
+    if (cutoff < 200) cutoff = 200;
+    if (cutoff < 75000) cutoff = 75000;
+    double taps[128];
+    int nt = or_lowpass_fir(cutoff, fs, 101, taps);
+    int d1 = (int)round((double)fs / 192000.0);
+    if (d1 < 1) d1 = 1;
+    int rate = fs / d1;
+    if (demod_rate_out) *demod_rate_out = rate;
+    int nd = (n + d1 - 1) / d1;
+    cf32 *dec = (cf32 *)malloc(sizeof(cf32) * (size_t)nd);
+    double inc = offset != 0 ? -2 * OR_PI * offset / (double)fs : 0.0;
+    /* shifted samples feeding the decimated outputs only (ApplyFIR then Decimate) */
+    cf32 *sh = (cf32 *)malloc(sizeof(cf32) * (size_t)n);
+    double ph = 0.0;
+    for (int i = 0; i < n; i++) {
+        if (offset == 0) {
+            sh[i] = iq[i];
+            continue;
+        }
+        ph += inc;
+        double re = cos(ph), im = sin(ph);
+        sh[i].re = (float)((double)iq[i].re * re - (double)iq[i].im * im);
+        sh[i].im = (float)((double)iq[i].re * im + (double)iq[i].im * re);
+    }
+    for (int j = 0; j < nd; j++) {
+        int i = j * d1;
+        double ar = 0, ai = 0;
+        for (int k = 0; k < nt; k++) {
+            int idx = i - k;
+            if (idx < 0) break;
+            ar += (double)sh[idx].re * taps[k];
+            ai += (double)sh[idx].im * taps[k];
+        }
+        dec[j].re = (float)ar;
+        dec[j].im = (float)ai;
+    }
+    free(sh);
+    if (nd < 2) {
+        free(dec);
+        return 0;
+    }
+    int nm = nd - 1;
+    float *mono = (float *)malloc(sizeof(float) * (size_t)nm);
+    or_fm_discrim(dec, nd, mono);
+    free(dec);
+    float *st = (float *)malloc(sizeof(float) * (size_t)nm * 2);
+    int locked = or_wfm_stereo_decode_batch(mono, nm, rate, st, NULL, NULL, NULL);
+    if (!locked)
+        for (int i = 0; i < nm; i++) st[2 * i] = st[2 * i + 1] = mono[i];
+    free(mono);
+    int orate = rate, nf = nm;
+    float *audio = st;
+    if (rate != 48000) {
+        or_resampler *rs = (or_resampler *)malloc(sizeof(or_resampler) * 2);
+        if (or_resampler_init_any(&rs[0], rate, 48000, 32) != 0 || or_resampler_init_any(&rs[1], rate, 48000, 32) != 0) {
+            free(rs);
+            free(st);
+            return -1;
+        }
+        size_t cap = (size_t)((double)nm * 48000.0 / (double)rate) + 64;
+        float *tmp = (float *)malloc(sizeof(float) * (size_t)nm);
+        float *o0 = (float *)malloc(sizeof(float) * cap), *o1 = (float *)malloc(sizeof(float) * cap);
+        for (int i = 0; i < nm; i++) tmp[i] = st[2 * i];
+        int c0 = or_resampler_process(&rs[0], tmp, nm, o0);
+        for (int i = 0; i < nm; i++) tmp[i] = st[2 * i + 1];
+        int c1 = or_resampler_process(&rs[1], tmp, nm, o1);
+        nf = c0 < c1 ? c0 : c1;
+        audio = (float *)malloc(sizeof(float) * (size_t)(2 * nf + 1));
+        for (int i = 0; i < nf; i++) {
+            audio[2 * i] = o0[i];
+            audio[2 * i + 1] = o1[i];
+        }
+        or_resampler_release(&rs[0]);
+        or_resampler_release(&rs[1]);
+        free(rs);
+        free(tmp);
+        free(o0);
+        free(o1);
+        free(st);
+        orate = 48000;
+    }
+    if (2 * nf > out_cap) {
+        free(audio);
+        return -1;
+    }
+    if (deemph_us > 0 && orate > 0) {
+        double tau = deemph_us * 1e-6;
+        double al = exp(-1.0 / ((double)orate * tau));
+        double yl = 0, yr = 0;
+        for (int i = 0; i < nf; i++) {
+            yl = al * yl + (1 - al) * (double)audio[2 * i];
+            audio[2 * i] = (float)yl;
+            yr = al * yr + (1 - al) * (double)audio[2 * i + 1];
+            audio[2 * i + 1] = (float)yr;
+        }
+    }
+    for (int i = 0; i < 2 * nf; i++) out[i] = audio[i] * 0.35f;
+    free(audio);
+    *out_rate = orate;
+    *locked_out = locked;
+    return 2 * nf;
+}
+
+/* demod.wfmStereo (demod/fm.go:92-123), WFMStereo.Demod: discriminator, 15 kHz
+ * L+R, 53k-23k band, a free-running 38 kHz carrier pre-incremented from phase
+ * 0 (no pilot loop), L-R through the 15 kHz filter, L/R matrix; all filters
+ * ApplyFIRReal from a zero history.  out: 2*(n-1) floats.  Returns frames. */
+int or_wfm_stereo_free(const cf32 *iq, int n, int rate, float *out) {
+    if (n < 2) return 0;
+    int m = n - 1;
+    float *base = (float *)malloc(sizeof(float) * (size_t)m * 5);
+    float *lpr = base + m, *hi = base + 2 * (size_t)m, *lo = base + 3 * (size_t)m, *lr = base + 4 * (size_t)m;
+    or_fm_discrim(iq, n, base);
+    double lp[101], h53[101], h23[101];
+    or_lowpass_fir(15000, rate, 101, lp);
+    or_lowpass_fir(53000, rate, 101, h53);
+    or_lowpass_fir(23000, rate, 101, h23);
+    apply_fir_real(base, m, lp, 101, lpr);
+    apply_fir_real(base, m, h53, 101, hi);
+    apply_fir_real(base, m, h23, 101, lo);
+    double phase = 0.0, inc = 2 * OR_PI * 38000 / (double)rate;
+    for (int i = 0; i < m; i++) {
+        float bpf = hi[i] - lo[i];
+        phase += inc;
+        lr[i] = bpf * (float)(2 * cos(phase));
+    }
+    apply_fir_real(lr, m, lp, 101, hi);
+    for (int i = 0; i < m; i++) {
+        out[2 * i] = 0.5f * (lpr[i] + hi[i]);
+        out[2 * i + 1] = 0.5f * (lpr[i] - hi[i]);
+    }
+    free(base);
+    return m;
+}
+
+/* recorder/cpu_audio.go:10-75 demodAudioCPU, the one-shot demod of a segment
+ * (live /api/demod and event recordings): FreqShift, 101-tap LowpassFIR at
+ * max(bw/2, 200) (75 kHz at least for the 192 kS/s WFM demodulators), ApplyFIR,
+ * Decimate by round(fs/demodRate) from index 0, the mode's Demod at the actual
+ * rate (WFM: the discriminator; WFM_STEREO: the free-running stereo decoder),
+ * then above 48 kHz a 63-tap anti-alias LowpassFIR at 21.6 kHz and every
+ * round(rate/48000)-th sample (stereo: whole frames only).  Writes the audio
+ * to out (capacity out_cap floats); returns the float count or -1. */
+int or_demod_audio_segment(int mode, const cf32 *iq, int n, int fs, double offset, double bw, float *out,
+                           int out_cap, int *channels_out, int *out_rate, int *demod_rate_out) {
+    *channels_out = mode == OR_MODE_WFM_STEREO ? 2 : 1;
+    *out_rate = 0;
+    if (n <= 0 || fs <= 0) return 0;
+    int drate = (mode == OR_MODE_WFM || mode == OR_MODE_WFM_STEREO) ? 192000 : 48000;
+    double cutoff = bw / 2;
+    if (cutoff < 200) cutoff = 200;
+    if (cutoff < 75000 && drate >= 192000) cutoff = 75000;
+    double taps[128];
+    int nt = or_lowpass_fir(cutoff, fs, 101, taps);
+    int d1 = (int)round((double)fs / (double)drate);
+    if (d1 < 1) d1 = 1;
+    int rate = fs / d1;
+    *demod_rate_out = rate;
+    int nd = (n + d1 - 1) / d1;
+    cf32 *sh = (cf32 *)malloc(sizeof(cf32) * (size_t)n);
+    double inc = offset != 0 ? -2 * OR_PI * offset / (double)fs : 0.0, ph = 0.0;
+    for (int i = 0; i < n; i++) {
+        if (offset == 0) {
+            sh[i] = iq[i];
+            continue;
+        }
+        ph += inc;
+        double re = cos(ph), im = sin(ph);
+        sh[i].re = (float)((double)iq[i].re * re - (double)iq[i].im * im);
+        sh[i].im = (float)((double)iq[i].re * im + (double)iq[i].im * re);
+    }
+    cf32 *dec = (cf32 *)malloc(sizeof(cf32) * (size_t)nd);
+    for (int j = 0; j < nd; j++) {
+        double ar = 0, ai = 0;
+        for (int k = 0; k < nt; k++) {
+            int idx = j * d1 - k;
+            if (idx < 0) break;
+            ar += (double)sh[idx].re * taps[k];
+            ai += (double)sh[idx].im * taps[k];
+        }
+        dec[j].re = (float)ar;
+        dec[j].im = (float)ai;
+    }
+    free(sh);
+    float *audio = (float *)malloc(sizeof(float) * (size_t)(2 * nd + 2));
+    int na = 0;  /* floats */
+    switch (mode) {
+    case OR_MODE_NFM:
+    case OR_MODE_WFM: na = or_fm_discrim(dec, nd, audio); break;
+    case OR_MODE_WFM_STEREO: na = 2 * or_wfm_stereo_free(dec, nd, rate, audio); break;
+    case OR_MODE_AM: na = or_am_demod(dec, nd, audio); break;
+    case OR_MODE_USB: na = or_ssb_demod(dec, nd, rate, 1, audio); break;
+    case OR_MODE_LSB: na = or_ssb_demod(dec, nd, rate, 0, audio); break;
+    case OR_MODE_CW: na = or_cw_demod(dec, nd, rate, audio); break;
+    default: break;
+    }
+    free(dec);
+    int C = *channels_out, orate = rate, nout = na;
+    if (rate > 48000 && na > 0) {
+        double aa[64];
+        int na_t = or_lowpass_fir(48000.0 / 2.0 * 0.9, rate, 63, aa);
+        int d2 = (int)round((double)rate / 48000.0);
+        if (d2 < 1) d2 = 1;
+        int frames = na / C;
+        float *ch = (float *)malloc(sizeof(float) * (size_t)frames * 2);
+        float *flt = ch + frames;
+        int of = C == 2 ? frames / d2 : (frames + d2 - 1) / d2;
+        if (C * of > out_cap) {
+            free(ch);
+            free(audio);
+            return -1;
+        }
+        for (int c = 0; c < C; c++) {
+            for (int i = 0; i < frames; i++) ch[i] = audio[i * C + c];
+            apply_fir_real(ch, frames, aa, na_t, flt);
+            for (int i = 0; i < of; i++) out[i * C + c] = flt[i * d2];
+        }
+        free(ch);
+        nout = C * of;
+        orate = rate / d2;
+    } else {
+        if (na > out_cap) {
+            free(audio);
+            return -1;
+        }
+        memcpy(out, audio, sizeof(float) * (size_t)na);
+    }
+    free(audio);
+    *out_rate = orate;
+    return nout;
 }

@@ -77,6 +77,8 @@ def _load() -> C.CDLL:
         "or_decim_fir_phase": (i, [P]),
         "or_resampler_size": (C.c_size_t, []),
         "or_resampler_init": (i, [P, i, i, i]),
+        "or_resampler_init_any": (i, [P, i, i, i]),
+        "or_resampler_release": (None, [P]),
         "or_resampler_ratio": (None, [P, P, P, P, P]),
         "or_resampler_bank": (None, [P, P]),
         "or_resampler_process": (i, [P, P, i, P]),
@@ -84,6 +86,10 @@ def _load() -> C.CDLL:
         "or_audio48_init": (i, [P, i, i, i, d]),
         "or_audio48_process": (i, [P, P, i, P, P]),
         "or_stereo_pilot": (i, [P, i, i, i, d, P, P, P, P]),
+        "or_wfm_stereo_decode_batch": (i, [P, i, i, P, P, P, P]),
+        "or_wfm_batch_audio": (i, [P, i, i, d, d, d, P, i, P, P, P]),
+        "or_wfm_stereo_free": (i, [P, i, i, P]),
+        "or_demod_audio_segment": (i, [i, P, i, i, d, d, P, i, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -465,8 +471,12 @@ class Resampler:
 
     def __init__(self, in_rate: int, out_rate: int, taps_per_phase: int = 32):
         self._buf = C.create_string_buffer(_lib.or_resampler_size())
-        if _lib.or_resampler_init(self._buf, int(in_rate), int(out_rate), int(taps_per_phase)) != 0:
+        if _lib.or_resampler_init_any(self._buf, int(in_rate), int(out_rate), int(taps_per_phase)) != 0:
             raise ValueError("resampler bank too large")
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_buf", None) is not None:
+            _lib.or_resampler_release(self._buf)
 
     def ratio(self):
         l, m, k, t = C.c_int(), C.c_int(), C.c_int(), C.c_int()
@@ -519,3 +529,54 @@ def stereo_pilot(iq, sample_rate: int, window: bool = True, threshold: float = 4
     lk = _lib.or_stereo_pilot(_p(x), x.size, int(sample_rate), 1 if window else 0, float(threshold),
                               C.byref(ratio), C.byref(best), C.byref(med), _p(mags))
     return bool(lk), ratio.value, best.value, med.value, mags
+
+
+def wfm_stereo_decode_batch(mono, sample_rate: int):
+    """wfmStereoDecodeBatch (recorder/wfm_batch_stereo.go:74-155).  Returns
+    (interleaved L/R float32, locked, pilot/total power ratio, loop Hz, mean
+    |err|)."""
+    m = np.ascontiguousarray(mono, dtype=np.float32)
+    out = np.zeros(2 * m.size, np.float32)
+    ratio, fhz, err = C.c_double(), C.c_double(), C.c_double()
+    lk = _lib.or_wfm_stereo_decode_batch(_p(m), m.size, int(sample_rate), _p(out), C.byref(ratio), C.byref(fhz),
+                                         C.byref(err))
+    return out, bool(lk), ratio.value, fhz.value, err.value
+
+
+def wfm_batch_audio(iq, sample_rate: int, offset_hz: float, bandwidth: float, deemph_us: float = 50.0):
+    """demodWFMStereoBatchAudio (recorder/wfm_batch_stereo.go:10-72) over one
+    capture.  Returns (interleaved float32 L/R audio, its rate, locked, demod
+    rate)."""
+    x = _c64(iq)
+    cap = 2 * (int(x.size * 48000 / max(1, sample_rate)) + x.size // 4 + 256)
+    out = np.zeros(cap, np.float32)
+    orate, lk, drate = C.c_int(), C.c_int(), C.c_int()
+    n = _lib.or_wfm_batch_audio(_p(x), x.size, int(sample_rate), float(offset_hz), float(bandwidth), float(deemph_us),
+                                _p(out), cap, C.byref(orate), C.byref(lk), C.byref(drate))
+    if n < 0:
+        raise ValueError("batch audio: output capacity or resampler")
+    return out[:n].copy(), orate.value, bool(lk.value), drate.value
+
+
+def wfm_stereo_free(iq, sample_rate: int):
+    """demod.wfmStereo (demod/fm.go:92-123): free-running 38 kHz stereo of one
+    call.  Returns interleaved float32 L/R (2*(n-1))."""
+    x = _c64(iq)
+    out = np.zeros(2 * max(x.size, 1), np.float32)
+    m = _lib.or_wfm_stereo_free(_p(x), x.size, int(sample_rate), _p(out))
+    return out[: 2 * m].copy()
+
+
+def demod_audio_segment(mode: int, iq, sample_rate: int, offset_hz: float, bandwidth: float):
+    """demodAudioCPU (recorder/cpu_audio.go:10-75) over one segment.  Returns
+    (audio float32, channels, audio rate, demod rate)."""
+    x = _c64(iq)
+    cap = 2 * x.size + 64
+    out = np.zeros(cap, np.float32)
+    ch, orate, drate = C.c_int(), C.c_int(), C.c_int()
+    n = _lib.or_demod_audio_segment(int(mode), _p(x), x.size, int(sample_rate), float(offset_hz), float(bandwidth),
+                                    _p(out), cap, C.byref(ch), C.byref(orate), C.byref(drate))
+    if n < 0:
+        raise ValueError("segment audio: output capacity")
+    return out[:n].copy(), ch.value, orate.value, drate.value
+

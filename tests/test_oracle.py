@@ -440,3 +440,84 @@ def test_channel_demod_decim_halves_the_demod_rate():
     assert ra["audio"].size == 2 * (ra["iq"].size // 2 - 1)
     assert rb["audio"].size == 2 * (rb["iq"].size - 1)
     assert a.out_rate == 256_000
+
+
+def _wfm_capture(n_blocks=4):
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "argus-sdr_b200"))
+    from gpudemod import synth
+    scene, _ = synth.plain_wfm_scene(block=262_144)
+    return np.concatenate([scene.next_block().numpy() for _ in range(n_blocks)])
+
+
+def test_batch_stereo_decoder_equals_one_streaming_call():
+    """wfmStereoDecodeBatch and stereoDecodeStateful share their filters and
+    pilot loop (recorder/wfm_batch_stereo.go:74-145, streamer.go:1525-1644):
+    from a fresh state one streaming call yields the same L/R samples; only
+    the lock rule differs (pilot/total power ratio instead of coherence)."""
+    rng = np.random.default_rng(3)
+    rate, n = 192_000, 40_000
+    t = np.arange(n) / rate
+    mono = (0.3 * np.sin(2 * np.pi * 1000 * t) + 0.1 * np.sin(2 * np.pi * 19000 * t)
+            + 0.2 * np.sin(2 * np.pi * 38000 * t) * np.sin(2 * np.pi * 3000 * t)
+            + 0.01 * rng.standard_normal(n)).astype(np.float32)
+    batch, lk, ratio, fhz, err = O.wfm_stereo_decode_batch(mono, rate)
+    stream, _ = O.StereoDecoder().decode(mono, rate)
+    assert np.array_equal(batch, stream)
+    assert lk and ratio > 0.003 and abs(fhz - 19000) < 250 and err < 0.35
+
+
+def test_batch_audio_lock_rates_and_mono_fallback():
+    """demodWFMStereoBatchAudio (recorder/wfm_batch_stereo.go:10-72): 2.4 MS/s
+    decimates by round(12.5) = 13 to 184615 S/s and resamples to 48 kHz; a
+    stereo station locks, noise does not and yields duplicated mono."""
+    x = _wfm_capture()
+    a, rate, lk, drate = O.wfm_batch_audio(x, 2_400_000, 300_000.0, 250_000.0)
+    assert drate == 2_400_000 // 13 and rate == 48_000 and lk
+    nm = (x.size + 12) // 13 - 1
+    rs = O.Resampler(drate, 48_000)
+    assert a.size == 2 * rs.process(np.zeros(nm, np.float32)).size
+    assert not np.allclose(a[0::2], a[1::2])
+    nz = (np.random.default_rng(1).standard_normal(x.size) + 1j * np.random.default_rng(2).standard_normal(x.size))
+    b, rate2, lk2, _ = O.wfm_batch_audio((0.1 * nz).astype(np.complex64), 2_400_000, 300_000.0, 250_000.0)
+    assert not lk2 and np.array_equal(b[0::2], b[1::2])
+    # 1.92 MS/s: D 10 to exactly 192 kS/s; zero offset skips the shift
+    c, rate3, _, drate3 = O.wfm_batch_audio(x[:200_000], 1_920_000, 0.0, 100_000.0, deemph_us=0.0)
+    assert drate3 == 192_000 and rate3 == 48_000 and c.size > 0
+
+
+def test_free_running_stereo_matches_float64_model():
+    """demod.wfmStereo (demod/fm.go:92-123) against a float64 numpy model of
+    the same steps: discriminator, 15 kHz L+R, 53k-23k band times
+    2 cos((q+1) inc) through the 15 kHz filter (the L-R path carries the band
+    filter's extra 50-sample delay, as the reference does), L/R matrix."""
+    rate, n = 192_000, 30_000
+    q = np.arange(n)
+    left = 0.4 * np.sin(2 * np.pi * 1000 * q / rate)
+    c = 0.5 * left + 0.5 * left * np.cos(2 * np.pi * 38000 * (q + 1) / rate)
+    x = np.exp(1j * np.cumsum(np.concatenate([[0.0], 0.5 * c]))).astype(np.complex64)
+    out = O.wfm_stereo_free(x, rate)
+    assert out.size == 2 * n
+    disc = np.angle(x[1:].astype(np.complex128) * np.conj(x[:-1].astype(np.complex128)))
+    f = lambda s, h: np.convolve(s, h)[: s.size]
+    lp = O.lowpass_fir(15000, rate, 101)
+    lpr = f(disc, lp)
+    bpf = f(disc, O.lowpass_fir(53000, rate, 101)) - f(disc, O.lowpass_fir(23000, rate, 101))
+    lr = f(bpf * 2 * np.cos(2 * np.pi * 38000 * (q + 1) / rate), lp)
+    assert np.linalg.norm(out[0::2] - 0.5 * (lpr + lr)) <= 1e-5 * np.linalg.norm(lpr)
+    assert np.linalg.norm(out[1::2] - 0.5 * (lpr - lr)) <= 1e-5 * np.linalg.norm(lpr)
+
+
+def test_segment_rates_and_second_stage():
+    """demodAudioCPU (recorder/cpu_audio.go:10-75): decimation round(fs/48000)
+    or round(fs/192000), anti-alias stage only above 48 kHz, stereo keeps whole
+    frames."""
+    rng = np.random.default_rng(4)
+    x = (0.2 * (rng.standard_normal(240_000) + 1j * rng.standard_normal(240_000))).astype(np.complex64)
+    a, ch, rate, drate = O.demod_audio_segment(O.MODE_NFM, x, 2_400_000, 1e5, 12_500.0)
+    assert (ch, drate, rate) == (1, 48_000, 48_000) and a.size == 240_000 // 50 - 1
+    b, ch, rate, drate = O.demod_audio_segment(O.MODE_WFM_STEREO, x, 2_400_000, 0.0, 200_000.0)
+    frames = (240_000 + 12) // 13 - 1
+    assert (ch, drate, rate) == (2, 184_615, 46_153) and b.size == 2 * (frames // 4)
+    c, ch, rate, drate = O.demod_audio_segment(O.MODE_AM, x, 2_400_000, 0.0, 10_000.0)
+    assert abs(np.mean(c)) < 1e-3  # per-call mean removed
