@@ -67,6 +67,10 @@ class BatchAudioResult(C.Structure):
     _fields_ = [("n_out", C.c_int32), ("out_rate", C.c_int32), ("demod_rate", C.c_int32), ("locked", C.c_int32)]
 
 
+class IQFileMeta(C.Structure):
+    _fields_ = [("sample_rate", C.c_int64), ("center_hz", C.c_double), ("samples", C.c_int64)]
+
+
 class SegmentAudioResult(C.Structure):
     _fields_ = [("n_out", C.c_int32), ("channels", C.c_int32), ("out_rate", C.c_int32), ("demod_rate", C.c_int32)]
 
@@ -134,6 +138,12 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_destroy": (i, [P]),
         "gpud_wfm_batch_audio": (i, [P, i, i, i, d, d, d, P, i, C.POINTER(BatchAudioResult)]),
         "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
+        "gpud_iqfile_write": (i, [C.c_char_p, P, C.c_int64, C.c_int64, d]),
+        "gpud_iqfile_open": (i, [C.c_char_p, C.POINTER(P), C.POINTER(IQFileMeta)]),
+        "gpud_iqfile_close": (None, [P]),
+        "gpud_iqfile_read": (i, [P, P, C.c_int64, i, P]),
+        "gpud_iqfile_seek": (i, [P, C.c_int64]),
+        "gpud_iqfile_tell": (C.c_int64, [P]),
         "gpud_runner_admit": (i, [P, C.POINTER(ChannelSpec), pi]),
         "gpud_runner_retire": (i, [P, i]),
         "gpud_runner_update": (i, [P, i, d, d]),

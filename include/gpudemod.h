@@ -154,6 +154,8 @@ GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
 #define GPUD_E_MODE (-29)          /* unknown demod mode */
 #define GPUD_E_DEVICE_STATUS (-30) /* a kernel reported a bounds/status failure */
 #define GPUD_E_STATE (-31)         /* snapshot blob does not match the slot geometry */
+#define GPUD_E_IO (-33)            /* a snapshot file cannot be opened, mapped or written */
+#define GPUD_E_FORMAT (-34)        /* not an SDRIQ001 file, or shorter than its header says */
 
 /* Demod modes: DemodType of gpudemod.go:69-76 plus WFM_STEREO and IQ-only. */
 enum {
@@ -441,6 +443,32 @@ typedef struct {
 GPUD_API int GPUD_CALL gpud_demod_audio_segment(int mode, const gpud_float2 *iq, int n, int iq_on_device,
                                                 int sample_rate, double offset_hz, double bandwidth, float *out,
                                                 int out_cap, gpud_segment_audio_result *res);
+
+/* ======================================================================
+ * Part 5 -- SDRIQ001 snapshots (internal/iqfile/iqfile.go): write, mapped
+ * read and a looping replay source feeding host or device blocks
+ * ====================================================================== */
+typedef struct gpud_iqfile gpud_iqfile;
+typedef struct {
+    int64_t sample_rate;
+    double center_hz;
+    int64_t samples;
+} gpud_iqfile_meta;
+
+/* iqfile.Write (iqfile.go:33-59): magic, rate, centre, count, cf32 samples. */
+GPUD_API int GPUD_CALL gpud_iqfile_write(const char *path, const gpud_float2 *iq, int64_t n, int64_t sample_rate,
+                                         double center_hz);
+/* iqfile.Read / NewSource (iqfile.go:62-116): GPUD_E_FORMAT on a bad magic or
+ * a file shorter than its header's count, GPUD_E_IO when it cannot be opened. */
+GPUD_API int GPUD_CALL gpud_iqfile_open(const char *path, gpud_iqfile **out, gpud_iqfile_meta *meta);
+GPUD_API void GPUD_CALL gpud_iqfile_close(gpud_iqfile *f);
+/* Source.ReadIQ (iqfile.go:128-148): the next n samples, looping at the end
+ * (zeros for an empty file), into host memory or, with dst_on_device, device
+ * memory on `stream` (a cudaStream_t; NULL: the legacy default stream). */
+GPUD_API int GPUD_CALL gpud_iqfile_read(gpud_iqfile *f, gpud_float2 *dst, int64_t n, int dst_on_device,
+                                        void *stream);
+GPUD_API int GPUD_CALL gpud_iqfile_seek(gpud_iqfile *f, int64_t pos);
+GPUD_API int64_t GPUD_CALL gpud_iqfile_tell(const gpud_iqfile *f);
 
 #ifdef __cplusplus
 }
