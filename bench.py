@@ -222,7 +222,10 @@ def stage_key(name):
 # DRAM bytes per launch of the dominant kernel, read+write, from an ncu
 # capture (--set full) of that kernel on the same workload; None where no
 # capture exists.
-NCU_TRAFFIC = {("fm_band", "extract"): 8.58e6, ("mixed", "extract"): 8.91e6}
+NCU_TRAFFIC = {("fm_band", "extract"): 8.58e6, ("mixed", "extract"): 8.91e6,
+               # k_extract_mod captured at 512 headroom channels (10.5 MB read, 42.2 MB
+               # of partial sums written), scaled by the channel count to 2048
+               ("headroom", "extract"): 52.6e6 * 2048 / 512}
 
 
 def measured_peaks():
@@ -844,7 +847,8 @@ def run_headroom(args, world, rank, local):
     ach = work[dk]["flop"] / (kern[dom] * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
             "peak_source": "cuBLAS SGEMM (TF32 off), measured in this run", "kernel": dom,
-            "ms_per_launch": kern[dom], "algorithmic_flop": work[dk]["flop"], "traffic": None,
+            "ms_per_launch": kern[dom], "algorithmic_flop": work[dk]["flop"],
+            "traffic": NCU_TRAFFIC.get(("headroom", dk)) if n_live == 2048 else None,
             "block": {"gflop": flop / args.steps / 1e9, "min_bytes": b_min, "roofline_ms": t_roof,
                       "measured_ms": block_ms, "frac": t_roof / block_ms,
                       "hbm_peak_gbs": hbm_peak, "hbm_peak_source": peak_kind}}
