@@ -17,6 +17,13 @@
 
 #include "gpud_internal.cuh"
 
+#ifndef GPUD_DENSE_STAGE_U
+#define GPUD_DENSE_STAGE_U 4
+#endif
+#ifndef GPUD_COLUMN_STAGE_U
+#define GPUD_COLUMN_STAGE_U 4
+#endif
+
 namespace gpud {
 
 // ===========================================================================
@@ -79,7 +86,7 @@ __device__ __forceinline__ void dense_stage(float2 *Z, int Mp, int D, int total,
     const int dm = kDenseThreads / D, dq = kDenseThreads - dm * D;
     const int nfull = total / kDenseThreads;  // rounds in which every thread has a sample
     const bool interior = ibase >= 0 && ibase + total <= n;
-    constexpr int U = 4;
+    constexpr int U = GPUD_DENSE_STAGE_U;  // staged loads in flight per thread
     int k = 0;
     if (interior) {
         const float2 *xp = x + ibase + t;
@@ -452,7 +459,7 @@ struct GroupTile {
 template <class Fetch>
 __device__ __forceinline__ void stage_columns(int Pc, int M, int Mp, int D, int cb0, float2 *Z, const Fetch &fetch) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int U = 4;
+    constexpr int U = GPUD_COLUMN_STAGE_U;  // columns in flight per lane
     for (int m0 = warp; m0 < M; m0 += 8 * U) {
         for (int r = lane; r < Pc; r += 32) {
             float2 v[U];

@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import BatchAudioResult, SegmentAudioResult, ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
+from ._lib import BatchAudioResult, RDSJob, RDSResult, SegmentAudioResult, ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
 
 # DemodType (gpudemod.go:69-76) -> runner modes
 DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
@@ -412,4 +412,43 @@ def demod_audio_segment(mode: int, iq, sample_rate: int, offset_hz: float, bandw
                                               float(bandwidth), out.ctypes.data, cap, C.byref(res)))
     del keep
     return out[: res.n_out].copy(), res.channels, res.out_rate, res.demod_rate
+
+
+class RDSDecoder:
+    """rds.Decoder (internal/rds/rds.go:78-636) for a batch of stations on the
+    device (gpud_rds_*): one Decode call per job, state per station kept on
+    the device."""
+
+    def __init__(self, max_stations: int, max_samples: int):
+        self._d = C.c_void_p()
+        _check(None, lib.gpud_rds_decoder_create(int(max_stations), int(max_samples), C.byref(self._d)))
+
+    def close(self):
+        if self._d:
+            lib.gpud_rds_decoder_destroy(self._d)
+            self._d = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def reset(self, station: int):
+        _check(None, lib.gpud_rds_decoder_reset(self._d, int(station)))
+
+    def run(self, jobs):
+        """jobs: (samples, sample_rate, station) with samples a CUDA complex64
+        tensor (or host data, copied to the device).  Returns one dict per job."""
+        import torch
+        keep, arr = [], (RDSJob * max(1, len(jobs)))()
+        for k, (x, fs, st) in enumerate(jobs):
+            t = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(x, np.complex64))
+            t = t.to("cuda", torch.complex64).contiguous()
+            keep.append(t)
+            arr[k] = RDSJob(t.data_ptr() if t.numel() else None, t.numel(), int(fs), int(st), 0)
+        res = (RDSResult * max(1, len(jobs)))()
+        _check(None, lib.gpud_rds_decode_run(self._d, arr, len(jobs), None, res))
+        return [{"groups": r.groups, "groups_total": r.groups_total, "status": r.status, "pi": r.pi,
+                 "ps": r.ps.decode("ascii"), "rt": r.rt.decode("ascii")} for r in res[: len(jobs)]]
+
+    def decode(self, samples, sample_rate: int, station: int = 0):
+        return self.run([(samples, sample_rate, station)])[0]
 

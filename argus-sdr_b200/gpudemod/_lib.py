@@ -67,6 +67,16 @@ class BatchAudioResult(C.Structure):
     _fields_ = [("n_out", C.c_int32), ("out_rate", C.c_int32), ("demod_rate", C.c_int32), ("locked", C.c_int32)]
 
 
+class RDSJob(C.Structure):
+    _fields_ = [("samples", C.c_void_p), ("n", C.c_int32), ("sample_rate", C.c_int32), ("station", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class RDSResult(C.Structure):
+    _fields_ = [("groups", C.c_int32), ("groups_total", C.c_int32), ("status", C.c_int32), ("pi", C.c_uint16),
+                ("pad", C.c_uint16), ("ps", C.c_char * 9), ("rt", C.c_char * 65), ("pad2", C.c_char * 2)]
+
+
 class IQFileMeta(C.Structure):
     _fields_ = [("sample_rate", C.c_int64), ("center_hz", C.c_double), ("samples", C.c_int64)]
 
@@ -139,6 +149,10 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_wfm_batch_audio": (i, [P, i, i, i, d, d, d, P, i, C.POINTER(BatchAudioResult)]),
         "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
         "gpud_iqfile_write": (i, [C.c_char_p, P, C.c_int64, C.c_int64, d]),
+        "gpud_rds_decoder_create": (i, [i, i, C.POINTER(P)]),
+        "gpud_rds_decoder_destroy": (i, [P]),
+        "gpud_rds_decoder_reset": (i, [P, i]),
+        "gpud_rds_decode_run": (i, [P, C.POINTER(RDSJob), i, P, C.POINTER(RDSResult)]),
         "gpud_iqfile_open": (i, [C.c_char_p, C.POINTER(P), C.POINTER(IQFileMeta)]),
         "gpud_iqfile_close": (None, [P]),
         "gpud_iqfile_read": (i, [P, P, C.c_int64, i, P]),

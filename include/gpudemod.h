@@ -470,6 +470,44 @@ GPUD_API int GPUD_CALL gpud_iqfile_read(gpud_iqfile *f, gpud_float2 *dst, int64_
 GPUD_API int GPUD_CALL gpud_iqfile_seek(gpud_iqfile *f, int64_t pos);
 GPUD_API int64_t GPUD_CALL gpud_iqfile_tell(const gpud_iqfile *f);
 
+/* ======================================================================
+ * Part 6 -- RDS decoder for a batch of stations (internal/rds/rds.go:78-636,
+ * rds.Decoder.Decode, called per station and RDS window by
+ * cmd/sdrd/pipeline_runtime.go:1137): symbol timing, Costas loop,
+ * differential decoding, block sync with one-bit correction and flywheel,
+ * PI / PS (group 0A) / RT (group 2A).  State per station stays on the device.
+ * ====================================================================== */
+typedef struct gpud_rds_decoder gpud_rds_decoder;
+
+typedef struct {
+    const gpud_float2 *samples; /* device pointer: RDS baseband (RDSBasebandComplex output) */
+    int32_t n;                  /* below 104: ignored, as the reference does */
+    int32_t sample_rate;
+    int32_t station;            /* 0 .. max_stations-1, distinct within one run */
+    int32_t pad;
+} gpud_rds_job;
+
+typedef struct {
+    int32_t groups;        /* groups applied by this call */
+    int32_t groups_total;  /* over all calls of the station */
+    int32_t status;        /* 0; 1: the timing loop stopped advancing (input far out of range) */
+    uint16_t pi;
+    uint16_t pad;
+    char ps[9];            /* Program Service name, trailing spaces trimmed */
+    char rt[65];           /* RadioText */
+    char pad2[2];
+} gpud_rds_result;
+
+/* max_samples bounds n of every job. */
+GPUD_API int GPUD_CALL gpud_rds_decoder_create(int max_stations, int max_samples, gpud_rds_decoder **out);
+GPUD_API int GPUD_CALL gpud_rds_decoder_destroy(gpud_rds_decoder *r);
+/* A new decoder state for the station (rds.Decoder{} of a newly found station). */
+GPUD_API int GPUD_CALL gpud_rds_decoder_reset(gpud_rds_decoder *r, int station);
+/* One Decode call per job, all jobs in one launch on `stream`; returns once
+ * results (host, count entries) are written. */
+GPUD_API int GPUD_CALL gpud_rds_decode_run(gpud_rds_decoder *r, const gpud_rds_job *jobs, int count,
+                                           gpud_stream_handle stream, gpud_rds_result *results);
+
 #ifdef __cplusplus
 }
 #endif
