@@ -452,3 +452,42 @@ class RDSDecoder:
     def decode(self, samples, sample_rate: int, station: int = 0):
         return self.run([(samples, sample_rate, station)])[0]
 
+
+class Spectrum:
+    """Surveillance spectrum on the device (gpud_spectrum_*): fftutil.Spectrum
+    and WelchPSD (internal/fft/fft.go, welch.go) in float64, power-of-two
+    sizes up to 8192."""
+
+    def __init__(self, max_fft: int = 8192, max_segments: int = 64):
+        self._s = C.c_void_p()
+        _check(None, lib.gpud_spectrum_create(int(max_fft), int(max_segments), C.byref(self._s)))
+
+    def close(self):
+        if self._s:
+            lib.gpud_spectrum_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def _dev(iq):
+        import torch
+        t = iq if isinstance(iq, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(iq, np.complex64))
+        return t.to("cuda", torch.complex64).contiguous()
+
+    def single(self, iq, hann: bool = True):
+        t = self._dev(iq)
+        out = np.zeros(t.numel(), np.float64)
+        _check(None, lib.gpud_spectrum_single(self._s, t.data_ptr(), t.numel(), 1 if hann else 0, None,
+                                              out.ctypes.data))
+        return out
+
+    def welch(self, iq, seg: int, overlap: float = 0.5, hann: bool = True):
+        t = self._dev(iq)
+        out = np.zeros(max(seg, t.numel()), np.float64)
+        n = C.c_int()
+        _check(None, lib.gpud_spectrum_welch(self._s, t.data_ptr(), t.numel(), int(seg), float(overlap),
+                                             1 if hann else 0, None, out.ctypes.data, C.byref(n)))
+        return out[: n.value].copy()
+

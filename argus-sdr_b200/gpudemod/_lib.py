@@ -150,6 +150,10 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
         "gpud_iqfile_write": (i, [C.c_char_p, P, C.c_int64, C.c_int64, d]),
         "gpud_rds_decoder_create": (i, [i, i, C.POINTER(P)]),
+        "gpud_spectrum_create": (i, [i, i, C.POINTER(P)]),
+        "gpud_spectrum_destroy": (i, [P]),
+        "gpud_spectrum_single": (i, [P, P, i, i, P, P]),
+        "gpud_spectrum_welch": (i, [P, P, C.c_int64, i, d, i, P, P, pi]),
         "gpud_rds_decoder_destroy": (i, [P]),
         "gpud_rds_decoder_reset": (i, [P, i]),
         "gpud_rds_decode_run": (i, [P, C.POINTER(RDSJob), i, P, C.POINTER(RDSResult)]),

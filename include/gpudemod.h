@@ -508,6 +508,29 @@ GPUD_API int GPUD_CALL gpud_rds_decoder_reset(gpud_rds_decoder *r, int station);
 GPUD_API int GPUD_CALL gpud_rds_decode_run(gpud_rds_decoder *r, const gpud_rds_job *jobs, int count,
                                            gpud_stream_handle stream, gpud_rds_result *results);
 
+/* ======================================================================
+ * Part 7 -- surveillance spectrum (internal/fft/fft.go:19-55 Spectrum,
+ * internal/fft/welch.go:15-66 WelchPSD, called per frame by
+ * cmd/sdrd/pipeline_runtime.go:294-341; cuFFT or gonum there): float64
+ * transforms in shared memory, power-of-two sizes up to 8192, fftshifted dB.
+ * ====================================================================== */
+typedef struct gpud_spectrum gpud_spectrum;
+
+/* max_fft: a power of two <= 8192; max_segments: Welch segments per call. */
+GPUD_API int GPUD_CALL gpud_spectrum_create(int max_fft, int max_segments, gpud_spectrum **out);
+GPUD_API int GPUD_CALL gpud_spectrum_destroy(gpud_spectrum *s);
+/* Spectrum(iq, Hann(n) when hann, else none): n dB values, 20 log10(|X|/n + 1e-12),
+ * DC at index n/2.  iq: device pointer. */
+GPUD_API int GPUD_CALL gpud_spectrum_single(gpud_spectrum *s, const gpud_float2 *iq, int n, int hann,
+                                            gpud_stream_handle stream, double *out_db);
+/* WelchPSD(iq, seg_size, overlap, Hann when hann): segments at
+ * step = int(seg_size (1 - overlap)), overlap clamped to [0, 0.95], mean power,
+ * 10 log10(. + 1e-24), DC at seg_size/2; *n_out = seg_size.  Fewer samples than
+ * one segment: Spectrum of the whole vector without window (*n_out = n). */
+GPUD_API int GPUD_CALL gpud_spectrum_welch(gpud_spectrum *s, const gpud_float2 *iq, int64_t n, int seg_size,
+                                           double overlap, int hann, gpud_stream_handle stream, double *out_db,
+                                           int *n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -580,3 +580,45 @@ def demod_audio_segment(mode: int, iq, sample_rate: int, offset_hz: float, bandw
         raise ValueError("segment audio: output capacity")
     return out[:n].copy(), ch.value, orate.value, drate.value
 
+
+
+# --------------------------------------------------------------------------
+# surveillance spectrum (internal/fft): the published DFT in float64 (numpy's
+# FFT), with the reference's window, scaling, floor and fftshift
+# --------------------------------------------------------------------------
+
+def hann(n: int) -> np.ndarray:
+    """fftutil.Hann (fft.go:5-17)."""
+    if n <= 1:
+        return np.ones(max(n, 0))
+    return 0.5 * (1 - np.cos(2 * np.pi * np.arange(n) / (n - 1)))
+
+
+def spectrum(iq, window=None) -> np.ndarray:
+    """fftutil.Spectrum (fft.go:19-55): 20 log10(|X|/n + 1e-12), DC at n/2."""
+    x = np.asarray(iq, np.complex64).astype(np.complex128)
+    n = x.size
+    if n == 0:
+        return np.zeros(0)
+    if window is not None and len(window) == n:
+        x = x * np.asarray(window, np.float64)
+    mag = np.abs(np.fft.fft(x)) / n
+    return np.roll(20 * np.log10(mag + 1e-12), n // 2)
+
+
+def welch_psd(iq, seg: int, overlap: float, window=None) -> np.ndarray:
+    """fftutil.WelchPSD (welch.go:15-66): mean |X|^2/n^2 over segments at
+    step int(seg (1 - overlap)), 10 log10(. + 1e-24), DC at seg/2; fewer
+    samples than a segment: Spectrum(iq, window)."""
+    x = np.asarray(iq, np.complex64).astype(np.complex128)
+    overlap = min(max(overlap, 0.0), 0.95)
+    step = max(1, int(seg * (1 - overlap)))
+    acc, segs = np.zeros(seg), 0
+    w = np.asarray(window, np.float64) if window is not None and len(window) == seg else 1.0
+    for start in range(0, x.size - seg + 1, step):
+        mag = np.abs(np.fft.fft(x[start:start + seg] * w)) / seg
+        acc += mag * mag
+        segs += 1
+    if segs == 0:
+        return spectrum(iq, window)
+    return np.roll(10 * np.log10(acc / segs + 1e-24), seg // 2)
