@@ -88,7 +88,22 @@ __device__ __forceinline__ void dense_stage(float2 *Z, int Mp, int D, int total,
     const bool interior = ibase >= 0 && ibase + total <= n;
     constexpr int U = GPUD_DENSE_STAGE_U;  // staged loads in flight per thread
     int k = 0;
-    if (interior) {
+    if (interior && 32 % D == 0) {
+        // D divides 32: the thread's phase row never changes (256 is a
+        // multiple of D) and its column advances by dm = 256/D, a multiple of
+        // 8, so the padded column c + c/8 advances by the constant 9*dm/8.
+        const float2 *xp = x + ibase + t;
+        float2 *zp = Z + (D - 1 - q) * Mp + mr + (mr >> 3);
+        const int dz = dm + (dm >> 3);
+        for (; k + U <= nfull; k += U) {
+            float2 xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = __ldg(xp + (k + u) * kDenseThreads);
+#pragma unroll
+            for (int u = 0; u < U; ++u) zp[(k + u) * dz] = cmulf(xv[u], rp(k + u));
+        }
+        mr += k * dm;  // hand the position to the remaining rounds
+    } else if (interior) {
         const float2 *xp = x + ibase + t;
         for (; k + U <= nfull; k += U) {
             float2 xv[U];
