@@ -166,6 +166,21 @@ def fm_band_channels():
     return [dict(kind="WFM", T=TAPS, D=FS // OUT_RATE, out_rate=OUT_RATE) for _ in range(N_CH)]
 
 
+def extraction_form(T, D):
+    """The runner's choice of extraction kernel for a channel (host
+    choose_extraction): arms of <= 4 taps take the modulated form, else the
+    dense kernel when a 256-output tile's D phases fit in 200 KB of shared
+    memory, else phase groups."""
+    P, L = min(D, T), -(-T // D)
+    if L <= 4:
+        return "extract_mod"
+    M = 256 + L - 1
+    Mp = (M + (M >> 3) + 1) | 1
+    z = max((P * Mp * 8 + 15) & ~15, 8 * 288 * 16)
+    smem = z + ((P * L + 3) & ~3) * 4 + ((P * (256 + L - 1) + 255) // 256) * 8 + 16
+    return "extract_dense" if L <= 16 and smem <= 200 * 1024 else "extract_group"
+
+
 def algorithmic_work(chans, n_in=BLOCK):
     """Per block, summed over channels (the definitions the reference workload
     implies): extraction 4*T*n_out + min(6*n_in, 4*T*n_out) flop (complex x
@@ -176,12 +191,18 @@ def algorithmic_work(chans, n_in=BLOCK):
     wideband block read once + outputs + per-channel taps and history."""
     w = {k: {"flop": 0, "bytes": 0} for k in ("extract", "demod", "wfm_fir", "wfm_out", "pll", "rds", "audio48")}
     w["extract"]["bytes"] = 8 * n_in
+    forms = {}  # the same extraction work split by the kernel that does it
     per_out = {"WFM": 6, "NFM": 6, "AM": 5, "USB": 3, "LSB": 3, "CW": 1}
     for c in chans:
         T, D = c["T"], c["D"]
         n_out = n_in // D
-        w["extract"]["flop"] += 4 * T * n_out + min(6 * n_in, 4 * T * n_out)
-        w["extract"]["bytes"] += 8 * n_out + 4 * T + 16 * (T - 1)
+        f = 4 * T * n_out + min(6 * n_in, 4 * T * n_out)
+        b = 8 * n_out + 4 * T + 16 * (T - 1)
+        w["extract"]["flop"] += f
+        w["extract"]["bytes"] += b
+        fw = forms.setdefault(extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
+        fw["flop"] += f
+        fw["bytes"] += b
         w["demod"]["flop"] += per_out[c["kind"]] * n_out
         w["demod"]["bytes"] += 12 * n_out
         # 48 kHz back end: 33-tap arm per output frame and audio channel,
@@ -203,13 +224,18 @@ def algorithmic_work(chans, n_in=BLOCK):
             w["rds"]["flop"] += 404 * n_rds + 2 * n_out
             w["rds"]["bytes"] += 4 * n_out + 8 * n_rds
     w["per_block_flop"] = sum(v["flop"] for v in w.values())
+    w.update(forms)
     return w
 
 
 def stage_key(name):
-    """Work group of a runner stage name."""
+    """Work group of a runner stage name (extraction by kernel form)."""
+    if name.startswith("extract_dense"):
+        return "extract_dense"
+    if name in ("extract_group", "group_sum"):
+        return "extract_group"
     if name.startswith("extract"):
-        return "extract"
+        return name
     if name.startswith("pll"):
         return "pll"
     if name in ("demod", "am"):
@@ -222,10 +248,10 @@ def stage_key(name):
 # DRAM bytes per launch of the dominant kernel, read+write, from an ncu
 # capture (--set full) of that kernel on the same workload; None where no
 # capture exists.
-NCU_TRAFFIC = {("fm_band", "extract"): 8.58e6, ("mixed", "extract"): 8.91e6,
+NCU_TRAFFIC = {("fm_band", "extract_dense"): 8.58e6,
                # k_extract_mod captured at 512 headroom channels (10.5 MB read, 42.2 MB
                # of partial sums written), scaled by the channel count to 2048
-               ("headroom", "extract"): 52.6e6 * 2048 / 512}
+               ("headroom", "extract_mod"): 52.6e6 * 2048 / 512}
 
 
 def measured_peaks():
@@ -843,7 +869,7 @@ def run_headroom(args, world, rank, local):
             if k not in ("h2d", "d2h") and not k.startswith("wait")}
     block_ms = t_ms / args.steps
     work = algorithmic_work(chan_dicts(), n_in=blk)
-    b_min = sum(v["bytes"] for k, v in work.items() if isinstance(v, dict))
+    b_min = sum(v["bytes"] for k, v in work.items() if isinstance(v, dict) and not k.startswith("extract_"))
     t_roof = max(flop / args.steps / (fp32 * 1e12), b_min / (hbm_peak * 1e9)) * 1e3
     dom = max(kern, key=kern.get)
     dk = stage_key(dom)
