@@ -298,6 +298,7 @@ struct gpud_runner {
     WfmTapsHost *d_wtaps = nullptr;
     BinadeTable *d_tabs = nullptr;
     std::vector<int> class_rate;  // rate of each WFM rate class
+    std::vector<gpud_autotune_entry> tune;  // per (taps, decimation) extraction form overrides
     AudState *d_aud = nullptr;    // per slot
     double *d_d1taps = nullptr;   // per slot: pre-demod decimator taps
     float2 *d_d1hist = nullptr;   // per slot: its 100-sample history
@@ -1478,25 +1479,66 @@ GPUD_API int GPUD_CALL gpud_runner_channel_footprint(gpud_runner *r, const gpud_
 // form (phase groups of raw samples); else the dense kernel when all D phases
 // of a 256-output tile fit in shared memory (L <= 16); else phase groups of
 // at most pg phases each (large D, long arms); else the wide kernel.
-static void choose_extraction(Slot &s) {
-    s.ng = 1;
-    s.pg = s.P;
-    const bool mod = s.L <= kModMaxL;
-    if (!mod && s.L <= kDenseMaxL && dense_smem_bytes_host(s.P, s.L) <= kDenseSmemLimit) {
-        s.ext_kind = 0;
-        return;
-    }
+// Largest group of phases within a shared-memory budget (0: none).
+static int largest_group(const Slot &s, bool mod, int budget) {
     int pmax = 0;
-    for (int lo = 1, hi = s.P; lo <= hi;) {  // largest group within the shared-memory target
+    for (int lo = 1, hi = s.P; lo <= hi;) {
         int mid = (lo + hi) / 2;
-        if (mod ? mod_smem_bytes_host(mid, s.L) <= kModSmemTarget
-                : group_smem_bytes_host(mid, s.L) <= kGroupSmemTarget) {
+        if ((mod ? mod_smem_bytes_host(mid, s.L) : group_smem_bytes_host(mid, s.L)) <= budget) {
             pmax = mid;
             lo = mid + 1;
         } else {
             hi = mid - 1;
         }
     }
+    return pmax;
+}
+
+constexpr int kFormSmemCap = 220 * 1024;  // the dynamic shared memory the grouped kernels opt in to
+
+// Whether an autotune entry's form can run a channel of this geometry.
+static bool form_valid(int T, int D, int form, int pg) {
+    Slot s;
+    s.T = T;
+    s.D = D;
+    s.P = std::min(D, T);
+    s.L = (T + D - 1) / D;
+    switch (form) {
+    case GPUD_FORM_DENSE: return s.L >= 2 && s.L <= kDenseMaxL && dense_smem_bytes_host(s.P, s.L) <= kDenseSmemLimit;
+    case GPUD_FORM_WIDE: return wide_smem_bytes_host(T) <= 64 * 1024;
+    case GPUD_FORM_GROUP:
+        return pg > 0 ? pg <= s.P && group_smem_bytes_host(pg, s.L) <= kFormSmemCap
+                      : largest_group(s, false, kGroupSmemTarget) > 0;
+    case GPUD_FORM_MOD:
+        if (s.L > kModMaxL) return false;
+        return pg > 0 ? pg <= s.P && mod_smem_bytes_host(pg, s.L) <= kFormSmemCap
+                      : largest_group(s, true, kModSmemTarget) > 0;
+    default: return false;
+    }
+}
+
+static void choose_extraction(gpud_runner *r, Slot &s) {
+    s.ng = 1;
+    s.pg = s.P;
+    for (const auto &e : r->tune) {
+        if (e.taps != s.T || e.decim != s.D) continue;
+        if (e.form == GPUD_FORM_DENSE || e.form == GPUD_FORM_WIDE) {
+            s.ext_kind = e.form == GPUD_FORM_DENSE ? 0 : 1;
+            return;
+        }
+        const bool m = e.form == GPUD_FORM_MOD;
+        int pg = e.group_phases > 0 ? e.group_phases : largest_group(s, m, m ? kModSmemTarget : kGroupSmemTarget);
+        s.ext_kind = m ? 3 : 2;
+        s.ng = (s.P + pg - 1) / pg;
+        s.pg = (s.P + s.ng - 1) / s.ng;
+        return;
+    }
+    const bool mod = s.L <= kModMaxL;
+    if (!mod && s.L <= kDenseMaxL && dense_smem_bytes_host(s.P, s.L) <= kDenseSmemLimit) {
+        s.ext_kind = 0;
+        return;
+    }
+    const int pmax = largest_group(s, mod, mod ? kModSmemTarget : kGroupSmemTarget);
     if (pmax == 0) {
         s.ext_kind = 1;
         return;
@@ -1581,7 +1623,7 @@ static int admit_core(gpud_runner *r, const gpud_channel_spec *spec, int D, int 
         s.rs_L = r->rs_lmk[(size_t)rsclass].x;
         s.rs_M = r->rs_lmk[(size_t)rsclass].y;
     }
-    choose_extraction(s);
+    choose_extraction(r, s);
     s.footprint = fp;
     // The slot's memory is unused by every block in flight: write it now.
     std::vector<float> pm, h;
@@ -2176,5 +2218,32 @@ GPUD_API int GPUD_CALL gpud_demod_audio_segment(int mode, const gpud_float2 *iq,
     }
     gpud_runner_destroy(r);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// autotune table
+// ---------------------------------------------------------------------------
+GPUD_API int GPUD_CALL gpud_runner_set_autotune_table(gpud_runner *r, const gpud_autotune_entry *entries, int count) {
+    if (!r || count < 0 || (count > 0 && !entries)) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    for (int i = 0; i < count; ++i) {
+        const gpud_autotune_entry &e = entries[i];
+        if (e.taps <= 0 || e.decim <= 0 || e.group_phases < 0 || !form_valid(e.taps, e.decim, e.form, e.group_phases))
+            return set_err(r, GPUD_E_ARG, "autotune entry: form not valid for its geometry");
+    }
+    r->tune.assign(entries, entries + count);
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_channel_form(gpud_runner *r, int slot, int *form, int *group_phases, int *groups) {
+    if (!r || !form || !group_phases || !groups) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    if (slot < 0 || slot >= r->max_ch || !r->slots[(size_t)slot].active) return set_err(r, GPUD_E_SLOT, "bad slot");
+    const Slot &s = r->slots[(size_t)slot];
+    static const int kind_form[4] = {GPUD_FORM_DENSE, GPUD_FORM_WIDE, GPUD_FORM_GROUP, GPUD_FORM_MOD};
+    *form = kind_form[s.ext_kind];
+    *group_phases = s.pg;
+    *groups = s.ng;
+    return 0;
 }
 

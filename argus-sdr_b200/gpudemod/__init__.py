@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import BatchAudioResult, RDSJob, RDSResult, SegmentAudioResult, ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
+from ._lib import AutotuneEntry, BatchAudioResult, RDSJob, RDSResult, SegmentAudioResult, ChannelResult, ChannelSpec, PilotJob, PilotResult, RunnerStats, StageTime, lib
 
 # DemodType (gpudemod.go:69-76) -> runner modes
 DemodNFM, DemodWFM, DemodAM, DemodUSB, DemodLSB, DemodCW = range(6)
@@ -26,6 +26,7 @@ MODE_BY_NAME = {"IQ": MODE_IQ, "NFM": MODE_NFM, "WFM": MODE_WFM, "WFM_STEREO": M
                 "USB": MODE_USB, "LSB": MODE_LSB, "CW": MODE_CW}
 CH_EMIT_IQ, CH_RDS, CH_AUDIO48K, CH_DEEMPH75, CH_NO_DEEMPH = 1, 2, 4, 8, 16
 CH_PCM_F32, CH_BATCH_STEREO, CH_FREE_STEREO = 32, 64, 128
+FORM_DENSE, FORM_WIDE, FORM_GROUP, FORM_MOD = 0, 1, 2, 3
 SCHED_BATCHED, SCHED_PLAIN = 0, 1
 
 E_ARG, E_DECIM, E_TAPS, E_BUDGET, E_SLOTS, E_SLOT, E_BLOCK, E_TIMEOUT, E_CUDA, E_MODE, E_DEVICE_STATUS, E_STATE = \
@@ -178,6 +179,18 @@ class ChannelRunner:
 
     def update(self, slot: int, offset_hz: float, bandwidth: float):
         _check(self._r, lib.gpud_runner_update(self._r, int(slot), float(offset_hz), float(bandwidth)))
+
+    def set_autotune_table(self, entries):
+        """entries: (taps, decim, form, group_phases) overrides of the
+        extraction form per channel class (gpud_runner_set_autotune_table)."""
+        arr = (AutotuneEntry * max(1, len(entries)))(*[AutotuneEntry(*map(int, e)) for e in entries])
+        _check(self._r, lib.gpud_runner_set_autotune_table(self._r, arr, len(entries)))
+
+    def channel_form(self, slot: int):
+        """(form, phases per group, groups) of an admitted channel."""
+        f, pg, ng = C.c_int(), C.c_int(), C.c_int()
+        _check(self._r, lib.gpud_runner_channel_form(self._r, int(slot), C.byref(f), C.byref(pg), C.byref(ng)))
+        return f.value, pg.value, ng.value
 
     def set_schedule(self, schedule: int):
         _check(self._r, lib.gpud_runner_set_schedule(self._r, int(schedule)))

@@ -77,6 +77,10 @@ class RDSResult(C.Structure):
                 ("pad", C.c_uint16), ("ps", C.c_char * 9), ("rt", C.c_char * 65), ("pad2", C.c_char * 2)]
 
 
+class AutotuneEntry(C.Structure):
+    _fields_ = [("taps", C.c_int32), ("decim", C.c_int32), ("form", C.c_int32), ("group_phases", C.c_int32)]
+
+
 class IQFileMeta(C.Structure):
     _fields_ = [("sample_rate", C.c_int64), ("center_hz", C.c_double), ("samples", C.c_int64)]
 
@@ -146,6 +150,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         # runner
         "gpud_runner_create": (i, [i, i, i, i, C.c_uint64, C.POINTER(P)]),
         "gpud_runner_destroy": (i, [P]),
+        "gpud_runner_set_autotune_table": (i, [P, C.POINTER(AutotuneEntry), i]),
+        "gpud_runner_channel_form": (i, [P, i, pi, pi, pi]),
         "gpud_wfm_batch_audio": (i, [P, i, i, i, d, d, d, P, i, C.POINTER(BatchAudioResult)]),
         "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
         "gpud_iqfile_write": (i, [C.c_char_p, P, C.c_int64, C.c_int64, d]),

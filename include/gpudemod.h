@@ -13,8 +13,9 @@
  * Part 2 is the batched / serving runner that replaces the reference's
  * per-signal Go loop (BatchRunner.StreamingExtractGPU ->
  * executeStreamingGPUNativePrepared, streaming_gpu_native_prepare.go:17-108)
- * with one device-resident channel table, one fused launch sequence per IQ
- * block captured in a CUDA graph, and the demod chain (FM discriminator,
+ * with one device-resident channel table, one launch sequence per IQ block
+ * for all channels (up to three blocks in flight on their own streams,
+ * ordered by events), and the demod chain (FM discriminator,
  * AM, SSB, CW, WFM stereo with pilot PLL, RDS baseband) on the device.
  * Its return-code space extends the reference's with new negative codes only
  * (GPUD_E_*), none reused with another meaning.
@@ -192,7 +193,7 @@ enum {
 #define GPUD_CH_FREE_STEREO 128
 
 /* Schedules for gpud_runner_set_schedule. */
-#define GPUD_SCHED_BATCHED 0 /* one fused launch sequence for all channels (graph-captured) */
+#define GPUD_SCHED_BATCHED 0 /* one launch sequence per block for all channels */
 #define GPUD_SCHED_PLAIN 1   /* per-signal, synchronous: H2D, launches, D2H per channel */
 
 /* StreamingExtractJob (gpudemod/streaming_types.go:8-15) plus the demod mode. */
@@ -244,6 +245,22 @@ typedef struct {
     const float *pcm_f32;  /* GPUD_CH_AUDIO48K | GPUD_CH_PCM_F32: float samples (then pcm is NULL) */
 } gpud_channel_result;
 
+/* Extraction kernel forms (gpud_autotune_entry.form). */
+#define GPUD_FORM_DENSE 0 /* all D phases of a 256-output tile in shared memory (2 <= ceil(T/D) <= 16) */
+#define GPUD_FORM_WIDE 1  /* one warp per output, lanes over taps */
+#define GPUD_FORM_GROUP 2 /* phase groups of rotated samples; long arms in sliding windows */
+#define GPUD_FORM_MOD 3   /* phase groups of raw samples, NCO folded into the taps (ceil(T/D) <= 4) */
+
+/* One autotune override: channels with this applied tap count and decimation
+ * use `form`; group_phases (GROUP / MOD) fixes the phases per group, 0 lets
+ * the runner size it. */
+typedef struct {
+    int32_t taps;
+    int32_t decim;
+    int32_t form;
+    int32_t group_phases;
+} gpud_autotune_entry;
+
 /* Runner statistics. */
 typedef struct {
     uint64_t blocks;
@@ -274,6 +291,14 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r);
 /* Admit a channel (slot state resident on the device).  Refused with
  * GPUD_E_BUDGET when the channel's device footprint would exceed the budget,
  * GPUD_E_SLOTS at the channel cap.  New channels join at the next block. */
+/* Replaces the autotune table (count 0: none; the built-in rule then picks
+ * every channel's form).  Entries whose form cannot run their geometry are
+ * refused (GPUD_E_ARG).  Applies to channels admitted afterwards; a
+ * channel's form depends on its class alone, so its output is the same alone
+ * and in any mix under one table. */
+GPUD_API int GPUD_CALL gpud_runner_set_autotune_table(gpud_runner *r, const gpud_autotune_entry *entries, int count);
+/* The extraction form, phases per group and group count of an admitted channel. */
+GPUD_API int GPUD_CALL gpud_runner_channel_form(gpud_runner *r, int slot, int *form, int *group_phases, int *groups);
 GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out);
 GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot);
 /* Offset / bandwidth drift: the NCO increment follows the offset with the
