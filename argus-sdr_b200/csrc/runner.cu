@@ -37,6 +37,10 @@ struct WfmTaps;
 cudaError_t launch_extract_dense(int L, int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                  const float2 *hist, const float *taps, float2 *ext);
+cudaError_t launch_extract_dense_pipe(int L, int ng, int ntiles, int grid, int pmax, cudaStream_t sm,
+                                      const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                                      const ChanState *st, const float2 *x, int n, const float2 *hist,
+                                      const float *taps, float2 *ext, unsigned *fault);
 cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                 const float2 *hist, const float *taps, float2 *ext);
@@ -79,6 +83,7 @@ int audio48_tile();
 int rds_smem_bytes(int dr);
 int rds_tile();
 int dense_smem_bytes_host(int P, int L);
+int dense_pipe_groups_host(int P, int L, int cap);
 int dense_tile();
 int wide_smem_bytes_host(int T);
 int group_smem_bytes_host(int Pc, int L);
@@ -101,6 +106,10 @@ constexpr int kAudioDlStrideH = kWfmHist + 4;
 constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
+constexpr int kDensePipeSmemCap = 220 * 1024;  // what the pipelined dense kernel opts in to
+#ifndef GPUD_DENSE_PIPE
+#define GPUD_DENSE_PIPE 2  // most consumer groups of the pipelined dense kernel (0: one-tile-per-CTA kernel only)
+#endif
 constexpr int kGroupSmemTarget = 100 * 1024;  // two CTAs per SM
 constexpr int kModSmemTarget = 72 * 1024;     // three CTAs per SM
 constexpr int kModMaxL = 4;
@@ -212,6 +221,7 @@ struct BlockPlan {
     // work lists
     std::vector<int2> w_dense[kDenseMaxL + 1];
     int dense_smem[kDenseMaxL + 1] = {};
+    int dense_pmax[kDenseMaxL + 1] = {};  // most phases of a class's channels (pipelined form layout)
     std::vector<int2> w_wide;
     int wide_smem = 0;
     std::vector<int2> w_group, w_gsum;  // (entry, tile*ng + group), (entry, 256-output tile)
@@ -309,6 +319,9 @@ struct gpud_runner {
     bool pll_parallel = true;
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
+    // fault word the pipelined extraction kernel writes when a bounded wait
+    // gives up (page-locked, mapped into the device)
+    unsigned *h_fault = nullptr, *d_fault = nullptr;
     // frames
     Frame fr[kFrames];
     int nxt = 0;        // frame the next block uses
@@ -670,6 +683,13 @@ static int finish_frame(gpud_runner *r, int fi, int timeout_ms) {
     r->done_frame = fi;
     record_latency(r, f);
     prof_collect(r, f);
+    if (r->h_fault && *(volatile unsigned *)r->h_fault != 0) {
+        const unsigned code = *(volatile unsigned *)r->h_fault;
+        *(volatile unsigned *)r->h_fault = 0;
+        return set_err(r, GPUD_E_DEVICE_STATUS,
+                       code == 1 ? "extraction: producer wait for a free staging buffer gave up"
+                                 : "extraction: wait for a staged tile gave up");
+    }
     return 0;
 }
 
@@ -810,6 +830,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     for (int L = 0; L <= kDenseMaxL; ++L) {
         pl.w_dense[L].clear();
         pl.dense_smem[L] = 0;
+        pl.dense_pmax[L] = 0;
     }
     pl.w_wide.clear();
     pl.wide_smem = 0;
@@ -835,6 +856,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             if (s.ext_kind == 0) {
                 for (int t = 0; t * dense_tile() < sb.n_out; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
                 pl.dense_smem[s.L] = std::max(pl.dense_smem[s.L], dense_smem_bytes_host(s.P, s.L));
+                pl.dense_pmax[s.L] = std::max(pl.dense_pmax[s.L], s.P);
             } else if (s.ext_kind == 2 || s.ext_kind == 3) {
                 auto &wl = s.ext_kind == 2 ? pl.w_group : pl.w_mod;
                 for (int t = 0; t * dense_tile() < sb.n_out; ++t)
@@ -1048,8 +1070,17 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         if (pl.w_dense[L].empty()) continue;
         prof_mark(r, f, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str()
                                 : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
-        CK(launch_extract_dense(L, (int)pl.w_dense[L].size(), pl.dense_smem[L], f.s, d_w + w_dense_off[L], d_sb,
-                                r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
+        const int ntiles = (int)pl.w_dense[L].size();
+        const int ng = std::min(GPUD_DENSE_PIPE, dense_pipe_groups_host(pl.dense_pmax[L], L, kDensePipeSmemCap));
+        if (ng > 0 && r->d_fault && ((uintptr_t)x_dev & 15) == 0) {
+            // persistent: one CTA per SM over contiguous runs of tiles
+            CK(launch_extract_dense_pipe(L, ng, ntiles, std::min(ntiles, r->num_sms), pl.dense_pmax[L], f.s,
+                                         d_w + w_dense_off[L], d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist,
+                                         r->d_taps, d_ext, r->d_fault));
+        } else {
+            CK(launch_extract_dense(L, ntiles, pl.dense_smem[L], f.s, d_w + w_dense_off[L], d_sb, r->d_prm,
+                                    r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
+        }
         nl++;
     }
     if (!pl.w_group.empty()) {
@@ -1374,6 +1405,9 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
             r->num_sms = sms;
     }
+    CKC(cudaHostAlloc((void **)&r->h_fault, 64, cudaHostAllocMapped));
+    *(volatile unsigned *)r->h_fault = 0;
+    CKC(cudaHostGetDevicePointer((void **)&r->d_fault, r->h_fault, 0));
     for (auto &f : r->fr) {
         CKC(cudaStreamCreateWithFlags(&f.s, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_front, cudaEventDisableTiming));
@@ -1428,6 +1462,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         for (auto e : f.prof_ev) cudaEventDestroy(e);
         if (f.s) cudaStreamDestroy(f.s);
     }
+    if (r->h_fault) cudaFreeHost(r->h_fault);
     cudaFree(r->d_prm);
     cudaFree(r->d_st);
     cudaFree(r->d_taps);

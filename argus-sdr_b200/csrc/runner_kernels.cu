@@ -347,6 +347,366 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
         });
 }
 
+// ---------------------------------------------------------------------------
+// Dense form, persistent pipelined variant (k_extract_dense_pipe<L, NG>).
+//
+// One CTA per SM walks a contiguous run of the class's tiles (consecutive
+// tiles of a channel stay together).  Warp 16 is the producer: it loads the
+// next tile's descriptors ahead of time and, as soon as the previous tile has
+// been staged, brings the next tile's polyphase taps and (for tiles inside
+// the block) its raw input span into shared memory with bulk copies whose
+// completion is counted on an mbarrier.  The 16 consumer warps form NG groups
+// that take the tiles in turn, each with its own Z: a group rotates and
+// transposes its tile from the raw span into Z (tiles that reach into the
+// history or past the block end stage from global memory as k_extract_dense
+// does), releases the raw span, then runs the FIR rows and the cross-warp
+// reduction while the other group stages the next tile.  The global-load
+// latency of the one-tile-per-CTA kernel (descriptor chain, then staging
+// loads) thereby overlaps arithmetic.  Every mbarrier wait is bounded: a wait
+// that gives up stores a code in the runner's fault word and the CTA returns
+// (the host reports GPUD_E_DEVICE_STATUS).
+//
+// Barrier use: full[g] completes once per tile of group g (the producer's
+// arrival plus the bulk-copy bytes), `empty` once per staged tile (tiles are
+// staged strictly in order, each after the previous one's release), named
+// barrier 1 + g synchronises group g.
+// ---------------------------------------------------------------------------
+constexpr int kPipeCW = 16;                     // consumer warps
+constexpr int kPipeThreads = 32 * kPipeCW + 32;  // + the producer warp
+constexpr int kPipeMaxRounds = 64;              // staging rounds per tile (two table entries per producer lane)
+constexpr unsigned kPipeWaitPolls = 1u << 22;
+
+struct PipeDesc {
+    const float2 *hist;
+    uint64_t u0, inc;
+    int j0, n_out, ext_off, ibase, total, nk, D, P, H, precise, tma, off;
+};
+static_assert(32 + sizeof(PipeDesc) <= 128, "the descriptor sits between the mbarriers and the rotation table");
+
+struct PipeLayout {
+    int o_w, o_taps, tstride, o_z, zstride, o_r, bytes;
+};
+
+// Shared memory of a launch whose channels have at most pmax phases, ng
+// consumer groups: mbarriers (full[2], empty) | descriptor | rotation table |
+// taps x4 | Z (and reduction) per group | raw span.
+__host__ __device__ inline PipeLayout pipe_layout(int pmax, int L, int ng) {
+    PipeLayout lo;
+    lo.o_w = 128;
+    lo.o_taps = lo.o_w + kPipeMaxRounds * 8;
+    lo.tstride = (pmax * L + 3) & ~3;  // floats; bulk-copy sizes are multiples of 16 bytes
+    lo.o_z = lo.o_taps + 4 * lo.tstride * 4;
+    const int z = pmax * dense_row_stride(L) * 8;
+    const int red = (kPipeCW / ng) * kRedStride * 16;
+    lo.zstride = ((z > red ? z : red) + 15) & ~15;
+    lo.o_r = lo.o_z + ng * lo.zstride;
+    lo.bytes = lo.o_r + (((pmax * (kDenseOT + L - 1) + 2) * 8 + 15) & ~15);
+    return lo;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase of the given parity: false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+    for (unsigned i = 0; i < kPipeWaitPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i >= 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// Bulk copy global -> this CTA's shared memory, completion counted on bar.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void named_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Named barrier that also ORs a predicate over the participating threads.
+__device__ __forceinline__ bool named_sync_or(int id, int count, bool pred) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((unsigned)pred), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void pipe_fault(unsigned *fault, unsigned code) {
+    *(volatile unsigned *)fault = code;
+    __threadfence_system();
+}
+
+// Rows, cross-warp reduction (Z reused) and output of one tile for a consumer
+// group of GW warps synchronised on named barrier `bar`.
+template <bool PREC, int GW, class Row, class Out>
+__device__ __forceinline__ void pipe_tile_sum(int rows, int gw, int lane, int gt, int bar, const Row &row, float2 *Z,
+                                              const Out &out) {
+    constexpr int R = kDenseR;
+    constexpr int GNT = 32 * GW;
+    if constexpr (!PREC) {
+        float ar[R], ai[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
+        for (int pp = gw; pp < rows; pp += GW) row(pp, lane, ar, ai);
+        named_sync(bar, GNT);
+        float2 *red = Z + gw * kRedStride;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int o = lane * R + r;
+            red[o + (o >> 3)] = make_float2(ar[r], ai[r]);
+        }
+        named_sync(bar, GNT);
+        for (int o = gt; o < kDenseOT; o += GNT) {
+            float2 sum = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int wv = 0; wv < GW; ++wv) {
+                const float2 v = Z[wv * kRedStride + o + (o >> 3)];
+                sum.x += v.x;
+                sum.y += v.y;
+            }
+            out(o, sum);
+        }
+    } else {
+        double dr[R], di[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) dr[r] = di[r] = 0.0;
+        for (int pp = gw; pp < rows; pp += GW) {
+            float ar[R], ai[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) ar[r] = ai[r] = 0.f;
+            row(pp, lane, ar, ai);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                dr[r] += (double)ar[r];
+                di[r] += (double)ai[r];
+            }
+        }
+        named_sync(bar, GNT);
+        double2 *Z64 = reinterpret_cast<double2 *>(Z);
+        double2 *red = Z64 + gw * kRedStride;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int o = lane * R + r;
+            red[o + (o >> 3)] = make_double2(dr[r], di[r]);
+        }
+        named_sync(bar, GNT);
+        for (int o = gt; o < kDenseOT; o += GNT) {
+            double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int wv = 0; wv < GW; ++wv) {
+                const double2 v = Z64[wv * kRedStride + o + (o >> 3)];
+                sum.x += v.x;
+                sum.y += v.y;
+            }
+            out(o, sum);
+        }
+    }
+}
+
+template <int L, int NG>
+__global__ void __launch_bounds__(kPipeThreads, 1)
+k_extract_dense_pipe(const int2 *__restrict__ work, int ntiles, int pmax, const SlotBlock *__restrict__ sbt,
+                     const ChanParams *__restrict__ prm, const ChanState *__restrict__ st,
+                     const float2 *__restrict__ x, int n, const float2 *__restrict__ hist_arena,
+                     const float *__restrict__ taps_arena, float2 *__restrict__ ext, unsigned *fault) {
+    constexpr int GW = kPipeCW / NG;  // warps per consumer group
+    constexpr int GNT = 32 * GW;      // threads per consumer group
+    extern __shared__ __align__(128) unsigned char psm[];
+    const PipeLayout lo = pipe_layout(pmax, L, NG);
+    uint64_t *full = reinterpret_cast<uint64_t *>(psm);  // full[0], full[1]
+    uint64_t *empty = full + 2;
+    PipeDesc *dsc = reinterpret_cast<PipeDesc *>(psm + 32);
+    float2 *wt = reinterpret_cast<float2 *>(psm + lo.o_w);
+    float *tsm = reinterpret_cast<float *>(psm + lo.o_taps);
+    float2 *Rw = reinterpret_cast<float2 *>(psm + lo.o_r);
+    const int b0 = (int)((long long)ntiles * blockIdx.x / gridDim.x);
+    const int b1 = (int)((long long)ntiles * (blockIdx.x + 1) / gridDim.x);
+    const int nt = b1 - b0;
+    if (threadIdx.x == 0) {
+        mbar_init(full, 1);
+        mbar_init(full + 1, 1);
+        mbar_init(empty, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int M = kDenseOT + L - 1;
+    const int Mp = dense_row_stride(L);
+
+    if (warp == kPipeCW) {
+        // ---- producer ----
+        for (int it = 0; it < nt; ++it) {
+            const int2 w = work[b0 + it];
+            const SlotBlock &sb = sbt[w.x];
+            const ChanParams &cp = prm[sb.slot];
+            PipeDesc d;
+            d.D = cp.decim;
+            d.P = cp.nphase;
+            d.j0 = w.y * kDenseOT;
+            d.n_out = sb.n_out;
+            d.ext_off = sb.ext_off;
+            d.u0 = st[sb.slot].nco_q;
+            d.inc = cp.inc_q;
+            d.ibase = (d.D - sb.pc - 1) + (d.j0 - (L - 1)) * d.D - (d.D - 1);
+            d.total = d.P * M;
+            d.nk = (d.total + GNT - 1) / GNT;
+            d.hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+            d.H = sb.hist_len;
+            d.precise = cp.precise_sum;
+            const int a0 = d.ibase & ~1;
+            const int cnt = (d.ibase - a0 + d.total + 1) & ~1;
+            d.tma = d.ibase >= 0 && (long long)a0 + cnt <= (long long)n;
+            d.off = d.tma ? d.ibase - a0 : 0;
+            // rotation of staging round k: exp(j k GNT inc), exact from the Q0.64 phase
+            const float2 w0 = q64_phasor((uint64_t)lane * (uint64_t)GNT * d.inc);
+            const float2 w1 = q64_phasor((uint64_t)(lane + 32) * (uint64_t)GNT * d.inc);
+            const float *tsrc = taps_arena + cp.taps_off;
+            // the previous tile has been staged: the raw span, the table and
+            // the descriptor are free; taps buffer it & 3 was last read by
+            // tile it - 4, finished before tile it - 2 of its group was staged
+            if (it > 0 && !mbar_wait_bounded(empty, (unsigned)(it - 1) & 1u)) {
+                if (lane == 0) pipe_fault(fault, 1u);
+                return;
+            }
+            if (lane < d.nk) wt[lane] = w0;
+            if (lane + 32 < d.nk) wt[lane + 32] = w1;
+            if (lane == 0) *dsc = d;
+            __syncwarp();
+            if (lane == 0) {
+                uint64_t *fb = full + (NG == 2 ? (it & 1) : 0);
+                const unsigned tb = (unsigned)(((d.P * L + 3) & ~3) * 4);
+                const unsigned rb = d.tma ? (unsigned)cnt * 8u : 0u;
+                mbar_arrive_expect_tx(fb, tb + rb);
+                bulk_to_smem(tsm + (it & 3) * lo.tstride, tsrc, tb, fb);
+                if (d.tma) bulk_to_smem(Rw, x + a0, rb, fb);
+            }
+        }
+        return;
+    }
+
+    // ---- consumers: group g takes tiles g, g + NG, ... ----
+    const int g = warp / GW, gw = warp - g * GW;
+    const int gt = (int)threadIdx.x - g * GNT;
+    float2 *Z = reinterpret_cast<float2 *>(psm + lo.o_z + g * lo.zstride);
+    uint64_t *fb = full + g;
+    for (int it = g, kl = 0; it < nt; it += NG, ++kl) {
+        const bool ok = mbar_wait_bounded(fb, (unsigned)kl & 1u);
+        // the group has read its previous tile's reduction; all agree whether
+        // to go on
+        if (named_sync_or(1 + g, GNT, !ok)) {
+            if (gt == 0) pipe_fault(fault, 2u);
+            return;
+        }
+        const PipeDesc d = *dsc;
+        const int D = d.D;
+        const float2 a = q64_phasor(d.u0 + (uint64_t)(int64_t)(d.ibase + gt) * d.inc);
+        int mr = gt / D, q = gt - (gt / D) * D;
+        const int dm = GNT / D, dq = GNT - dm * D;
+        if (d.tma) {
+            const float2 *sp = Rw + d.off + gt;
+            const int nfull = d.total / GNT;
+            int k = 0;
+            if ((GNT / 8) % D == 0) {
+                // the thread's phase row is fixed and its padded column
+                // advances by the constant dm + dm/8 (dm a multiple of 8)
+                float2 *zp = Z + (D - 1 - q) * Mp + mr + (mr >> 3);
+                const int dz = dm + (dm >> 3);
+                for (; k + 4 <= nfull; k += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) zp[(k + u) * dz] = cmulf(sp[(k + u) * GNT], cmulf(a, wt[k + u]));
+                }
+                for (; k < nfull; ++k) zp[k * dz] = cmulf(sp[k * GNT], cmulf(a, wt[k]));
+                mr += k * dm;
+            }
+            for (; k < d.nk; ++k) {
+                if (gt + k * GNT < d.total)
+                    Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = cmulf(sp[k * GNT], cmulf(a, wt[k]));
+                q += dq;
+                mr += dm;
+                if (q >= D) {
+                    q -= D;
+                    ++mr;
+                }
+            }
+        } else {
+            // tile at a block edge: history before sample 0, zeros past n
+            for (int k = 0; k < d.nk; ++k) {
+                const int ip = gt + k * GNT;
+                if (ip < d.total) {
+                    const int i = d.ibase + ip;
+                    float2 v;
+                    if (i >= 0) {
+                        v = i < n ? cmulf(__ldg(x + i), cmulf(a, wt[k])) : make_float2(0.f, 0.f);
+                    } else {
+                        const int hi = d.H + i;
+                        v = hi >= 0 ? d.hist[hi] : make_float2(0.f, 0.f);
+                    }
+                    Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = v;
+                }
+                q += dq;
+                mr += dm;
+                if (q >= D) {
+                    q -= D;
+                    ++mr;
+                }
+            }
+        }
+        named_sync(1 + g, GNT);
+        if (gt == 0) mbar_arrive(empty);  // the raw span, the table and the descriptor may be refilled
+
+        const float *hb = tsm + (it & 3) * lo.tstride;
+        auto row = [&](int p, int ln, float *ar, float *ai) { group_row<L>(Z + p * Mp, hb + p * L, ln, ar, ai); };
+        float2 *dst = ext + d.ext_off + d.j0;
+        const int nv = d.n_out - d.j0;
+        if (d.precise)
+            pipe_tile_sum<true, GW>(d.P, gw, lane, gt, 1 + g, row, Z, [&](int o, double2 v) {
+                if (o < nv) dst[o] = make_float2((float)v.x, (float)v.y);
+            });
+        else
+            pipe_tile_sum<false, GW>(d.P, gw, lane, gt, 1 + g, row, Z, [&](int o, float2 v) {
+                if (o < nv) dst[o] = v;
+            });
+    }
+}
+
 // Wide form (short polyphase arms, or tiles too large for shared memory): one
 // warp per kWideOPW outputs, lanes stride the taps, warp-shuffle reduction.
 // The NCO rotation is folded into the taps: for a sample of this block,
@@ -2136,6 +2496,54 @@ cudaError_t launch_extract_dense(int L, int grid, int smem, cudaStream_t sm, con
     switch (L) {
 #define GPUD_CASE(LL) \
     case LL: return launch_dense_L<LL>(grid, smem, sm, work, sbt, prm, st, x, n, hist, taps, ext);
+        GPUD_CASE(2) GPUD_CASE(3) GPUD_CASE(4) GPUD_CASE(5) GPUD_CASE(6) GPUD_CASE(7) GPUD_CASE(8)
+        GPUD_CASE(9) GPUD_CASE(10) GPUD_CASE(11) GPUD_CASE(12) GPUD_CASE(13) GPUD_CASE(14)
+        GPUD_CASE(15) GPUD_CASE(16)
+#undef GPUD_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int L, int NG>
+static cudaError_t launch_dense_pipe_LG(int ntiles, int grid, int pmax, cudaStream_t sm, const int2 *work,
+                                        const SlotBlock *sbt, const ChanParams *prm, const ChanState *st,
+                                        const float2 *x, int n, const float2 *hist, const float *taps, float2 *ext,
+                                        unsigned *fault) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_extract_dense_pipe<L, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        attr_set = true;
+    }
+    const int smem = pipe_layout(pmax, L, NG).bytes;
+    k_extract_dense_pipe<L, NG><<<grid, kPipeThreads, smem, sm>>>(work, ntiles, pmax, sbt, prm, st, x, n, hist,
+                                                                  taps, ext, fault);
+    return cudaGetLastError();
+}
+
+// Consumer groups of the pipelined dense form for a class whose channels have
+// at most P phases (two when both groups' Z fit beside the raw span), or 0
+// when it does not fit in cap bytes or needs more rotation-table rounds than
+// the producer warp fills.
+int dense_pipe_groups_host(int P, int L, int cap) {
+    const int total = P * (kDenseOT + L - 1);
+    if (total <= kPipeMaxRounds * 32 * (kPipeCW / 2) && pipe_layout(P, L, 2).bytes <= cap) return 2;
+    if (total <= kPipeMaxRounds * 32 * kPipeCW && pipe_layout(P, L, 1).bytes <= cap) return 1;
+    return 0;
+}
+
+cudaError_t launch_extract_dense_pipe(int L, int ng, int ntiles, int grid, int pmax, cudaStream_t sm,
+                                      const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
+                                      const ChanState *st, const float2 *x, int n, const float2 *hist,
+                                      const float *taps, float2 *ext, unsigned *fault) {
+    if (((uintptr_t)x & 15) != 0 || (ng != 1 && ng != 2)) return cudaErrorInvalidValue;
+    switch (L * 4 + ng) {
+#define GPUD_CASE(LL)                                                                                              \
+    case LL * 4 + 1:                                                                                               \
+        return launch_dense_pipe_LG<LL, 1>(ntiles, grid, pmax, sm, work, sbt, prm, st, x, n, hist, taps, ext,     \
+                                           fault);                                                                 \
+    case LL * 4 + 2:                                                                                               \
+        return launch_dense_pipe_LG<LL, 2>(ntiles, grid, pmax, sm, work, sbt, prm, st, x, n, hist, taps, ext,     \
+                                           fault);
         GPUD_CASE(2) GPUD_CASE(3) GPUD_CASE(4) GPUD_CASE(5) GPUD_CASE(6) GPUD_CASE(7) GPUD_CASE(8)
         GPUD_CASE(9) GPUD_CASE(10) GPUD_CASE(11) GPUD_CASE(12) GPUD_CASE(13) GPUD_CASE(14)
         GPUD_CASE(15) GPUD_CASE(16)
