@@ -149,6 +149,20 @@ struct SlotBlock {
     int32_t pad_sb;
 };
 
+// Channel group extracted on the tensor cores (gemm_extract.cu): channels of
+// one decimation D, tap count T and phase count pc share the input grid.
+struct GemmGroup {
+    int32_t nmem;    // channels (members[mem_off .. mem_off + nmem): SlotBlock rows)
+    int32_t ncol;    // N = 2 * channels, padded to a multiple of 16
+    int32_t D, L, T, pc;
+    int32_t n_out;   // outputs of every member this block
+    int32_t jt0;     // first output of the group tiles (earlier ones: dense kernel)
+    int32_t b_off;   // byte offset of the packed taps in the frame's buffer
+    int32_t mem_off;
+    int32_t ns;      // taps stages in shared memory
+    int32_t na;      // TMEM accumulators (arm u accumulates into u % na; summed in the epilogue)
+};
+
 // Rational polyphase resampler bank (dsp/resample.go:45-93) for one input rate.
 constexpr int kRsTaps = 33;     // taps per arm at 32 taps per phase (odd prototype)
 struct RsBank {
@@ -171,6 +185,67 @@ struct DevResult {
     int32_t pll_iters;
     int32_t pad[2];
 };
+
+// ---------------------------------------------------------------------------
+// Shared-memory pipeline primitives (sm_90+ PTX): mbarriers with bounded
+// waits, bulk copies global -> shared counted on an mbarrier, and the fault
+// word a kernel writes when a bounded wait gives up.
+// ---------------------------------------------------------------------------
+constexpr unsigned kWaitPolls = 1u << 22;  // polls (64 ns apart after the first 64) before a wait gives up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase of the given parity: false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+    for (unsigned i = 0; i < kWaitPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i >= 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// Bulk copy global -> this CTA's shared memory, completion counted on bar.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Record a fault code in the runner's page-locked fault word (read by the host
+// once the block completes).
+__device__ __forceinline__ void device_fault(unsigned *fault, unsigned code) {
+    *(volatile unsigned *)fault = code;
+    __threadfence_system();
+}
 
 // Exact sequential float64 accumulation x_k = fl(x_{k-1} + inc), x_0 = 0
 // (dsp.FreqShift's `phase += inc`, dsp/freqshift.go:13-15), evaluated in

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <time.h>
@@ -41,6 +42,14 @@ cudaError_t launch_extract_dense_pipe(int L, int ng, int ntiles, int grid, int p
                                       const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                                       const ChanState *st, const float2 *x, int n, const float2 *hist,
                                       const float *taps, float2 *ext, unsigned *fault);
+cudaError_t launch_gemm_pack(int ngroups, int max_l, cudaStream_t sm, const GemmGroup *groups, const int *members,
+                             const SlotBlock *sbt, const ChanParams *prm, const float *taps, float *gb);
+cudaError_t launch_extract_gemm(int grid, int smem, cudaStream_t sm, const int2 *work, const GemmGroup *groups,
+                                const int *members, const SlotBlock *sbt, const ChanParams *prm, const ChanState *st,
+                                const float2 *x, int n, const float *gb, float2 *ext, unsigned *fault);
+int gemm_smem_bytes_host(int D, int L, int N, int ns);
+int gemm_tile();
+size_t gemm_pack_bytes_host(int D, int L, int N);
 cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                 const float2 *hist, const float *taps, float2 *ext);
@@ -107,6 +116,12 @@ constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
 constexpr int kDensePipeSmemCap = 220 * 1024;  // what the pipelined dense kernel opts in to
+#ifndef GPUD_GEMM_EXTRACT
+#define GPUD_GEMM_EXTRACT 1  // 0: no tensor-core channel groups
+#endif
+constexpr int kGemmMinChannels = 4;           // smaller groups stay on the dense kernel
+constexpr int kGemmSmemCap = 220 * 1024;
+constexpr int kGemmFirstOutput = 256;         // outputs before it (history) stay on the dense kernel
 #ifndef GPUD_DENSE_PIPE
 #define GPUD_DENSE_PIPE 2  // most consumer groups of the pipelined dense kernel (0: one-tile-per-CTA kernel only)
 #endif
@@ -222,6 +237,12 @@ struct BlockPlan {
     std::vector<int2> w_dense[kDenseMaxL + 1];
     int dense_smem[kDenseMaxL + 1] = {};
     int dense_pmax[kDenseMaxL + 1] = {};  // most phases of a class's channels (pipelined form layout)
+    // tensor-core channel groups (gemm_extract.cu)
+    std::vector<GemmGroup> groups;
+    std::vector<int> gmembers;            // SlotBlock rows of the groups' channels
+    std::vector<int2> w_gemm;             // (group, 128-output tile from kGemmFirstOutput)
+    int gemm_smem = 0, gemm_max_l = 0;
+    size_t gemm_b_bytes = 0;              // packed taps of all groups
     std::vector<int2> w_wide;
     int wide_smem = 0;
     std::vector<int2> w_group, w_gsum;  // (entry, tile*ng + group), (entry, 256-output tile)
@@ -270,6 +291,8 @@ struct Frame {
     int64_t rs_cap = 0;
     double2 *d_part = nullptr;  // phase-group partial sums (double2 slots)
     int64_t part_cap = 0;
+    float *d_gb = nullptr;      // packed taps of the tensor-core channel groups
+    size_t gb_cap = 0;
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
@@ -772,6 +795,76 @@ static void plan_slot(gpud_runner *r, BlockPlan &pl, int slot, int n) {
 }
 
 // Offsets (emitting slots' IQ first so one D2H covers it) and work lists.
+// Tensor-core channel groups of a block: dense-form channels with the same
+// decimation (a multiple of 4), tap count and phase count share the input
+// grid; groups of at least kGemmMinChannels (split to fit shared memory) take
+// every output from kGemmFirstOutput on in the group kernel.  Float64-summed
+// channels stay on the dense kernel.  Returns the grouped flag of every row.
+static std::vector<char> plan_gemm_groups(gpud_runner *r, BlockPlan &pl) {
+    pl.groups.clear();
+    pl.gmembers.clear();
+    pl.w_gemm.clear();
+    pl.gemm_smem = pl.gemm_max_l = 0;
+    pl.gemm_b_bytes = 0;
+    std::vector<char> grouped(pl.sbs.size(), 0);
+    if (!GPUD_GEMM_EXTRACT || !r->d_fault) return grouped;
+    std::map<std::tuple<int, int, int>, std::vector<int>> by_key;
+    for (int i = 0; i < (int)pl.sbs.size(); ++i) {
+        const SlotBlock &sb = pl.sbs[(size_t)i];
+        const Slot &s = r->slots[(size_t)sb.slot];
+        if (s.ext_kind != 0 || s.D % 4 != 0 || precise_sum(s.spec) || sb.n_out <= kGemmFirstOutput) continue;
+        by_key[std::make_tuple(s.D, s.T, sb.pc)].push_back(i);
+    }
+    for (auto &kv : by_key) {
+        const std::vector<int> &rows = kv.second;
+        if ((int)rows.size() < kGemmMinChannels) continue;
+        const int D = std::get<0>(kv.first), T = std::get<1>(kv.first), pc = std::get<2>(kv.first);
+        const int L = (T + D - 1) / D;
+        int cmax = 0;  // most channels per group (a multiple of 8) with two taps stages in shared memory
+        for (int c = 8; c <= 128; c += 8)
+            if (gemm_smem_bytes_host(D, L, 2 * c, 2) <= kGemmSmemCap) cmax = c;
+        if (cmax < kGemmMinChannels) continue;
+        const int nchunk = ((int)rows.size() + cmax - 1) / cmax;
+        const int per = ((int)rows.size() + nchunk - 1) / nchunk;
+        for (int c0 = 0; c0 < (int)rows.size(); c0 += per) {
+            const int C = std::min(per, (int)rows.size() - c0);
+            if (C < kGemmMinChannels) break;
+            GemmGroup g{};
+            g.nmem = C;
+            g.ncol = ((2 * C + 15) / 16) * 16;
+            g.D = D;
+            g.L = L;
+            g.T = T;
+            g.pc = pc;
+            g.n_out = pl.sbs[(size_t)rows[(size_t)c0]].n_out;
+            g.jt0 = kGemmFirstOutput;
+            g.ns = gemm_smem_bytes_host(D, L, g.ncol, 3) <= kGemmSmemCap ? 3 : 2;
+            // accumulators: as many arms apart as fit in the TMEM share of one
+            // of the CTAs that the shared memory lets reside on an SM
+            {
+                const int per_sm = std::max(1, (228 * 1024) / (gemm_smem_bytes_host(D, L, g.ncol, g.ns) + 1024));
+                int p2 = 1;
+                while (p2 < std::min(per_sm, 4)) p2 <<= 1;
+                const int cols = 512 / p2;  // a power-of-two share: the allocations of resident CTAs never wait
+                g.na = std::max(1, std::min(L, cols / g.ncol));
+            }
+            g.b_off = (int)pl.gemm_b_bytes;
+            g.mem_off = (int)pl.gmembers.size();
+            pl.gemm_b_bytes += align256(gemm_pack_bytes_host(D, L, g.ncol));
+            pl.gemm_smem = std::max(pl.gemm_smem, gemm_smem_bytes_host(D, L, g.ncol, g.ns));
+            pl.gemm_max_l = std::max(pl.gemm_max_l, L);
+            const int gi = (int)pl.groups.size();
+            for (int k = 0; k < C; ++k) {
+                pl.gmembers.push_back(rows[(size_t)(c0 + k)]);
+                grouped[(size_t)rows[(size_t)(c0 + k)]] = 1;
+            }
+            for (int t = 0; kGemmFirstOutput + t * gemm_tile() < g.n_out; ++t) pl.w_gemm.push_back(make_int2(gi, t));
+            pl.groups.push_back(g);
+        }
+    }
+    return grouped;
+}
+
 static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     int64_t ext = 0;
     pl.tot_emit_ext = 0;
@@ -849,12 +942,15 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.w_free.clear();
     pl.batch_stereo = false;
     pl.rds_smem = 0;
+    std::vector<char> grouped = plan_gemm_groups(r, pl);
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
         Slot &s = r->slots[(size_t)sb.slot];
         if (sb.n_out > 0) {
             if (s.ext_kind == 0) {
-                for (int t = 0; t * dense_tile() < sb.n_out; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
+                // a grouped channel keeps only the outputs before kGemmFirstOutput here
+                const int n_dense = grouped[(size_t)i] ? kGemmFirstOutput : sb.n_out;
+                for (int t = 0; t * dense_tile() < n_dense; ++t) pl.w_dense[s.L].push_back(make_int2(i, t));
                 pl.dense_smem[s.L] = std::max(pl.dense_smem[s.L], dense_smem_bytes_host(s.P, s.L));
                 pl.dense_pmax[s.L] = std::max(pl.dense_pmax[s.L], s.P);
             } else if (s.ext_kind == 2 || s.ext_kind == 3) {
@@ -942,9 +1038,17 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() + pl.w_gsum.size() +
-          pl.w_mod.size() + pl.w_free.size();
+          pl.w_mod.size() + pl.w_free.size() + pl.w_gemm.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
-                   align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) + 4096;
+                   align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) +
+                   align256(pl.groups.size() * sizeof(GemmGroup)) + align256(pl.gmembers.size() * 4) + 4096;
+    if (pl.gemm_b_bytes > f.gb_cap) {
+        cudaFree(f.d_gb);
+        f.d_gb = nullptr;
+        size_t cap = pl.gemm_b_bytes * 5 / 4 + 4096;
+        CK(cudaMalloc((void **)&f.d_gb, cap));
+        f.gb_cap = cap;
+    }
     if (dneed > f.desc_cap) {
         cudaFree(f.d_desc);
         if (f.h_desc) cudaFreeHost(f.h_desc);
@@ -1038,18 +1142,25 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
            o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec),
-           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod), o_free = put(pl.w_free);
+           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod), o_free = put(pl.w_free),
+           o_gemm = put(pl.w_gemm);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
     std::memcpy(hd + o_aud, pl.aud_list.data(), pl.aud_list.size() * 4);
-    size_t dbytes = o_aud + pl.aud_list.size() * 4;
+    size_t o_ggr = o_aud + align256(pl.aud_list.size() * 4);
+    std::memcpy(hd + o_ggr, pl.groups.data(), pl.groups.size() * sizeof(GemmGroup));
+    size_t o_gmem = o_ggr + align256(pl.groups.size() * sizeof(GemmGroup));
+    std::memcpy(hd + o_gmem, pl.gmembers.data(), pl.gmembers.size() * 4);
+    size_t dbytes = o_gmem + pl.gmembers.size() * 4;
     CK(cudaMemcpyAsync(f.d_desc, hd, dbytes, cudaMemcpyHostToDevice, f.s));
     f.h2d += dbytes;
     const SlotBlock *d_sb = (const SlotBlock *)(f.d_desc + o_sb);
     const int2 *d_w = (const int2 *)(f.d_desc + o_w);
     const int *d_pll = (const int *)(f.d_desc + o_pll);
     const int *d_aud_list = (const int *)(f.d_desc + o_aud);
+    const GemmGroup *d_groups = (const GemmGroup *)(f.d_desc + o_ggr);
+    const int *d_gmem = (const int *)(f.d_desc + o_gmem);
 
     // output arena: results | PCM | RDS | audio (host part, then device part) | IQ (emitted part first)
     f.off_res = 0;
@@ -1082,6 +1193,15 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                                     r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
         }
         nl++;
+    }
+    if (!pl.w_gemm.empty()) {
+        prof_mark(r, f, "gemm_pack");
+        CK(launch_gemm_pack((int)pl.groups.size(), pl.gemm_max_l, f.s, d_groups, d_gmem, d_sb, r->d_prm, r->d_taps,
+                            f.d_gb));
+        prof_mark(r, f, "extract_gemm");
+        CK(launch_extract_gemm((int)pl.w_gemm.size(), pl.gemm_smem, f.s, d_w + o_gemm, d_groups, d_gmem, d_sb,
+                               r->d_prm, r->d_st, x_dev, n, f.d_gb, d_ext, r->d_fault));
+        nl += 2;
     }
     if (!pl.w_group.empty()) {
         prof_mark(r, f, "extract_group");
@@ -1453,6 +1573,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_block);
         cudaFree(f.d_rs);
         cudaFree(f.d_part);
+        cudaFree(f.d_gb);
         if (f.h_desc) cudaFreeHost(f.h_desc);
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);

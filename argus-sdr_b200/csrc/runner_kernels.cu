@@ -374,7 +374,6 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
 constexpr int kPipeCW = 16;                     // consumer warps
 constexpr int kPipeThreads = 32 * kPipeCW + 32;  // + the producer warp
 constexpr int kPipeMaxRounds = 64;              // staging rounds per tile (two table entries per producer lane)
-constexpr unsigned kPipeWaitPolls = 1u << 22;
 
 struct PipeDesc {
     const float2 *hist;
@@ -404,53 +403,6 @@ __host__ __device__ inline PipeLayout pipe_layout(int pmax, int L, int ng) {
     return lo;
 }
 
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for the phase of the given parity: false when it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
-    for (unsigned i = 0; i < kPipeWaitPolls; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (i >= 64) __nanosleep(64);
-    }
-    return false;
-}
-
-// Bulk copy global -> this CTA's shared memory, completion counted on bar.
-// Both addresses 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
 __device__ __forceinline__ void named_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -467,11 +419,6 @@ __device__ __forceinline__ bool named_sync_or(int id, int count, bool pred) {
         : "r"((unsigned)pred), "r"(id), "r"(count)
         : "memory");
     return r != 0;
-}
-
-__device__ __forceinline__ void pipe_fault(unsigned *fault, unsigned code) {
-    *(volatile unsigned *)fault = code;
-    __threadfence_system();
 }
 
 // Rows, cross-warp reduction (Z reused) and output of one tile for a consumer
@@ -603,7 +550,7 @@ k_extract_dense_pipe(const int2 *__restrict__ work, int ntiles, int pmax, const 
             // the descriptor are free; taps buffer it & 3 was last read by
             // tile it - 4, finished before tile it - 2 of its group was staged
             if (it > 0 && !mbar_wait_bounded(empty, (unsigned)(it - 1) & 1u)) {
-                if (lane == 0) pipe_fault(fault, 1u);
+                if (lane == 0) device_fault(fault, 1u);
                 return;
             }
             if (lane < d.nk) wt[lane] = w0;
@@ -632,7 +579,7 @@ k_extract_dense_pipe(const int2 *__restrict__ work, int ntiles, int pmax, const 
         // the group has read its previous tile's reduction; all agree whether
         // to go on
         if (named_sync_or(1 + g, GNT, !ok)) {
-            if (gt == 0) pipe_fault(fault, 2u);
+            if (gt == 0) device_fault(fault, 2u);
             return;
         }
         const PipeDesc d = *dsc;
@@ -667,25 +614,37 @@ k_extract_dense_pipe(const int2 *__restrict__ work, int ntiles, int pmax, const 
                 }
             }
         } else {
-            // tile at a block edge: history before sample 0, zeros past n
-            for (int k = 0; k < d.nk; ++k) {
-                const int ip = gt + k * GNT;
-                if (ip < d.total) {
-                    const int i = d.ibase + ip;
-                    float2 v;
-                    if (i >= 0) {
-                        v = i < n ? cmulf(__ldg(x + i), cmulf(a, wt[k])) : make_float2(0.f, 0.f);
-                    } else {
-                        const int hi = d.H + i;
-                        v = hi >= 0 ? d.hist[hi] : make_float2(0.f, 0.f);
+            // tile at a block edge: history before sample 0, zeros past n;
+            // four loads in flight per thread
+            constexpr int U = 4;
+            for (int k0 = 0; k0 < d.nk; k0 += U) {
+                float2 v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int ip = gt + (k0 + u) * GNT, i = d.ibase + ip;
+                    v[u] = make_float2(0.f, 0.f);
+                    if (k0 + u < d.nk && ip < d.total) {
+                        if (i >= 0) {
+                            if (i < n) v[u] = __ldg(x + i);
+                        } else if (d.H + i >= 0) {
+                            v[u] = d.hist[d.H + i];
+                        }
                     }
-                    Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = v;
                 }
-                q += dq;
-                mr += dm;
-                if (q >= D) {
-                    q -= D;
-                    ++mr;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = k0 + u, ip = gt + k * GNT;
+                    if (k < d.nk && ip < d.total) {
+                        // block samples are rotated here; history samples were stored rotated
+                        const float2 z = d.ibase + ip >= 0 ? cmulf(v[u], cmulf(a, wt[k])) : v[u];
+                        Z[(D - 1 - q) * Mp + mr + (mr >> 3)] = z;
+                    }
+                    q += dq;
+                    mr += dm;
+                    if (q >= D) {
+                        q -= D;
+                        ++mr;
+                    }
                 }
             }
         }

@@ -1,0 +1,64 @@
+"""Tensor-core extraction of channel groups (gemm_extract.cu): channels that
+share decimation, tap count and phase count are extracted as one TF32x3 GEMM
+on tcgen05; groups of several sizes (padded columns, a partial last tile) and
+the channels left on the dense kernel (too few to group, decimation not a
+multiple of 4) all give the oracle's extraction across ragged blocks, and the
+group kernel is the one that ran."""
+import numpy as np
+import pytest
+
+import gpudemod as G
+from gpudemod import synth
+from oracle import oracle as O
+from signals import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FS = 10_000_000
+BLOCK = 1 << 18
+LENGTHS = [BLOCK, BLOCK - 777, BLOCK - 3, BLOCK - 32]
+
+
+def _specs():
+    rng = np.random.default_rng(11)
+    out = []
+    # 12 channels of (256 taps, D 32): one group, N = 32
+    for _ in range(12):
+        out.append((256, 32, float(rng.uniform(-4.5e6, 4.5e6)), float(rng.uniform(80e3, 250e3))))
+    # 5 channels of (100 taps, D 20): one group of 5, N = 16 (6 padded columns)
+    for _ in range(5):
+        out.append((100, 20, float(rng.uniform(-4.5e6, 4.5e6)), float(rng.uniform(40e3, 150e3))))
+    # 3 channels of (64, 16): too few, dense kernel
+    for _ in range(3):
+        out.append((64, 16, float(rng.uniform(-4.5e6, 4.5e6)), 100e3))
+    # 4 channels of (250, 25): decimation not a multiple of 4, dense kernel
+    for _ in range(4):
+        out.append((250, 25, float(rng.uniform(-4.5e6, 4.5e6)), 120e3))
+    return out
+
+
+def test_groups_match_oracle(cuda):
+    scene, _ = synth.fm_band_scene(block=BLOCK, n_stations=8, seconds=0.3)
+    blocks = [scene.next_block().numpy()[:n] for n in LENGTHS]
+    specs = _specs()
+    r = G.ChannelRunner(FS, BLOCK, max_channels=len(specs), max_taps=1024)
+    try:
+        r.set_autotune_table([(T, D, G.FORM_DENSE, 0) for T, D in {(s[0], s[1]) for s in specs}])
+        r.set_profiling(True)
+        slots, oracles = [], []
+        for k, (T, D, off, bw) in enumerate(specs):
+            s = r.admit(k + 1, off, bw, FS // D, T, G.MODE_IQ, G.CH_EMIT_IQ)
+            assert r.channel_form(s)[0] == G.FORM_DENSE
+            slots.append(s)
+            oracles.append(O.OracleChannel(FS, off, bw, FS // D, T, O.MODE_NFM, rds=False))
+        for b, x in enumerate(blocks):
+            r.process_block(x)
+            names = [n for n, _ in r.stage_times()]
+            assert "extract_gemm" in names, names
+            for k, (s, oc) in enumerate(zip(slots, oracles)):
+                g, w = r.result(s), oc.process(x)
+                assert g["n_iq"] == w["iq"].size, (specs[k], b)
+                err = rel_l2(g["iq"], w["iq"])
+                assert err <= 1e-5, (specs[k], b, err)
+    finally:
+        r.close()
