@@ -131,8 +131,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr)
         : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Packed taps of every group, arm u (grid.x) of group blockIdx.y: the planes
 // of the arm's K range for all N rows, hi then lo, in the staging layout of
@@ -191,6 +192,7 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
     uint64_t *fullb = reinterpret_cast<uint64_t *>(gsm);  // [3]: taps stage filled
     uint64_t *freeb = fullb + 3;                          // [3]: taps stage consumed by the MMAs
     uint64_t *accb = fullb + 6;                           // every MMA of the tile done
+    uint64_t *rawb = fullb + 7;                           // raw block span landed
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gsm + 64);
     GemmOut *outc = reinterpret_cast<GemmOut *>(gsm + 128);
     const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -205,6 +207,7 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
             mbar_init(freeb + i, 1);
         }
         mbar_init(accb, 1);
+        mbar_init(rawb, 1);
         mbar_init_fence();
     }
     if (warp == 0) {
@@ -218,9 +221,24 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    // taps of the first arms: one bulk copy per stage
+    // The tile's raw block span comes in by one bulk copy into the last taps
+    // stage (filled with its arm only after the staging below) when it fits
+    // there and lies inside the block; the taps of the other first arms by
+    // one bulk copy per stage.
+    const int rows = kGemmM + L - 1;
+    const int i0 = -g.pc + (j0 - L + 1) * D;
+    const int total = rows * D;
+    const int a0 = i0 & ~1;
+    const int cnt = (i0 - a0 + total + 1) & ~1;
+    const bool raw = (long long)a0 + cnt <= (long long)n && cnt * 8 <= lo.b_stage;
+    const int nb0 = raw ? NS - 1 : NS;  // stages loaded before the staging
+    char *rawp = reinterpret_cast<char *>(gsm + lo.o_b + (NS - 1) * lo.b_stage);
     if (tid == 0) {
-        for (int u = 0; u < NS && u < L; ++u) {
+        if (raw) {
+            mbar_arrive_expect_tx(rawb, (unsigned)cnt * 8u);
+            bulk_to_smem(rawp, x + a0, (unsigned)cnt * 8u, rawb);
+        }
+        for (int u = 0; u < nb0 && u < L; ++u) {
             mbar_arrive_expect_tx(fullb + u, (unsigned)lo.b_stage);
             bulk_to_smem(gsm + lo.o_b + u * lo.b_stage, gblk + (size_t)u * lo.b_stage, (unsigned)lo.b_stage,
                          fullb + u);
@@ -238,12 +256,30 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
         outc[tid] = o;
     }
     // block rows j0-L+1 .. j0+127 of X2, split into TF32 hi and lo planes;
-    // eight loads in flight per thread
-    {
+    // from the raw span in shared memory, or (tiles past the block end)
+    // eight global loads in flight per thread
+    bool raw_ok = true;
+    if (raw) raw_ok = __syncthreads_and(mbar_wait_bounded(rawb, 0u));
+    if (raw && raw_ok) {
+        const float2 *src = reinterpret_cast<const float2 *>(rawp) + (i0 - a0);
+        int r = tid / D, pp = tid - (tid / D) * D;
+        const int dr = kGemmThreads / D, dp = kGemmThreads - dr * D;
+        for (int s0 = tid; s0 < total; s0 += kGemmThreads) {
+            const float2 v = src[s0];
+            const float2 h = make_float2(tf32_round(v.x), tf32_round(v.y));
+            const int off = (pp >> 1) * lo.a_plane + r * 16 + (pp & 1) * 8;
+            *reinterpret_cast<float2 *>(gsm + lo.o_a + off) = h;
+            *reinterpret_cast<float2 *>(gsm + lo.o_alo + off) =
+                make_float2(tf32_round(v.x - h.x), tf32_round(v.y - h.y));
+            pp += dp;
+            r += dr;
+            if (pp >= D) {
+                pp -= D;
+                ++r;
+            }
+        }
+    } else if (!raw) {
         constexpr int U = 8;
-        const int rows = kGemmM + L - 1;
-        const int i0 = -g.pc + (j0 - L + 1) * D;
-        const int total = rows * D;
         int r = tid / D, pp = tid - (tid / D) * D;
         const int dr = kGemmThreads / D, dp = kGemmThreads - dr * D;
         for (int s0 = tid; s0 < total; s0 += U * kGemmThreads) {
@@ -273,14 +309,27 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the staging is read by the tensor core
     __syncthreads();
+    if (!raw_ok && tid == 0) device_fault(fault, 5u);
+    // the raw span has been consumed: its stage takes its arm
+    if (tid == 0 && nb0 < NS && nb0 < L) {
+        mbar_arrive_expect_tx(fullb + nb0, (unsigned)lo.b_stage);
+        bulk_to_smem(gsm + lo.o_b + nb0 * lo.b_stage, gblk + (size_t)nb0 * lo.b_stage, (unsigned)lo.b_stage,
+                     fullb + nb0);
+    }
 
     if (tid == 0) {
         const uint32_t idesc = umma_idesc_tf32(N);
-        const uint32_t a_hi = smem_u32(gsm + lo.o_a), a_lo = smem_u32(gsm + lo.o_alo);
-        const uint32_t b0 = smem_u32(gsm + lo.o_b);
         const uint32_t bplane = (uint32_t)N * 16u;
-        bool ok = true;
-        for (int u = 0; u < L; ++u) {
+        // descriptors of offset 0; the start-address field (16-byte units,
+        // below 2^14 for any shared address) takes the offsets by addition
+        const uint64_t dah0 = umma_desc(smem_u32(gsm + lo.o_a), (uint32_t)lo.a_plane, 128u);
+        const uint64_t dal0 = umma_desc(smem_u32(gsm + lo.o_alo), (uint32_t)lo.a_plane, 128u);
+        const uint64_t db0 = umma_desc(smem_u32(gsm + lo.o_b), bplane, 128u);
+        const uint64_t a_step = (uint64_t)(2 * lo.a_plane) >> 4, b_step = (uint64_t)(2 * bplane) >> 4;
+        const uint64_t b_lo = (uint64_t)((uint32_t)lo.planes * bplane) >> 4;
+        const int nsteps = lo.planes / 2;
+        bool ok = raw_ok;  // no staging, no MMAs (the fault is recorded above)
+        for (int u = 0; ok && u < L; ++u) {
             const uint32_t dacc = tmem + (uint32_t)((u % NA) * N);
             uint32_t acc = u < NA ? 0u : 1u;  // the first arm of an accumulator overwrites it
             const int stg = u % NS;
@@ -289,19 +338,17 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
                 break;
             }
             tc_fence_after();
-            const uint32_t bh = b0 + (uint32_t)(stg * lo.b_stage), bl = bh + (uint32_t)lo.planes * bplane;
-            const uint32_t arow = (uint32_t)(L - 1 - u) * 16u;  // arm u reads the rows u earlier
-            for (int s = 0; s < lo.planes / 2; ++s) {
-                const uint32_t ao = (uint32_t)(2 * s) * (uint32_t)lo.a_plane + arow;
-                const uint32_t bo = (uint32_t)(2 * s) * bplane;
-                const uint64_t dah = umma_desc(a_hi + ao, (uint32_t)lo.a_plane, 128u);
-                const uint64_t dal = umma_desc(a_lo + ao, (uint32_t)lo.a_plane, 128u);
-                const uint64_t dbh = umma_desc(bh + bo, bplane, 128u);
-                const uint64_t dbl = umma_desc(bl + bo, bplane, 128u);
+            uint64_t dah = dah0 + (uint64_t)(L - 1 - u);  // arm u reads the rows u earlier (16 bytes a row)
+            uint64_t dal = dal0 + (uint64_t)(L - 1 - u);
+            uint64_t dbh = db0 + ((uint64_t)(stg * lo.b_stage) >> 4);
+            for (int s = 0; s < nsteps; ++s) {
                 umma_tf32(dacc, dah, dbh, idesc, acc);
                 acc = 1;
-                umma_tf32(dacc, dah, dbl, idesc, 1u);
+                umma_tf32(dacc, dah, dbh + b_lo, idesc, 1u);
                 umma_tf32(dacc, dal, dbh, idesc, 1u);
+                dah += a_step;
+                dal += a_step;
+                dbh += b_step;
             }
             umma_commit(freeb + stg);
             // refill the previous arm's stage once its MMAs are done (the
@@ -317,8 +364,8 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
                              (unsigned)lo.b_stage, fullb + ps);
             }
         }
-        if (!ok) device_fault(fault, 3u);
-        umma_commit(accb);  // after every MMA issued above
+        if (!ok && raw_ok) device_fault(fault, 3u);
+        umma_commit(accb);  // after every MMA issued above (at once when none was)
     }
 
     // epilogue: warp w reads TMEM lanes 32*(w%4).. (its 32 output rows) and
@@ -329,13 +376,21 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
     if (done) {
         const int qd = warp & 3;
         const int j = j0 + qd * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(qd * 32) << 16);
         for (int ch = warp >> 2; ch < N / 16; ch += 2) {
             float sum[16];
-            for (int a = 0; a < NA; ++a) {
-                uint32_t v[16];
-                tmem_ld16(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(a * N + ch * 16), v);
+            // two accumulators in flight per wait
+            for (int a = 0; a < NA; a += 2) {
+                uint32_t v0[16], v1[16];
+                tmem_ld16(lane_base + (uint32_t)(a * N + ch * 16), v0);
+                if (a + 1 < NA) tmem_ld16(lane_base + (uint32_t)((a + 1) * N + ch * 16), v1);
+                tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) sum[i] = a == 0 ? __uint_as_float(v[i]) : sum[i] + __uint_as_float(v[i]);
+                for (int i = 0; i < 16; ++i) {
+                    float t = __uint_as_float(v0[i]);
+                    if (a + 1 < NA) t += __uint_as_float(v1[i]);
+                    sum[i] = a == 0 ? t : sum[i] + t;
+                }
             }
             if (j < g.n_out) {
 #pragma unroll

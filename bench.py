@@ -181,6 +181,46 @@ def extraction_form(T, D):
     return "extract_dense" if L <= 16 and smem <= 200 * 1024 else "extract_group"
 
 
+def gemm_grouped(chans, n_in=BLOCK):
+    """Indices of the channels the runner extracts as tensor-core channel
+    groups (host plan_gemm_groups): dense-form channels whose decimation is a
+    multiple of 4, not float64-summed (FM modes at >= 4x their bandwidth),
+    with more than 256 outputs, in (taps, decimation) classes of at least 4
+    channels (all channels of a workload share the phase count here: they are
+    admitted together and every block length is a multiple of the
+    decimation).  Also returns the executed tensor flop per block: three TF32
+    passes of a 128 x N x 2*L*D real GEMM per 128-output tile."""
+    classes = {}
+    for i, c in enumerate(chans):
+        T, D = c["T"], c["D"]
+        fm = c["kind"] in ("NFM", "WFM")
+        precise = fm and c.get("bw") is not None and c["out_rate"] >= 4 * max(c["bw"], 400.0)
+        if extraction_form(T, D) != "extract_dense" or D % 4 or precise or n_in // D <= 256:
+            continue
+        classes.setdefault((T, D), []).append(i)
+    grouped, tensor_flop = set(), 0
+    for (T, D), idx in classes.items():
+        if len(idx) < 4:
+            continue
+        L = -(-T // D)
+        rp = ((128 + L - 1 + 7) // 8) * 8 + 1
+        smem = lambda n, ns: 128 + 128 * 24 + 2 * (D // 2) * rp * 16 + ns * 2 * (D // 2) * n * 16
+        cmax = max([c for c in range(8, 129, 8) if smem(2 * c, 2) <= 220 * 1024] or [0])
+        if cmax < 4:
+            continue
+        nchunk = -(-len(idx) // cmax)
+        per = -(-len(idx) // nchunk)
+        for c0 in range(0, len(idx), per):
+            members = idx[c0:c0 + per]
+            if len(members) < 4:
+                break
+            grouped.update(members)
+            ncol = -(-2 * len(members) // 16) * 16
+            tiles = -(-(n_in // D - 256) // 128)
+            tensor_flop += 3 * 2 * 128 * ncol * 2 * L * D * tiles
+    return grouped, tensor_flop
+
+
 def algorithmic_work(chans, n_in=BLOCK):
     """Per block, summed over channels (the definitions the reference workload
     implies): extraction 4*T*n_out + min(6*n_in, 4*T*n_out) flop (complex x
@@ -193,16 +233,27 @@ def algorithmic_work(chans, n_in=BLOCK):
     w["extract"]["bytes"] = 8 * n_in
     forms = {}  # the same extraction work split by the kernel that does it
     per_out = {"WFM": 6, "NFM": 6, "AM": 5, "USB": 3, "LSB": 3, "CW": 1}
-    for c in chans:
+    grouped, tensor_flop = gemm_grouped(chans, n_in)
+    for i, c in enumerate(chans):
         T, D = c["T"], c["D"]
         n_out = n_in // D
         f = 4 * T * n_out + min(6 * n_in, 4 * T * n_out)
         b = 8 * n_out + 4 * T + 16 * (T - 1)
         w["extract"]["flop"] += f
         w["extract"]["bytes"] += b
-        fw = forms.setdefault(extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
-        fw["flop"] += f
-        fw["bytes"] += b
+        if i in grouped:
+            # outputs 0..255 (the carried history) on the dense kernel, the rest in the group kernel
+            f0 = f * 256 / n_out
+            fw = forms.setdefault("extract_dense", {"flop": 0, "bytes": 8 * n_in})
+            fw["flop"] += f0
+            fw["bytes"] += 8 * 256
+            fw = forms.setdefault("extract_gemm", {"flop": 0, "bytes": 8 * n_in, "tensor_flop": tensor_flop})
+            fw["flop"] += f - f0
+            fw["bytes"] += b - 8 * 256
+        else:
+            fw = forms.setdefault(extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
+            fw["flop"] += f
+            fw["bytes"] += b
         w["demod"]["flop"] += per_out[c["kind"]] * n_out
         w["demod"]["bytes"] += 12 * n_out
         # 48 kHz back end: 33-tap arm per output frame and audio channel,
@@ -254,6 +305,33 @@ NCU_TRAFFIC = {("fm_band", "extract_dense"): 8.58e6,
                ("headroom", "extract_mod"): 52.6e6 * 2048 / 512}
 
 
+def kernel_roofline(name, ms, work, fp32, tf32, hbm_peak, peak_kind, wl):
+    """Roofline entry of one kernel from its per-launch device time: the
+    tensor-core group kernel against the measured TF32 tensor rate (executed
+    flop of its three TF32 passes; its float32-equivalent FIR rate beside it),
+    every other kernel against FP32 or HBM, whichever bounds its algorithmic
+    work."""
+    key = stage_key(name)
+    w = work.get(key, {"flop": 0, "bytes": 0})
+    ach_tf = w["flop"] / (ms * 1e-3) / 1e12
+    ach_gbs = w["bytes"] / (ms * 1e-3) / 1e9
+    if "tensor_flop" in w and tf32:
+        t = w["tensor_flop"] / (ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": t, "peak": tf32, "unit": "TFLOP/s", "frac": t / tf32,
+                "peak_source": "cuBLAS TF32 GEMM 8192^3, measured in this run",
+                "executed_tensor_flop": w["tensor_flop"], "fp32_equiv_tflops": ach_tf}
+    elif fp32 is not None and (w["flop"] / (fp32 * 1e12)) >= (w["bytes"] / (hbm_peak * 1e9)):
+        roof = {"bound": "fp32", "achieved": ach_tf, "peak": fp32, "unit": "TFLOP/s", "frac": ach_tf / fp32,
+                "peak_source": "cuBLAS SGEMM (TF32 off), measured in this run"}
+    else:
+        roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach_gbs / hbm_peak, "peak_source": f"{peak_kind} HBM copy"}
+    roof.update({"kernel": name, "ms_per_launch": ms, "traffic": NCU_TRAFFIC.get((wl, key)),
+                 "algorithmic_flop": w["flop"], "algorithmic_bytes": w["bytes"],
+                 "hbm_frac": ach_gbs / hbm_peak, "hbm_peak_gbs": hbm_peak})
+    return roof
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -263,10 +341,11 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def fp32_peak_tflops():
-    """cuBLAS SGEMM (TF32 off) 8192^3 as the measured FP32 FMA peak on this GPU."""
+def fp32_peak_tflops(tf32=False):
+    """cuBLAS SGEMM 8192^3 as the measured FP32 FMA peak on this GPU (TF32
+    off), or with TF32 tensor cores on as the measured TF32 tensor peak."""
     import torch
-    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = bool(tf32)
     a = torch.randn(8192, 8192, device="cuda")
     b = torch.randn(8192, 8192, device="cuda")
     for _ in range(2):
@@ -281,6 +360,7 @@ def fp32_peak_tflops():
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
     del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
@@ -472,27 +552,16 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     # ---- roofline of the dominant kernel --------------------------------
     hbm_peak, peak_kind = measured_peaks()
     fp32 = fp32_peak_tflops() if not args.profile_only else None
+    tf32 = fp32_peak_tflops(tf32=True) if not args.profile_only else None
     # per-launch device time of each kernel; the intervals that cover a wait
     # on the other block in flight and the copies are not kernels
     kern = {k: statistics.mean(v) for k, v in stage_acc.items()
             if k not in ("h2d", "d2h") and not k.startswith("wait")}
     waits = {k: round(statistics.mean(v), 4) for k, v in stage_acc.items() if k.startswith("wait")}
     dom = max(kern, key=kern.get)
-    dom_key = stage_key(dom)
-    w = work.get(dom_key, {"flop": 0, "bytes": 0})
-    dom_ms = kern[dom]
-    ach_tf = w["flop"] / (dom_ms * 1e-3) / 1e12
-    ach_gbs = w["bytes"] / (dom_ms * 1e-3) / 1e9
-    fp32_bound = fp32 is not None and (w["flop"] / (fp32 * 1e12)) >= (w["bytes"] / (hbm_peak * 1e9))
-    if fp32_bound:
-        roof = {"bound": "fp32", "achieved": ach_tf, "peak": fp32, "unit": "TFLOP/s", "frac": ach_tf / fp32,
-                "peak_source": "cuBLAS SGEMM (TF32 off), measured in this run"}
-    else:
-        roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": ach_gbs / hbm_peak, "peak_source": f"{peak_kind} HBM copy"}
-    roof.update({"kernel": dom, "ms_per_launch": dom_ms, "traffic": NCU_TRAFFIC.get((wl, dom_key)),
-                 "algorithmic_flop": w["flop"], "algorithmic_bytes": w["bytes"],
-                 "hbm_frac": ach_gbs / hbm_peak, "hbm_peak_gbs": hbm_peak})
+    roof = kernel_roofline(dom, kern[dom], work, fp32, tf32, hbm_peak, peak_kind, wl)
+    extraction = {k: kernel_roofline(k, v, work, fp32, tf32, hbm_peak, peak_kind, wl)
+                  for k, v in kern.items() if k.startswith("extract")}
     block_ms_sum = sum(kern.values())
     stages = {k: round(v, 4) for k, v in sorted(kern.items(), key=lambda kv: -kv[1])}
 
@@ -514,6 +583,7 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
         "latency_ms": {"p50": st_value["p50_block_ms"], "p99": st_value["p99_block_ms"],
                        "block_period_ms": BLOCK / FS * 1e3},
         "roofline": roof,
+        "extraction_rooflines": extraction,
         "stage_ms": stages,
         "wait_ms": waits,
         "block_gflop": total_flop / 1e9,
@@ -873,10 +943,11 @@ def run_headroom(args, world, rank, local):
     t_roof = max(flop / args.steps / (fp32 * 1e12), b_min / (hbm_peak * 1e9)) * 1e3
     dom = max(kern, key=kern.get)
     dk = stage_key(dom)
-    ach = work[dk]["flop"] / (kern[dom] * 1e-3) / 1e12
+    wdk = work.get(dk, {"flop": 0})
+    ach = wdk["flop"] / (kern[dom] * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
             "peak_source": "cuBLAS SGEMM (TF32 off), measured in this run", "kernel": dom,
-            "ms_per_launch": kern[dom], "algorithmic_flop": work[dk]["flop"],
+            "ms_per_launch": kern[dom], "algorithmic_flop": wdk["flop"],
             "traffic": NCU_TRAFFIC.get(("headroom", dk)) if n_live == 2048 else None,
             "block": {"gflop": flop / args.steps / 1e9, "min_bytes": b_min, "roofline_ms": t_roof,
                       "measured_ms": block_ms, "frac": t_roof / block_ms,
