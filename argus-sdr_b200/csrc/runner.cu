@@ -1183,7 +1183,10 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                                 : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
         const int ntiles = (int)pl.w_dense[L].size();
         const int ng = std::min(GPUD_DENSE_PIPE, dense_pipe_groups_host(pl.dense_pmax[L], L, kDensePipeSmemCap));
-        if (ng > 0 && r->d_fault && ((uintptr_t)x_dev & 15) == 0) {
+        // the persistent kernel pays off with at least two tiles per SM; a
+        // smaller class (e.g. the history tiles of grouped channels) runs one
+        // tile per CTA, whose smaller CTAs share SMs with the other blocks in flight
+        if (ng > 0 && ntiles >= 2 * r->num_sms && r->d_fault && ((uintptr_t)x_dev & 15) == 0) {
             // persistent: one CTA per SM over contiguous runs of tiles
             CK(launch_extract_dense_pipe(L, ng, ntiles, std::min(ntiles, r->num_sms), pl.dense_pmax[L], f.s,
                                          d_w + w_dense_off[L], d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist,
