@@ -342,6 +342,7 @@ struct gpud_runner {
     bool pll_parallel = true;
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
+    bool channel_groups = true;  // tensor-core channel groups (gpud_runner_set_channel_groups)
     // fault word the pipelined extraction kernel writes when a bounded wait
     // gives up (page-locked, mapped into the device)
     unsigned *h_fault = nullptr, *d_fault = nullptr;
@@ -807,7 +808,7 @@ static std::vector<char> plan_gemm_groups(gpud_runner *r, BlockPlan &pl) {
     pl.gemm_smem = pl.gemm_max_l = 0;
     pl.gemm_b_bytes = 0;
     std::vector<char> grouped(pl.sbs.size(), 0);
-    if (!GPUD_GEMM_EXTRACT || !r->d_fault) return grouped;
+    if (!GPUD_GEMM_EXTRACT || !r->channel_groups || !r->d_fault) return grouped;
     std::map<std::tuple<int, int, int>, std::vector<int>> by_key;
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
@@ -2391,6 +2392,13 @@ GPUD_API int GPUD_CALL gpud_runner_set_autotune_table(gpud_runner *r, const gpud
             return set_err(r, GPUD_E_ARG, "autotune entry: form not valid for its geometry");
     }
     r->tune.assign(entries, entries + count);
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_set_channel_groups(gpud_runner *r, int enable) {
+    if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    r->channel_groups = enable != 0;
     return 0;
 }
 

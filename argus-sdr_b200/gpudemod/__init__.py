@@ -186,6 +186,12 @@ class ChannelRunner:
         arr = (AutotuneEntry * max(1, len(entries)))(*[AutotuneEntry(*map(int, e)) for e in entries])
         _check(self._r, lib.gpud_runner_set_autotune_table(self._r, arr, len(entries)))
 
+    def set_channel_groups(self, enable: bool):
+        """Tensor-core channel groups on (default) or off
+        (gpud_runner_set_channel_groups); off keeps every channel's output
+        bit-identical alone and in any mix."""
+        _check(self._r, lib.gpud_runner_set_channel_groups(self._r, 1 if enable else 0))
+
     def channel_form(self, slot: int):
         """(form, phases per group, groups) of an admitted channel."""
         f, pg, ng = C.c_int(), C.c_int(), C.c_int()

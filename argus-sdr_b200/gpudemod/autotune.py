@@ -3,8 +3,8 @@ decimation D) it times every form the geometry admits -- dense tiles, phase
 groups at two group sizes, the modulated short-arm form, the warp-per-output
 form -- on a scratch runner filled with channels of that class, and keeps the
 fastest.  The result is a table for ChannelRunner.set_autotune_table; a
-channel's form then depends on its class alone, so outputs stay identical
-alone and in any mix under one table.
+channel's form then depends on its class alone, so (with channel groups off)
+outputs stay identical alone and in any mix under one table.
 
 Timing: the runner's per-stage CUDA events around the extraction launches of
 steady blocks (the first block of each trial is a warm-up)."""

@@ -294,11 +294,20 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r);
 /* Replaces the autotune table (count 0: none; the built-in rule then picks
  * every channel's form).  Entries whose form cannot run their geometry are
  * refused (GPUD_E_ARG).  Applies to channels admitted afterwards; a
- * channel's form depends on its class alone, so its output is the same alone
- * and in any mix under one table. */
+ * channel's form depends on its class alone, so (with channel groups off,
+ * below) its output is the same alone and in any mix under one table. */
 GPUD_API int GPUD_CALL gpud_runner_set_autotune_table(gpud_runner *r, const gpud_autotune_entry *entries, int count);
 /* The extraction form, phases per group and group count of an admitted channel. */
 GPUD_API int GPUD_CALL gpud_runner_channel_form(gpud_runner *r, int slot, int *form, int *group_phases, int *groups);
+/* Channel groups on the tensor cores (no reference counterpart; on by
+ * default).  Dense-form channels of one decimation (a multiple of 4), tap
+ * count and phase count, at least 4 of them, are extracted together as one
+ * TF32x3 GEMM per 128-output tile from output 256 on.  A grouped channel's
+ * IQ then depends on whether its class has company in the block (a different
+ * summation order, within the 1e-5 parity bar of the ungrouped result); with
+ * groups off (enable 0) every channel's output is bit-identical alone and in
+ * any mix.  Takes effect at the next block. */
+GPUD_API int GPUD_CALL gpud_runner_set_channel_groups(gpud_runner *r, int enable);
 GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out);
 GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot);
 /* Offset / bandwidth drift: the NCO increment follows the offset with the

@@ -62,3 +62,39 @@ def test_groups_match_oracle(cuda):
                 assert err <= 1e-5, (specs[k], b, err)
     finally:
         r.close()
+
+
+def test_groups_switch_and_mix_invariance(cuda):
+    """With channel groups off a channel's IQ is bit-identical alone and in a
+    mix that would form a group; with them on the grouped IQ stays within the
+    parity bar of the ungrouped one."""
+    scene, _ = synth.fm_band_scene(block=BLOCK, n_stations=8, seconds=0.3)
+    blocks = [scene.next_block().numpy()[:n] for n in LENGTHS[:3]]
+    rng = np.random.default_rng(3)
+    specs = [(k + 1, float(rng.uniform(-4.5e6, 4.5e6)), 200e3, FS // 32, 256, G.MODE_IQ, G.CH_EMIT_IQ)
+             for k in range(6)]
+
+    def run(channels, groups):
+        r = G.ChannelRunner(FS, BLOCK, max_channels=8, max_taps=1024)
+        try:
+            r.set_channel_groups(groups)
+            r.set_profiling(True)
+            slots = [r.admit(*s) for s in channels]
+            out, grouped = [], False
+            for x in blocks:
+                r.process_block(x)
+                grouped |= "extract_gemm" in [n for n, _ in r.stage_times()]
+                out.append(r.result(slots[0])["iq"].copy())
+            return out, grouped
+        finally:
+            r.close()
+
+    alone, g0 = run(specs[:1], True)
+    assert not g0
+    off, g1 = run(specs, False)
+    assert not g1
+    on, g2 = run(specs, True)
+    assert g2
+    for a, b, c in zip(alone, off, on):
+        assert np.array_equal(a, b)
+        assert rel_l2(c, a) <= 1e-5
