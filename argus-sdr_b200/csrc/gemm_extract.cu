@@ -351,17 +351,20 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
                 dbh += b_step;
             }
             umma_commit(freeb + stg);
-            // refill the previous arm's stage once its MMAs are done (the
-            // current arm's MMAs keep the tensor core busy meanwhile)
-            if (u >= 1 && u - 1 + NS < L) {
-                const int ps = (u - 1) % NS;
-                if (!mbar_wait_bounded(freeb + ps, (unsigned)((u - 1) / NS) & 1u)) {
+            // refill: with several stages, the previous arm's stage once its
+            // MMAs are done (the current arm's keep the tensor core busy
+            // meanwhile) takes arm u-1+NS; with one stage, this arm's stage
+            // takes arm u+1 once this arm's MMAs are done
+            const int t = NS > 1 ? u - 1 + NS : u + 1;  // arm to load
+            if (t - NS >= 0 && t < L) {
+                const int ps = t % NS;
+                if (!mbar_wait_bounded(freeb + ps, (unsigned)((t - NS) / NS) & 1u)) {
                     ok = false;
                     break;
                 }
                 mbar_arrive_expect_tx(fullb + ps, (unsigned)lo.b_stage);
-                bulk_to_smem(gsm + lo.o_b + ps * lo.b_stage, gblk + (size_t)(u - 1 + NS) * lo.b_stage,
-                             (unsigned)lo.b_stage, fullb + ps);
+                bulk_to_smem(gsm + lo.o_b + ps * lo.b_stage, gblk + (size_t)t * lo.b_stage, (unsigned)lo.b_stage,
+                             fullb + ps);
             }
         }
         if (!ok && raw_ok) device_fault(fault, 3u);

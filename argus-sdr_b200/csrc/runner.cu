@@ -116,6 +116,9 @@ constexpr int kMaxWfmClasses = 16;
 constexpr int kDenseMaxL = 16;
 constexpr int kDenseSmemLimit = 200 * 1024;
 constexpr int kDensePipeSmemCap = 220 * 1024;  // what the pipelined dense kernel opts in to
+#ifndef GPUD_GEMM_PAIR
+#define GPUD_GEMM_PAIR 1  // 0: three taps stages, one group CTA per SM
+#endif
 #ifndef GPUD_GEMM_EXTRACT
 #define GPUD_GEMM_EXTRACT 1  // 0: no tensor-core channel groups
 #endif
@@ -840,6 +843,11 @@ static std::vector<char> plan_gemm_groups(gpud_runner *r, BlockPlan &pl) {
             g.n_out = pl.sbs[(size_t)rows[(size_t)c0]].n_out;
             g.jt0 = kGemmFirstOutput;
             g.ns = gemm_smem_bytes_host(D, L, g.ncol, 3) <= kGemmSmemCap ? 3 : 2;
+#if GPUD_GEMM_PAIR
+            // one taps stage when two CTAs then fit on an SM: one CTA's MMAs
+            // overlap the other's staging and epilogue
+            if (2 * (gemm_smem_bytes_host(D, L, g.ncol, 1) + 1024) <= 228 * 1024) g.ns = 1;
+#endif
             // accumulators: as many arms apart as fit in the TMEM share of one
             // of the CTAs that the shared memory lets reside on an SM
             {
