@@ -280,6 +280,8 @@ struct PendingOp {
 struct Frame {
     cudaStream_t s = nullptr;
     cudaEvent_t ev_front = nullptr, ev_back = nullptr, ev_done = nullptr, ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t s2 = nullptr;  // side stream: dense classes beside the channel-group kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     char *d_desc = nullptr, *h_desc = nullptr;
     size_t desc_cap = 0;
     char *d_out = nullptr, *h_out = nullptr;
@@ -1186,10 +1188,21 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     const WfmTaps *wt = (const WfmTaps *)r->d_wtaps;
     int nl = 0;
     // ---- front half ----
+    // With channel groups the dense classes (the groups' history tiles among
+    // them) run on the frame's side stream beside the group kernel, whose
+    // CTAs leave SMs free; the frame stream joins it before the first reader
+    // of the extracted IQ.  Their stage times are then not recorded.
+    const bool side = !pl.w_gemm.empty() && f.s2;
+    cudaStream_t ds = side ? f.s2 : f.s;
+    if (side) {
+        CK(cudaEventRecord(f.ev_fork, f.s));
+        CK(cudaStreamWaitEvent(f.s2, f.ev_fork, 0));
+    }
     for (int L = 0; L <= kDenseMaxL; ++L) {
         if (pl.w_dense[L].empty()) continue;
-        prof_mark(r, f, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str()
-                                : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
+        if (!side)
+            prof_mark(r, f, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str()
+                                    : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
         const int ntiles = (int)pl.w_dense[L].size();
         const int ng = std::min(GPUD_DENSE_PIPE, dense_pipe_groups_host(pl.dense_pmax[L], L, kDensePipeSmemCap));
         // the persistent kernel pays off with at least two tiles per SM; a
@@ -1197,11 +1210,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         // tile per CTA, whose smaller CTAs share SMs with the other blocks in flight
         if (ng > 0 && ntiles >= 2 * r->num_sms && r->d_fault && ((uintptr_t)x_dev & 15) == 0) {
             // persistent: one CTA per SM over contiguous runs of tiles
-            CK(launch_extract_dense_pipe(L, ng, ntiles, std::min(ntiles, r->num_sms), pl.dense_pmax[L], f.s,
+            CK(launch_extract_dense_pipe(L, ng, ntiles, std::min(ntiles, r->num_sms), pl.dense_pmax[L], ds,
                                          d_w + w_dense_off[L], d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist,
                                          r->d_taps, d_ext, r->d_fault));
         } else {
-            CK(launch_extract_dense(L, ntiles, pl.dense_smem[L], f.s, d_w + w_dense_off[L], d_sb, r->d_prm,
+            CK(launch_extract_dense(L, ntiles, pl.dense_smem[L], ds, d_w + w_dense_off[L], d_sb, r->d_prm,
                                     r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
         }
         nl++;
@@ -1237,6 +1250,10 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         CK(launch_extract_wide((int)pl.w_wide.size(), pl.wide_smem, f.s, d_w + o_wide, d_sb, r->d_prm, r->d_st, x_dev,
                                n, r->d_hist, r->d_taps, d_ext));
         nl++;
+    }
+    if (side) {
+        CK(cudaEventRecord(f.ev_join, f.s2));
+        CK(cudaStreamWaitEvent(f.s, f.ev_join, 0));
     }
     if (!pl.w_dec.empty()) {
         prof_mark(r, f, "decim2");
@@ -1543,6 +1560,9 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     for (auto &f : r->fr) {
         CKC(cudaStreamCreateWithFlags(&f.s, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_front, cudaEventDisableTiming));
+        CKC(cudaStreamCreateWithFlags(&f.s2, cudaStreamNonBlocking));
+        CKC(cudaEventCreateWithFlags(&f.ev_fork, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&f.ev_join, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&f.ev_back, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&f.ev_done, cudaEventDisableTiming));
         CKC(cudaEventCreate(&f.ev0));
@@ -1590,9 +1610,13 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);
         if (f.h_in) cudaFreeHost(f.h_in);
-        for (auto e : {f.ev_front, f.ev_back, f.ev_done, f.ev0, f.ev1})
+        for (auto e : {f.ev_front, f.ev_back, f.ev_done, f.ev0, f.ev1, f.ev_fork, f.ev_join})
             if (e) cudaEventDestroy(e);
         for (auto e : f.prof_ev) cudaEventDestroy(e);
+        if (f.s2) {
+            cudaStreamSynchronize(f.s2);
+            cudaStreamDestroy(f.s2);
+        }
         if (f.s) cudaStreamDestroy(f.s);
     }
     if (r->h_fault) cudaFreeHost(r->h_fault);
