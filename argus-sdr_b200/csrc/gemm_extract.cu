@@ -25,9 +25,11 @@
 // both operands from shared memory and accumulates in TMEM; float32 accuracy
 // comes from three TF32 passes (x_hi*g_hi + x_hi*g_lo + x_lo*g_hi, x_hi and
 // x_lo the TF32 roundings of x and of x - x_hi).  The arms accumulate into
-// several TMEM accumulators (arm u into u % na), so no accumulator takes more
-// than ceil(L/na) arms of sequential tensor-core additions -- the arms' partial
-// sums are far larger than a narrow channel's output -- and the epilogue adds
+// several TMEM accumulators (the x_hi*g_hi pass of arm u into u % (na-1), the
+// small correction passes into the last), so no large accumulator takes more
+// than ceil(L/(na-1)) arms of sequential tensor-core roundings -- the arms'
+// partial sums are far larger than a narrow channel's output -- and the
+// epilogue adds
 // the accumulators in float32 after reading them with tcgen05.ld, applies
 // each channel's output rotation exp(j phi_c(n_j)) from the exact Q0.64 phase
 // and stores the extracted IQ.
@@ -329,9 +331,15 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
         const uint64_t b_lo = (uint64_t)((uint32_t)lo.planes * bplane) >> 4;
         const int nsteps = lo.planes / 2;
         bool ok = raw_ok;  // no staging, no MMAs (the fault is recorded above)
+        // the x_hi*g_hi pass of arm u into accumulator u % NH; both correction
+        // passes (2^-11 of it) into the last one, so no large accumulator is
+        // rounded for the small terms
+        const int NH = NA > 1 ? NA - 1 : 1;
+        const uint32_t dcor = tmem + (uint32_t)((NA - 1) * N);
+        uint32_t acc_cor = NA > 1 ? 0u : 1u;
         for (int u = 0; ok && u < L; ++u) {
-            const uint32_t dacc = tmem + (uint32_t)((u % NA) * N);
-            uint32_t acc = u < NA ? 0u : 1u;  // the first arm of an accumulator overwrites it
+            const uint32_t dacc = tmem + (uint32_t)((u % NH) * N);
+            uint32_t acc = u < NH ? 0u : 1u;  // the first arm of an accumulator overwrites it
             const int stg = u % NS;
             if (!mbar_wait_bounded(fullb + stg, (unsigned)(u / NS) & 1u)) {
                 ok = false;
@@ -341,14 +349,18 @@ k_extract_gemm(const int2 *__restrict__ work, const GemmGroup *__restrict__ grou
             uint64_t dah = dah0 + (uint64_t)(L - 1 - u);  // arm u reads the rows u earlier (16 bytes a row)
             uint64_t dal = dal0 + (uint64_t)(L - 1 - u);
             uint64_t dbh = db0 + ((uint64_t)(stg * lo.b_stage) >> 4);
+            // the arm's x_hi*g_hi MMAs, then its correction MMAs: consecutive
+            // MMAs stay on one accumulator (switching between them costs
+            // tensor-core throughput)
             for (int s = 0; s < nsteps; ++s) {
-                umma_tf32(dacc, dah, dbh, idesc, acc);
+                umma_tf32(dacc, dah + (uint64_t)s * a_step, dbh + (uint64_t)s * b_step, idesc, acc);
                 acc = 1;
-                umma_tf32(dacc, dah, dbh + b_lo, idesc, 1u);
-                umma_tf32(dacc, dal, dbh, idesc, 1u);
-                dah += a_step;
-                dal += a_step;
-                dbh += b_step;
+            }
+            const uint32_t dc = NA > 1 ? dcor : dacc;
+            for (int s = 0; s < nsteps; ++s) {
+                umma_tf32(dc, dah + (uint64_t)s * a_step, dbh + (uint64_t)s * b_step + b_lo, idesc, acc_cor);
+                acc_cor = 1;
+                umma_tf32(dc, dal + (uint64_t)s * a_step, dbh + (uint64_t)s * b_step, idesc, 1u);
             }
             umma_commit(freeb + stg);
             // refill: with several stages, the previous arm's stage once its

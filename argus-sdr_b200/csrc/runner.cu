@@ -215,6 +215,7 @@ static int build_binade_table(double inc, BinadeTable *t) {
 // ---------------------------------------------------------------------------
 struct Slot {
     bool active = false;
+    uint64_t pver = 0;  // version of the taps and NCO increment (the channel-group taps cache key)
     uint64_t reusable_after = 0;  // a retired slot is reused once this ticket completed
     gpud_channel_spec spec{};
     int D = 1, T = 1, P = 1, L = 1, hcap = 0;
@@ -298,6 +299,7 @@ struct Frame {
     int64_t part_cap = 0;
     float *d_gb = nullptr;      // packed taps of the tensor-core channel groups
     size_t gb_cap = 0;
+    std::vector<uint64_t> gb_key;  // the groups and member versions d_gb was packed for
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
@@ -360,6 +362,7 @@ struct gpud_runner {
     std::vector<PendingOp> pending;
     // stats
     uint64_t blocks = 0, launches = 0;
+    uint64_t pver_seq = 0;  // source of Slot::pver
     int graph_rebuilds = 0;
     std::vector<float> lat_ms;
     size_t lat_pos = 0;
@@ -1059,6 +1062,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         size_t cap = pl.gemm_b_bytes * 5 / 4 + 4096;
         CK(cudaMalloc((void **)&f.d_gb, cap));
         f.gb_cap = cap;
+        f.gb_key.clear();  // a new buffer holds no packed taps
     }
     if (dneed > f.desc_cap) {
         cudaFree(f.d_desc);
@@ -1220,13 +1224,31 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         nl++;
     }
     if (!pl.w_gemm.empty()) {
-        prof_mark(r, f, "gemm_pack");
-        CK(launch_gemm_pack((int)pl.groups.size(), pl.gemm_max_l, f.s, d_groups, d_gmem, d_sb, r->d_prm, r->d_taps,
-                            f.d_gb));
+        // the packed taps depend on the group layout and on each member's taps
+        // and NCO increment: repack only when one of them changed since this
+        // frame's buffer was packed
+        std::vector<uint64_t> key;
+        key.reserve(pl.groups.size() * 4 + pl.gmembers.size());
+        for (const GemmGroup &g : pl.groups) {
+            key.push_back(((uint64_t)(uint32_t)g.nmem << 32) | (uint32_t)g.ncol);
+            key.push_back(((uint64_t)(uint32_t)g.D << 32) | (uint32_t)g.T);
+            key.push_back((uint64_t)(uint32_t)g.b_off);
+        }
+        for (int row : pl.gmembers) {
+            const int slot = pl.sbs[(size_t)row].slot;
+            key.push_back(((uint64_t)(uint32_t)slot << 40) ^ r->slots[(size_t)slot].pver);
+        }
+        if (key != f.gb_key) {
+            prof_mark(r, f, "gemm_pack");
+            CK(launch_gemm_pack((int)pl.groups.size(), pl.gemm_max_l, f.s, d_groups, d_gmem, d_sb, r->d_prm,
+                                r->d_taps, f.d_gb));
+            f.gb_key = std::move(key);
+            nl++;
+        }
         prof_mark(r, f, "extract_gemm");
         CK(launch_extract_gemm((int)pl.w_gemm.size(), pl.gemm_smem, f.s, d_w + o_gemm, d_groups, d_gmem, d_sb,
                                r->d_prm, r->d_st, x_dev, n, f.d_gb, d_ext, r->d_fault));
-        nl += 2;
+        nl++;
     }
     if (!pl.w_group.empty()) {
         prof_mark(r, f, "extract_group");
@@ -1809,6 +1831,7 @@ static int admit_core(gpud_runner *r, const gpud_channel_spec *spec, int D, int 
     s.rs_class = rsclass;
     s.aud_ch = spec->mode == GPUD_MODE_WFM_STEREO ? 2 : 1;
     s.deemph_us = deemph_us;
+    s.pver = ++r->pver_seq;
     s.d1 = d1;
     s.d1_phase = 0;
     if (rsclass >= 0) {
@@ -1882,6 +1905,7 @@ GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offse
     double cutoff = bandwidth / 2;
     if (cutoff < 200) cutoff = 200;
     if (cutoff != s.cutoff) {
+        s.pver = ++r->pver_seq;
         std::vector<float> pm, h;
         design_taps(r, s, bandwidth, pm, h, &s.cutoff);
         queue_write(r, slot, r->d_taps + s.taps_off, pm.data(), pm.size() * 4);
@@ -1890,6 +1914,7 @@ GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offse
     bool was_precise = precise_sum(s.spec);
     s.spec.bandwidth = bandwidth;
     if (offset_hz != s.spec.offset_hz || precise_sum(s.spec) != was_precise) {
+        s.pver = ++r->pver_seq;
         s.spec.offset_hz = offset_hz;
         ChanParams p;
         fill_params(r, slot, &p);
@@ -2149,6 +2174,7 @@ GPUD_API int GPUD_CALL gpud_runner_restore(gpud_runner *r, int slot, const void 
     s.rds_count = h.rds_count;
     s.rs_t = h.rs_t;
     if (h.cutoff != s.cutoff) {
+        s.pver = ++r->pver_seq;
         std::vector<float> pm, hh;
         design_taps(r, s, 2 * h.cutoff, pm, hh, &s.cutoff);
         CK(cudaMemcpy(r->d_taps + s.taps_off, pm.data(), pm.size() * 4, cudaMemcpyHostToDevice));

@@ -98,3 +98,40 @@ def test_groups_switch_and_mix_invariance(cuda):
     for a, b, c in zip(alone, off, on):
         assert np.array_equal(a, b)
         assert rel_l2(c, a) <= 1e-5
+
+
+
+def test_group_taps_follow_retune(cuda):
+    """The packed group taps are cached per frame (three frames): retunes of
+    members between blocks -- offset only, bandwidth only (new taps), both --
+    reach the group kernel on the next block in every frame; the grouped
+    runner stays within the parity bar of one with groups off that gets the
+    same calls."""
+    scene, _ = synth.fm_band_scene(block=BLOCK, n_stations=8, seconds=0.8)
+    blocks = [scene.next_block().numpy() for _ in range(9)]
+    rng = np.random.default_rng(9)
+    offs = [float(rng.uniform(-4.5e6, 4.5e6)) for _ in range(6)]
+    calls = {2: [(1, offs[1] + 777.0, 200e3)], 4: [(2, offs[2], 120e3)], 5: [(3, offs[3] - 2500.0, 90e3)]}
+
+    def run(groups):
+        r = G.ChannelRunner(FS, BLOCK, max_channels=8, max_taps=1024)
+        try:
+            r.set_channel_groups(groups)
+            r.set_profiling(True)
+            slots = [r.admit(k + 1, off, 200e3, FS // 32, 256, G.MODE_IQ, G.CH_EMIT_IQ)
+                     for k, off in enumerate(offs)]
+            out = []
+            for b, x in enumerate(blocks):
+                for k, off, bw in calls.get(b, []):
+                    r.update(slots[k], off, bw)
+                r.process_block(x)
+                assert ("extract_gemm" in [n for n, _ in r.stage_times()]) == groups
+                out.append([r.result(s)["iq"].copy() for s in slots])
+            return out
+        finally:
+            r.close()
+
+    on, off = run(True), run(False)
+    for b, (a, c) in enumerate(zip(on, off)):
+        for k, (x, y) in enumerate(zip(a, c)):
+            assert rel_l2(x, y) <= 1e-5, (b, k, rel_l2(x, y))
