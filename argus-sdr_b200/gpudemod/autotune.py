@@ -7,7 +7,11 @@ channel's form then depends on its class alone, so (with channel groups off)
 outputs stay identical alone and in any mix under one table.
 
 Timing: the runner's per-stage CUDA events around the extraction launches of
-steady blocks (the first block of each trial is a warm-up)."""
+steady blocks (the first block of each trial is a warm-up).  Trials run with
+the runner's default channel groups, so the dense candidate of a class
+measures the tensor-core group kernel that a deployment with four or more
+channels of the class would run (and the dense kernel for the first 256
+outputs, on the side stream, inside the group's interval)."""
 from __future__ import annotations
 
 import statistics
@@ -16,7 +20,10 @@ import numpy as np
 
 from . import FORM_DENSE, FORM_GROUP, FORM_MOD, FORM_WIDE, GPUDError, MODE_IQ, ChannelRunner
 
-_EXTRACT_STAGES = ("extract", "group_sum")
+# every extraction stage, the channel-group taps packing included (a repack
+# runs only when the group or a member's taps change, so a steady trial
+# mostly sees the group kernel itself)
+_EXTRACT_STAGES = ("extract", "group_sum", "gemm_pack")
 
 
 def _candidates(T: int, D: int):

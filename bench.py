@@ -332,6 +332,24 @@ def kernel_roofline(name, ms, work, fp32, tf32, hbm_peak, peak_kind, wl):
     return roof
 
 
+def h2d_rate(block, stream):
+    """Host-to-device copy rate (GB/s) of one pinned input block, timed
+    alone on the runner's stream: the bound of any e2e number whose every
+    block crosses the host link."""
+    import torch
+    dst = torch.empty_like(block, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            dst.copy_(block, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            dst.copy_(block, non_blocking=True)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return 10 * block.numel() * block.element_size() / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -532,6 +550,7 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     st = runner.stats()
     e2e = world * n_ch * BLOCK * args.steps / e2e_s / 1e6
     h2d, d2h = st["last_h2d_bytes"], st["last_d2h_bytes"]
+    h2d_gbs = h2d_rate(pinned[0], stream)
     if rank != 0:
         return None
 
@@ -577,6 +596,8 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 NCO/PLL state)",
         "data": "synthetic (seeded scene, stands in for live captures)",
         "e2e": {"value": e2e, "unit": "channel-MS/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "h2d_gbs": h2d_gbs,
+                "h2d_bound": world * n_ch * BLOCK / (h2d / (h2d_gbs * 1e9)) / 1e6,
                 "p50_block_ms": st["p50_block_ms"], "p99_block_ms": st["p99_block_ms"]},
         "plain_runner": {"value": plain_v, "unit": "channel-MS/s",
                          "speedup_batched_vs_plain": (value / plain_v) if plain_v else None},
