@@ -1274,6 +1274,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         nl++;
     }
     if (side) {
+        prof_mark(r, f, "wait_side");  // ends the group kernel's interval; the join wait is its own
         CK(cudaEventRecord(f.ev_join, f.s2));
         CK(cudaStreamWaitEvent(f.s, f.ev_join, 0));
     }
