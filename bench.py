@@ -14,7 +14,13 @@ launch sequence per block.  A step is one block through every channel.
   plain      the per-signal plain runner (one channel at a time, H2D/D2H per
              channel) on the same GPU and workload
   roofline   the dominant kernel, measured live from CUDA events between the
-             runner's launches over the timed region
+             runner's launches over the timed region (three blocks in flight,
+             so an interval includes the other blocks' kernels sharing SMs);
+             extraction_rooflines: every extraction kernel the same way;
+             rooflines_one_block_in_flight: the same from a short pass with one
+             block in flight after the timed passes
+  e2e.h2d_gbs  the pinned copy of one input block timed alone; h2d_bound the
+             e2e value that copy rate alone would allow
   cpu_baseline  the oracle (C restatement of the reference's Go CPU path) on a
              bounded sample, all host threads
 
@@ -554,6 +560,20 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     if rank != 0:
         return None
 
+    # ---- kernel times with one block in flight: no other block's kernels
+    # share the SMs (the pipelined intervals above include that contention)
+    iso_acc = {}
+    if not args.profile_only:
+        runner.set_host_outputs(False)
+        runner.set_profiling(True)
+        nxt = first + args.warmup + args.steps  # the stream continues after the e2e pass
+        for b in range(4):
+            runner.process_block(blocks[(nxt + b) % n_scene])
+            if b:
+                for name, ms in runner.stage_times():
+                    iso_acc.setdefault(name, []).append(ms)
+        runner.set_profiling(False)
+
     # ---- plain per-signal runner on the same GPU -------------------------
     plain_v = None
     if not args.profile_only and args.plain_steps > 0:
@@ -581,6 +601,14 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     roof = kernel_roofline(dom, kern[dom], work, fp32, tf32, hbm_peak, peak_kind, wl)
     extraction = {k: kernel_roofline(k, v, work, fp32, tf32, hbm_peak, peak_kind, wl)
                   for k, v in kern.items() if k.startswith("extract")}
+    iso = None
+    if iso_acc:
+        ik = {k: statistics.mean(v) for k, v in iso_acc.items() if k not in ("h2d", "d2h") and not k.startswith("wait")}
+        idom = max(ik, key=ik.get)
+        iso = {"dominant": kernel_roofline(idom, ik[idom], work, fp32, tf32, hbm_peak, peak_kind, wl),
+               "extraction": {k: kernel_roofline(k, v, work, fp32, tf32, hbm_peak, peak_kind, wl)
+                              for k, v in ik.items() if k.startswith("extract")},
+               "stage_ms": {k: round(v, 4) for k, v in sorted(ik.items(), key=lambda kv: -kv[1])}}
     block_ms_sum = sum(kern.values())
     stages = {k: round(v, 4) for k, v in sorted(kern.items(), key=lambda kv: -kv[1])}
 
@@ -605,6 +633,7 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
                        "block_period_ms": BLOCK / FS * 1e3},
         "roofline": roof,
         "extraction_rooflines": extraction,
+        "rooflines_one_block_in_flight": iso,
         "stage_ms": stages,
         "wait_ms": waits,
         "block_gflop": total_flop / 1e9,
