@@ -132,7 +132,10 @@ constexpr int kGroupSmemTarget = 100 * 1024;  // two CTAs per SM
 constexpr int kModSmemTarget = 72 * 1024;     // three CTAs per SM
 constexpr int kModMaxL = 4;
 constexpr int kPllMaxIters = 64;
-constexpr int kFrames = 3;  // blocks in flight
+#ifndef GPUD_FRAMES
+#define GPUD_FRAMES 3
+#endif
+constexpr int kFrames = GPUD_FRAMES;  // blocks in flight
 constexpr int kMaxRsClasses = 16;  // 48 kHz resampler banks (one per demod rate)
 
 // ---------------------------------------------------------------------------

@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--depth", type=int, default=3, help="blocks in flight (the runner holds three frames)")
     ap.add_argument("--cpu-blocks", type=int, default=2, help="cpu_baseline sample: blocks of 2^20 per channel")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu (no baselines)")
@@ -507,7 +508,7 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     runner.set_host_outputs(False)
     runner.set_profiling(True)
     clk = ClockSampler(local).__enter__()  # sampling starts before warmup (first sample ~0.2 s)
-    pipelined(runner, [blocks[s % n_scene] for s in range(args.warmup)])
+    pipelined(runner, [blocks[s % n_scene] for s in range(args.warmup)], args.depth)
     runner.reset_stats()
     l0 = G.kernel_launch_count()
     stage_acc = {}
@@ -517,9 +518,9 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     e0.record(stream)  # the runner's join stream: events there follow every submitted block
     tickets = []
     for s in range(args.steps):
-        tickets.append(runner.submit(blocks[(args.warmup + s) % n_scene]))  # three blocks in flight
-        if len(tickets) >= 3:
-            runner.wait(tickets[-3])
+        tickets.append(runner.submit(blocks[(args.warmup + s) % n_scene]))  # args.depth blocks in flight
+        if len(tickets) >= args.depth:
+            runner.wait(tickets[-args.depth])
             for name, ms in runner.stage_times():
                 stage_acc.setdefault(name, []).append(ms)
     runner.wait(tickets[-1])
@@ -542,12 +543,12 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     # ---- e2e: public C ABI from pinned host memory ---------------------------
     runner.set_profiling(False)
     runner.set_host_outputs(True)
-    pipelined(runner, pinned[:args.warmup])
+    pipelined(runner, pinned[:args.warmup], args.depth)
     runner.reset_stats()
     barrier(world)
     torch.cuda.synchronize()
     e0.record(stream)
-    pipelined(runner, pinned[args.warmup:])
+    pipelined(runner, pinned[args.warmup:], args.depth)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(world, e0.elapsed_time(e1)) * 1e-3

@@ -135,3 +135,34 @@ def test_group_taps_follow_retune(cuda):
     for b, (a, c) in enumerate(zip(on, off)):
         for k, (x, y) in enumerate(zip(a, c)):
             assert rel_l2(x, y) <= 1e-5, (b, k, rel_l2(x, y))
+
+
+def test_fm_band_group_matches_oracle(cuda):
+    """The FM band geometry: 40 WFM stereo stations of 256 taps at decimation
+    32 from 10 MS/s in 2^20-sample blocks form one 80-column group whose tiles
+    stage their block span by bulk copy; every channel's IQ and, for four of
+    them, the stereo audio and RDS baseband match the oracle."""
+    block = 1 << 20
+    scene, st = synth.fm_band_scene(block=block, n_stations=40, seconds=0.3)
+    r = G.ChannelRunner(FS, block, max_channels=40, max_taps=1024)
+    try:
+        r.set_profiling(True)
+        slots = [r.admit(k + 1, s.offset_hz, 250_000.0, 312_500, 256, G.MODE_WFM_STEREO, G.CH_RDS | G.CH_EMIT_IQ)
+                 for k, s in enumerate(st)]
+        iq_or = [O.OracleChannel(FS, s.offset_hz, 250_000.0, 312_500, 256, O.MODE_NFM, rds=False) for s in st]
+        full = {k: O.OracleChannel(FS, st[k].offset_hz, 250_000.0, 312_500, 256, O.MODE_WFM_STEREO, rds=True)
+                for k in (0, 13, 26, 39)}
+        for b in range(2):
+            x = scene.next_block().numpy()
+            r.process_block(x)
+            assert "extract_gemm" in [n for n, _ in r.stage_times()]
+            for k, (s, oc) in enumerate(zip(slots, iq_or)):
+                g, w = r.result(s), oc.process(x)
+                assert g["n_iq"] == w["iq"].size
+                assert rel_l2(g["iq"], w["iq"]) <= 1e-5, (k, b, rel_l2(g["iq"], w["iq"]))
+                if k in full:
+                    wf = full[k].process(x)
+                    assert rel_l2(g["audio"], wf["audio"]) <= 1e-5, (k, b, rel_l2(g["audio"], wf["audio"]))
+                    assert rel_l2(g["rds"], wf["rds"]) <= 1e-5, (k, b, rel_l2(g["rds"], wf["rds"]))
+    finally:
+        r.close()
