@@ -29,17 +29,19 @@
 // small correction passes into the last), so no large accumulator takes more
 // than ceil(L/(na-1)) arms of sequential tensor-core roundings -- the arms'
 // partial sums are far larger than a narrow channel's output -- and the
-// epilogue adds
-// the accumulators in float32 after reading them with tcgen05.ld, applies
-// each channel's output rotation exp(j phi_c(n_j)) from the exact Q0.64 phase
-// and stores the extracted IQ.
+// epilogue adds the accumulators in float32 after reading them with
+// tcgen05.ld, applies each channel's output rotation exp(j phi_c(n_j)) from
+// the exact Q0.64 phase and stores the extracted IQ.  The taps of each arm
+// arrive by one bulk copy into a stage freed by tcgen05.commit: one stage per
+// CTA when two CTAs then fit on an SM (one CTA's MMAs overlap the other's
+// staging and epilogue), else a ring of two or three.
 //
 // The first 256 outputs of each channel (which reach into the carried
 // history) stay on the dense polyphase kernel; the group kernel covers
-// outputs 256.. in 128-output tiles.  Taps are packed per block on the device
+// outputs 256.. in 128-output tiles.  Taps are packed on the device
 // (k_gemm_pack) from the channel's float32 direct-form taps and its NCO
-// increment, so every update path of the runner (admission, retune, snapshot
-// restore) reaches the group kernel without extra bookkeeping.
+// increment whenever a group's layout or a member's taps or increment
+// changed (the host keys each frame's packed buffer on them).
 #include "gpud_internal.cuh"
 
 namespace gpud {
