@@ -272,7 +272,9 @@ typedef struct {
     double p50_block_ms;    /* over the last 4096 blocks */
     double p99_block_ms;
     uint64_t kernel_launches; /* kernels launched by the runner since creation */
-    int32_t graph_rebuilds;
+    int32_t graph_rebuilds;   /* regrowths of the per-block work arrays and output arena (the
+                                 launch sequence is not graph-captured; a captured one would be
+                                 rebuilt on exactly these) */
     int32_t pad;
     uint64_t last_h2d_bytes;  /* host->device bytes of the last block */
     uint64_t last_d2h_bytes;  /* device->host bytes of the last block */
