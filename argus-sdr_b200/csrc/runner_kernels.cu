@@ -2302,11 +2302,38 @@ k_audio48_rs(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, c
     double *s_bank = s_aud;
     float *s_in = reinterpret_cast<float *>(s_aud + kAudBank);
     if (staged) {
-        for (int i = threadIdx.x; i < L * K; i += kAudThreads) s_bank[i] = bk.arm[i];
-        for (int i = threadIdx.x; i < win; i += kAudThreads) {
-            const int64_t g = lo + i;
-            for (int c = 0; c < C; ++c)
-                s_in[c * kAudWin + i] = g >= 0 ? in[g * C + c] : as.dl[c][-1 - g];
+        // eight loads in flight per thread: the staging, not the 33-tap dot
+        // products, sets this kernel's time
+        constexpr int U = 8;
+        const int nb = L * K;
+        for (int i0 = threadIdx.x; i0 < nb; i0 += U * kAudThreads) {
+            double v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * kAudThreads;
+                v[u] = i < nb ? bk.arm[i] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * kAudThreads;
+                if (i < nb) s_bank[i] = v[u];
+            }
+        }
+        for (int c = 0; c < C; ++c) {
+            for (int i0 = threadIdx.x; i0 < win; i0 += U * kAudThreads) {
+                float v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * kAudThreads;
+                    const int64_t g = lo + i;
+                    v[u] = i < win ? (g >= 0 ? in[g * C + c] : as.dl[c][-1 - g]) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * kAudThreads;
+                    if (i < win) s_in[c * kAudWin + i] = v[u];
+                }
+            }
         }
         __syncthreads();
     }
