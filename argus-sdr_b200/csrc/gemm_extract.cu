@@ -439,11 +439,9 @@ cudaError_t launch_gemm_pack(int ngroups, int max_l, cudaStream_t sm, const Gemm
 cudaError_t launch_extract_gemm(int grid, int smem, cudaStream_t sm, const int2 *work, const GemmGroup *groups,
                                 const int *members, const SlotBlock *sbt, const ChanParams *prm, const ChanState *st,
                                 const float2 *x, int n, const float *gb, float2 *ext, unsigned *fault) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_extract_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_gemm, 220 * 1024);
+    if (e != cudaSuccess) return e;
     k_extract_gemm<<<grid, kGemmThreads, smem, sm>>>(work, groups, members, sbt, prm, st, x, n, gb, ext, fault);
     return cudaGetLastError();
 }

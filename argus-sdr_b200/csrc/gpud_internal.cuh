@@ -11,6 +11,7 @@
 //   per-block buffers    extracted IQ, composite, pilot/bpf/lpr/lr work arrays
 //   output arena         results table | audio | RDS | emitted IQ (one D2H)
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -19,6 +20,22 @@
 #endif
 
 namespace gpud {
+
+// Opt kernel `fn` in to `bytes` of dynamic shared memory on the current
+// device.  cudaFuncSetAttribute acts on the current device only, so the
+// opt-in is made once per device: bit d of `done` (one mask per kernel, owned
+// by its launch helper) records device d.  Threads racing on the first launch
+// may both set the attribute, which is harmless.  Returns the API's error.
+inline cudaError_t smem_optin_once(std::atomic<uint64_t> &done, const void *fn, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // ---------------------------------------------------------------------------
 // NCO phase as an unsigned Q0.64 fraction of a turn.  Sample i of a block has

@@ -424,7 +424,10 @@ static __device__ __align__(256) float2 g_noalloc_scratch[GPUD_NOALLOC_MAX_NEW +
 // array's name is only a host-side stand-in, never a device address: it is
 // resolved with cudaGetSymbolAddress once per device, with that device
 // current, on the first call made on that device (make that first call before
-// any stream capture).
+// any stream capture).  The resolved address is kept for the life of the
+// process: cudaDeviceReset tears down the context that holds the array, and
+// the address kept for that device is then stale, so a process that resets a
+// device must not call the allocation-free entry point on it afterwards.
 static float2 *noalloc_scratch(cudaError_t *err) {
     static std::atomic<float2 *> cache[64];
     int dev = 0;
@@ -448,6 +451,12 @@ extern "C" GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_noall
     const gpud_float2 *in_new, int n_new, const float *polyphase_taps, int polyphase_len, int decim, int num_taps,
     gpud_float2 *history_state, int history_cap, int *history_len_io, int *phase_count_state, double *phase_state,
     double phase_inc, gpud_float2 *out, int out_cap, int *n_out) {
+    // the base entry point's argument codes come first (-10 null state
+    // pointers, -11 negative sizes), then the scratch limits
+    if (!polyphase_taps || decim <= 0 || num_taps <= 0 || !history_len_io || !phase_count_state || !phase_state ||
+        !n_out)
+        return -10;
+    if (n_new < 0 || out_cap < 0 || history_cap < 0) return -11;
     if (n_new > GPUD_NOALLOC_MAX_NEW || history_cap > GPUD_NOALLOC_MAX_HISTORY) return GPUD_E_SCRATCH;
     cudaError_t err = cudaSuccess;
     float2 *scratch = noalloc_scratch(&err);

@@ -2467,11 +2467,9 @@ template <int L>
 static cudaError_t launch_dense_L(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                   const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                   const float2 *hist, const float *taps, float2 *ext) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_extract_dense<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_dense<L>, 220 * 1024);
+    if (e != cudaSuccess) return e;
     k_extract_dense<L><<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
     return cudaGetLastError();
 }
@@ -2495,11 +2493,9 @@ static cudaError_t launch_dense_pipe_LG(int ntiles, int grid, int pmax, cudaStre
                                         const SlotBlock *sbt, const ChanParams *prm, const ChanState *st,
                                         const float2 *x, int n, const float2 *hist, const float *taps, float2 *ext,
                                         unsigned *fault) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_extract_dense_pipe<L, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_dense_pipe<L, NG>, 220 * 1024);
+    if (e != cudaSuccess) return e;
     const int smem = pipe_layout(pmax, L, NG).bytes;
     k_extract_dense_pipe<L, NG><<<grid, kPipeThreads, smem, sm>>>(work, ntiles, pmax, sbt, prm, st, x, n, hist,
                                                                   taps, ext, fault);
@@ -2541,11 +2537,9 @@ cudaError_t launch_extract_dense_pipe(int L, int ng, int ntiles, int grid, int p
 cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                 const float2 *hist, const float *taps, float2 *ext) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_extract_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_wide, 64 * 1024);
+    if (e != cudaSuccess) return e;
     k_extract_wide<<<grid, 256, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
     return cudaGetLastError();
 }
@@ -2553,12 +2547,9 @@ cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 
 cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                  const float2 *hist, const float *taps, float2 *ext, void *part) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_extract_group, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_group, 220 * 1024);
+    if (e != cudaSuccess) return e;
     k_extract_group<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
     return cudaGetLastError();
 }
@@ -2566,12 +2557,9 @@ cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2
 cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                const float2 *hist, const float *taps, float2 *ext, void *part) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_extract_mod, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_mod, 220 * 1024);
+    if (e != cudaSuccess) return e;
     k_extract_mod<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
     return cudaGetLastError();
 }
@@ -2696,12 +2684,9 @@ cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *
                            const SlotBlock *sbt, const ChanParams *prm, const RsBank *banks, AudState *aud,
                            const float *audio, float *rs_buf, int16_t *pcm) {
     const int smem = kAudBank * 8 + 2 * kAudWin * 4;
-    static bool attr_set = false;  // 64 KiB of dynamic shared memory needs the opt-in
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_audio48_rs, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> optin{0};  // 64 KiB of dynamic shared memory needs the opt-in
+    cudaError_t e = smem_optin_once(optin, (const void *)k_audio48_rs, smem);
+    if (e != cudaSuccess) return e;
     if (grid_rs > 0) k_audio48_rs<<<grid_rs, kAudThreads, smem, sm>>>(work, sbt, prm, banks, aud, audio, rs_buf);
     k_audio48_out<<<count, kAudOutThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
     return cudaGetLastError();

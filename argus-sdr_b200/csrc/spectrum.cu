@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/gpudemod.h"
+#include "gpud_internal.cuh"
 
 extern "C" void gpud_count_launch(int n);
 
@@ -115,11 +116,6 @@ GPUD_API int GPUD_CALL gpud_spectrum_create(int max_fft, int max_segments, gpud_
         gpud_spectrum_destroy(s);
         return GPUD_E_CUDA;
     }
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_spectrum_seg, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxFft * 16);
-        attr = true;
-    }
     *out = s;
     return 0;
 }
@@ -127,6 +123,9 @@ GPUD_API int GPUD_CALL gpud_spectrum_create(int max_fft, int max_segments, gpud_
 static int spectrum_launch(gpud_spectrum *s, const gpud_float2 *iq, int N, int segs, int step, int hann, int welch,
                            cudaStream_t st, double *out_db) {
     const int l2 = ilog2_exact(N);
+    // the shared-memory opt-in is per device: made on the launching device
+    static std::atomic<uint64_t> optin{0};
+    if (gpud::smem_optin_once(optin, (const void *)k_spectrum_seg, kMaxFft * 16) != cudaSuccess) return GPUD_E_CUDA;
     k_spectrum_seg<<<segs, kSpecThreads, N * 16, st>>>(reinterpret_cast<const float2 *>(iq), N, l2, step, hann, welch,
                                                        s->d_pow);
     k_spectrum_db<<<(N + 255) / 256, 256, 0, st>>>(s->d_pow, N, segs, welch, s->d_db);

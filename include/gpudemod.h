@@ -124,12 +124,14 @@ GPUD_API int GPUD_CALL gpud_launch_streaming_polyphase_stateful_cuda(
  * allocate device memory around the call (a real-time loop that must not stall
  * on cudaMalloc/cudaFree, which can synchronize the device; a process whose
  * device memory is committed to a fixed budget).  Same arguments minus the two
- * caller scratch buffers, same results and codes, plus GPUD_E_SCRATCH (-32)
- * when n_new > GPUD_NOALLOC_MAX_NEW or history_cap > GPUD_NOALLOC_MAX_HISTORY.
- * The scratch is one file-scope device array (about 2.1 MB) that every GPU
- * loading the library holds until exit; its device address is resolved on the
- * first call made on each device (make that call before any stream capture).
- * All calls share that array: calls that overlap on the GPU race. */
+ * caller scratch buffers, same results and codes (-10 and -11 are checked
+ * first), plus GPUD_E_SCRATCH (-32) when n_new > GPUD_NOALLOC_MAX_NEW or
+ * history_cap > GPUD_NOALLOC_MAX_HISTORY.  The scratch is one file-scope device
+ * array (about 2.1 MB) that every GPU loading the library holds until exit;
+ * its device address is resolved on the first call made on each device (make
+ * that call before any stream capture) and kept, so after cudaDeviceReset the
+ * entry point must not be called on that device again.  All calls share that
+ * array: calls that overlap on the GPU race. */
 #define GPUD_NOALLOC_MAX_NEW 262144
 #define GPUD_NOALLOC_MAX_HISTORY 4096
 #define GPUD_E_SCRATCH (-32)

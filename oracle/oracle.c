@@ -1839,3 +1839,127 @@ int or_demod_audio_segment(int mode, const cf32 *iq, int n, int fs, double offse
     *out_rate = orate;
     return nout;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Job construction (cmd/sdrd): the rules that turn detected signals into    */
+/* extraction jobs, i.e. which (out rate, taps, bandwidth) classes the       */
+/* extractor sees.  Go `int` is 64-bit: int64_t throughout.                  */
+/* ------------------------------------------------------------------------ */
+
+/* cmd/sdrd/streaming_refactor.go:105-137 nearestExactDecimationRate: the
+ * target itself when it divides the rate; else, over d = max(1, floor(sr /
+ * target) - 2) .. floor + 2, the rate sr / d (>= minRate, and only when it
+ * divides sr exactly) closest to the target, the first of equal distances;
+ * the target when none qualifies. */
+int64_t or_nearest_exact_decimation_rate(int64_t sample_rate, int64_t target, int64_t min_rate) {
+    if (sample_rate <= 0 || target <= 0) return target;
+    if (sample_rate % target == 0) return target;
+    int64_t td = sample_rate / target;
+    int64_t best = 0, best_dist = sample_rate;
+    int64_t d0 = td - 2 > 1 ? td - 2 : 1;
+    for (int64_t d = d0; d <= td + 2; d++) {
+        int64_t rate = sample_rate / d;
+        if (rate < min_rate) continue;
+        if (sample_rate % rate != 0) continue;
+        int64_t dist = target - rate;
+        if (dist < 0) dist = -dist;
+        if (dist < best_dist) {
+            best_dist = dist;
+            best = rate;
+        }
+    }
+    return best > 0 ? best : target;
+}
+
+/* cmd/sdrd/helpers.go:292-310 snapOutRate: among the divisors d <= 256 of the
+ * rate, the one closest to sr / target (float64 distance, first of equals);
+ * sr / d, or the target when the inputs are not positive. */
+int64_t or_snap_out_rate(int64_t sample_rate, int64_t target) {
+    if (sample_rate <= 0 || target <= 0) return target;
+    double ideal = (double)sample_rate / (double)target;
+    int64_t best_d = 0;
+    double best_err = 1.7976931348623157e308;
+    for (int64_t d = 1; d <= 256 && d <= sample_rate; d++) {
+        if (sample_rate % d != 0) continue;
+        double e = fabs((double)d - ideal);
+        if (e < best_err) {
+            best_err = e;
+            best_d = d;
+        }
+    }
+    if (best_d < 1) return target;
+    return sample_rate / best_d;
+}
+
+/* The WFM test shared by the job builders (streaming_refactor.go:27-28,
+ * helpers.go:178,449): centre in the 87.5-108 MHz broadcast band, or a
+ * classifier verdict of WFM / WFM_STEREO. */
+static int job_is_wfm(double center_hz, int class_wfm) {
+    double mhz = center_hz / 1e6;
+    return (mhz >= 87.5 && mhz <= 108.0) || class_wfm;
+}
+
+/* cmd/sdrd/streaming_refactor.go:16-60 buildStreamingJobs, one signal:
+ * bandwidth x bwMult (<= 0 means 1); WFM: out rate 512000 and bandwidth at
+ * least 250000; others: nearestExactDecimationRate(sr, 200000, 128000) and
+ * bandwidth at least 20000; taps = firTaps (<= 0 means 101); offset = centre
+ * - tuner centre.  Returns 0, or -1 where ExactIntegerDecimation rejects the
+ * out rate (the reference fails the whole batch). */
+int or_streaming_job(int64_t sample_rate, double tuner_center_hz, double sig_center_hz, double sig_bw_hz,
+                     int class_wfm, int fir_taps, double bw_mult, double *offset_hz, double *bw, int64_t *out_rate,
+                     int *num_taps) {
+    if (bw_mult <= 0) bw_mult = 1.0;
+    if (fir_taps <= 0) fir_taps = 101;
+    double b = sig_bw_hz * bw_mult;
+    int64_t rate;
+    if (job_is_wfm(sig_center_hz, class_wfm)) {
+        rate = 512000;
+        if (b < 250000) b = 250000;
+    } else {
+        rate = or_nearest_exact_decimation_rate(sample_rate, 200000, 128000);
+        if (b < 20000) b = 20000;
+    }
+    if (sample_rate <= 0 || rate <= 0 || sample_rate % rate != 0) return -1;
+    *offset_hz = sig_center_hz - tuner_center_hz;
+    *bw = b;
+    *out_rate = rate;
+    *num_taps = fir_taps;
+    return 0;
+}
+
+/* cmd/sdrd/helpers.go:174-194 extractSignalIQBatch, one signal's ExtractJob
+ * for the batch runner: out rate snapOutRate(sr, 512000) for WFM, else
+ * snapOutRate(sr, 200000); bandwidth floors 250000 (WFM) / 20000, no
+ * multiplier. */
+void or_batch_extract_job(int64_t sample_rate, double tuner_center_hz, double sig_center_hz, double sig_bw_hz,
+                          int class_wfm, double *offset_hz, double *bw, int64_t *out_rate) {
+    int wfm = job_is_wfm(sig_center_hz, class_wfm);
+    double b = sig_bw_hz;
+    if (wfm) {
+        if (b < 250000) b = 250000;
+    } else if (b < 20000) {
+        b = 20000;
+    }
+    *offset_hz = sig_center_hz - tuner_center_hz;
+    *bw = b;
+    *out_rate = or_snap_out_rate(sample_rate, wfm ? 512000 : 200000);
+}
+
+/* cmd/sdrd/pipeline_runtime.go:1094-1101: the RDS extraction job's out rate,
+ * ring rate / max(1, floor(ring rate / 250000)) (bandwidth 200000). */
+int64_t or_rds_job_out_rate(int64_t ring_rate) {
+    int64_t d = ring_rate / 250000;
+    if (d < 1) d = 1;
+    return ring_rate / d;
+}
+
+/* recorder/streamer.go:1098-1113 processSnippet's decim1: round(snip rate /
+ * demod rate), at least 1; WFM forced to 2 when above 2 and snip rate / 2 >=
+ * 200000.  Demod rates (OutputSampleRate in the demod package): WFM 192000, others
+ * 48000. */
+int or_snippet_decim(int64_t snip_rate, int64_t demod_rate, int wfm) {
+    int64_t d = (int64_t)round((double)snip_rate / (double)demod_rate);
+    if (d < 1) d = 1;
+    if (wfm && d > 2 && snip_rate / 2 >= 200000) d = 2;
+    return (int)d;
+}

@@ -71,6 +71,12 @@ def _load() -> C.CDLL:
         "or_channel_stereo_margins": (None, [P, P, P, P]),
         "or_channel_set_offset": (None, [P, d]),
         "or_channel_set_demod_decim": (i, [P, i]),
+        "or_nearest_exact_decimation_rate": (C.c_int64, [C.c_int64, C.c_int64, C.c_int64]),
+        "or_snap_out_rate": (C.c_int64, [C.c_int64, C.c_int64]),
+        "or_streaming_job": (i, [C.c_int64, d, d, d, i, i, d, P, P, P, P]),
+        "or_batch_extract_job": (None, [C.c_int64, d, d, d, i, P, P, P]),
+        "or_rds_job_out_rate": (C.c_int64, [C.c_int64]),
+        "or_snippet_decim": (i, [C.c_int64, C.c_int64, i]),
         "or_decim_fir_size": (C.c_size_t, []),
         "or_decim_fir_init": (i, [P, P, i, i]),
         "or_decim_fir_process": (i, [P, P, i, P]),
@@ -622,3 +628,45 @@ def welch_psd(iq, seg: int, overlap: float, window=None) -> np.ndarray:
     if segs == 0:
         return spectrum(iq, window)
     return np.roll(10 * np.log10(acc / segs + 1e-24), seg // 2)
+
+
+# --------------------------------------------------------------------------
+# job construction (cmd/sdrd): restated in oracle.c, wrapped here
+# --------------------------------------------------------------------------
+def nearest_exact_decimation_rate(sample_rate: int, target: int, min_rate: int) -> int:
+    """cmd/sdrd/streaming_refactor.go:105-137."""
+    return int(_lib.or_nearest_exact_decimation_rate(sample_rate, target, min_rate))
+
+
+def snap_out_rate(sample_rate: int, target: int) -> int:
+    """cmd/sdrd/helpers.go:292-310."""
+    return int(_lib.or_snap_out_rate(sample_rate, target))
+
+
+def streaming_job(sample_rate: int, tuner_center_hz: float, sig_center_hz: float, sig_bw_hz: float,
+                  class_wfm: bool, fir_taps: int = 0, bw_mult: float = 0.0):
+    """cmd/sdrd/streaming_refactor.go:16-60, one signal: (offset, bw, out_rate,
+    taps), or None where the reference returns ExactIntegerDecimation's error."""
+    off, bw, rate, taps = C.c_double(), C.c_double(), C.c_int64(), C.c_int()
+    rc = _lib.or_streaming_job(sample_rate, tuner_center_hz, sig_center_hz, sig_bw_hz, int(class_wfm), fir_taps,
+                               bw_mult, C.byref(off), C.byref(bw), C.byref(rate), C.byref(taps))
+    return None if rc else (off.value, bw.value, int(rate.value), int(taps.value))
+
+
+def batch_extract_job(sample_rate: int, tuner_center_hz: float, sig_center_hz: float, sig_bw_hz: float,
+                      class_wfm: bool):
+    """cmd/sdrd/helpers.go:174-194, one signal: (offset, bw, out_rate)."""
+    off, bw, rate = C.c_double(), C.c_double(), C.c_int64()
+    _lib.or_batch_extract_job(sample_rate, tuner_center_hz, sig_center_hz, sig_bw_hz, int(class_wfm), C.byref(off),
+                              C.byref(bw), C.byref(rate))
+    return off.value, bw.value, int(rate.value)
+
+
+def rds_job_out_rate(ring_rate: int) -> int:
+    """cmd/sdrd/pipeline_runtime.go:1094-1101."""
+    return int(_lib.or_rds_job_out_rate(ring_rate))
+
+
+def snippet_decim(snip_rate: int, demod_rate: int, wfm: bool) -> int:
+    """recorder/streamer.go:1098-1113."""
+    return int(_lib.or_snippet_decim(snip_rate, demod_rate, int(wfm)))

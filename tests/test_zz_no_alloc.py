@@ -73,12 +73,23 @@ def test_noalloc_matches_caller_scratch_entry_point(cuda):
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
+    import torch
+    taps = torch.zeros(16, dtype=torch.float32, device="cuda")
+    tp = C.c_void_p(taps.data_ptr())
     i, d = C.c_int(0), C.c_double(0.0)
     rc = lib.gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
-        None, GPUD_NOALLOC_MAX_NEW + 1, None, 16, 2, 8, None, 7, C.byref(i), C.byref(i), C.byref(d), 0.0, None, 0,
+        None, GPUD_NOALLOC_MAX_NEW + 1, tp, 16, 2, 8, None, 7, C.byref(i), C.byref(i), C.byref(d), 0.0, None, 0,
         C.byref(i))
     assert rc == GPUD_E_SCRATCH
     rc = lib.gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
-        None, 0, None, 16, 2, 8, None, GPUD_NOALLOC_MAX_HISTORY + 1, C.byref(i), C.byref(i), C.byref(d), 0.0, None,
+        None, 0, tp, 16, 2, 8, None, GPUD_NOALLOC_MAX_HISTORY + 1, C.byref(i), C.byref(i), C.byref(d), 0.0, None,
         0, C.byref(i))
     assert rc == GPUD_E_SCRATCH
+    # the base entry point's argument codes come before the scratch limits
+    rc = lib.gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
+        None, GPUD_NOALLOC_MAX_NEW + 1, tp, 16, 2, 8, None, 7, None, None, None, 0.0, None, 0, None)
+    assert rc == -10
+    rc = lib.gpud_launch_streaming_polyphase_stateful_noalloc_cuda(
+        None, -1, tp, 16, 2, 8, None, GPUD_NOALLOC_MAX_HISTORY + 1, C.byref(i), C.byref(i), C.byref(d), 0.0, None,
+        0, C.byref(i))
+    assert rc == -11
