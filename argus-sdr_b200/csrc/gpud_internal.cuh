@@ -13,6 +13,7 @@
 #pragma once
 #include <atomic>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #ifndef GPUD_PI
@@ -291,6 +292,12 @@ __device__ __forceinline__ double binade_value(const BinadeTable &t, int64_t k) 
     const BinadeEntry &b = t.e[lo];
     return b.x_start + (double)(k - b.k_start) * b.q;
 }
+
+// Host helpers shared by the runner and the engine entry points (runner.cu).
+// dsp.LowpassFIR (internal/dsp/fir.go:6-28): Hann-windowed sinc, odd length.
+std::vector<double> lowpass_fir(double cutoff_hz, int sample_rate, int taps);
+// Binade table of x_k = fl(x_{k-1} + inc), x_0 = 0, for inc > 0.
+int build_binade_table(double inc, BinadeTable *t);
 
 constexpr int kWfmTaps = 101;      // stereo / RDS filter length (streamer.go:1531-1545, fm.go:155)
 constexpr int kWfmHist = 100;

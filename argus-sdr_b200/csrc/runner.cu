@@ -143,7 +143,7 @@ constexpr int kMaxRsClasses = 16;  // 48 kHz resampler banks (one per demod rate
 // ---------------------------------------------------------------------------
 
 // dsp.LowpassFIR (internal/dsp/fir.go:6-28): Hann-windowed sinc, odd length.
-static std::vector<double> lowpass_fir(double cutoff_hz, int sample_rate, int taps) {
+std::vector<double> lowpass_fir(double cutoff_hz, int sample_rate, int taps) {
     if (taps % 2 == 0) taps++;
     std::vector<double> out((size_t)taps, 0.0);
     double fc = cutoff_hz / (double)sample_rate;
@@ -172,7 +172,7 @@ static void pll_coefficients(double loop_bw, double damping, int sample_rate, do
 }
 
 // Binade table of x_k = fl(x_{k-1} + inc), x_0 = 0, inc > 0 (see BinadeTable).
-static int build_binade_table(double inc, BinadeTable *t) {
+int build_binade_table(double inc, BinadeTable *t) {
     std::memset(t, 0, sizeof *t);
     const int64_t kmax = (int64_t)1 << 42;
     int64_t k = 1;

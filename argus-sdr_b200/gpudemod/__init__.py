@@ -333,6 +333,7 @@ class BatchRunner:
     def __init__(self, max_samples: int, sample_rate: int, max_channels: int = 256, max_taps: int = 1024):
         self._cr = ChannelRunner(sample_rate, max(1, max_samples), max_channels, max_taps)
         self.sampleRate = sample_rate
+        self._slots, self._slot_n, self._d_in = [], 0, None
 
     def StreamingExtractGPU(self, iq_new, jobs):
         """streaming_gpu_stub.go:21-26."""
@@ -350,10 +351,275 @@ class BatchRunner:
         """stream_state.go:18-24."""
         _check(self._cr._r, lib.gpud_runner_reset_all_signals(self._cr._r))
 
+    def ShiftFilterDecimateBatch(self, iq, jobs):
+        """batch_runner.go:61-68 with the GPU slot path of
+        batch_runner_windows.go:99-182: one H2D of the block; per job on its
+        own stream the shift from job.PhaseStart (phase PhaseStart + i*inc),
+        the 101-tap FIR (LowpassFIR(max(BW/2, 200)) as float32, zero history)
+        and the decimation by the exact integer factor (len(iq) // D outputs);
+        then each stream is synchronised and its output copied back.
+        Returns (outs, rates)."""
+        import torch
+        if self._cr is None:
+            raise ErrUnavailable("gpudemod batch runner unavailable")
+        n = len(iq)
+        outs, rates = [None] * len(jobs), [0] * len(jobs)
+        if n == 0:
+            return outs, rates
+        self._alloc_slots(len(jobs), n)
+        self._d_in[:n].copy_(torch.as_tensor(np.ascontiguousarray(iq, np.complex64)))
+        n_outs = []
+        for i, job in enumerate(jobs):
+            buf = self._slots[i]
+            taps = LowpassFIR(max(job.BW / 2, 200.0), self.sampleRate, 101).astype(np.float32)
+            buf["taps"][:taps.size].copy_(torch.from_numpy(taps))
+            decim = ExactIntegerDecimation(self.sampleRate, job.OutRate)
+            n_out = n // decim
+            if n_out <= 0:
+                raise ValueError("not enough output samples after decimation")
+            inc = -2.0 * np.pi * job.OffsetHz / self.sampleRate
+            torch.cuda.current_stream().synchronize()  # the block and taps copies have landed
+            s = buf["stream"]
+            for rc, what in ((lib.gpud_launch_freq_shift_stream_cuda(self._d_in.data_ptr(), buf["sh"].data_ptr(), n,
+                                                                     inc, float(job.PhaseStart), s), "freq shift"),
+                             (lib.gpud_launch_fir_v2_stream_cuda(buf["sh"].data_ptr(), buf["flt"].data_ptr(),
+                                                                 buf["taps"].data_ptr(), n, taps.size, s), "FIR v2"),
+                             (lib.gpud_launch_decimate_stream_cuda(buf["flt"].data_ptr(), buf["dec"].data_ptr(),
+                                                                   n_out, decim, s), "decimate")):
+                if rc != 0:
+                    raise RuntimeError(f"gpu {what} failed ({rc})")
+            n_outs.append(n_out)
+            rates[i] = self.sampleRate // decim
+        for i, n_out in enumerate(n_outs):
+            rc = lib.gpud_stream_sync(self._slots[i]["stream"])
+            if rc != 0:
+                raise RuntimeError(f"cuda stream sync failed ({rc})")
+            outs[i] = self._slots[i]["dec"][:n_out].cpu().numpy()
+        return outs, rates
+
+    def ShiftFilterDecimateBatchWithPhase(self, iq, jobs):
+        """batch_runner.go:72-98: ExtractResults with PhaseEnd = PhaseStart +
+        inc * len(iq)."""
+        outs, rates = self.ShiftFilterDecimateBatch(iq, jobs)
+        res = []
+        for i, job in enumerate(jobs):
+            inc = -2.0 * np.pi * job.OffsetHz / self.sampleRate
+            res.append(ExtractResult(outs[i], rates[i], job.PhaseStart + inc * len(iq)))
+        return res
+
+    def _alloc_slots(self, count: int, n: int):
+        """Per-slot device buffers and streams (batch_runner_windows.go:58-97):
+        reallocated when the slot count changes or the block grows."""
+        import torch
+        if len(self._slots) == count and n <= self._slot_n:
+            return
+        self._free_slots()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self._d_in = torch.empty(n, dtype=torch.complex64, device=dev)
+        for _ in range(count):
+            h = C.c_void_p()
+            rc = lib.gpud_stream_create(C.byref(h))
+            if rc != 0:
+                raise RuntimeError(f"cudaStreamCreate failed ({rc})")
+            self._slots.append({"sh": torch.empty(n, dtype=torch.complex64, device=dev),
+                                "flt": torch.empty(n, dtype=torch.complex64, device=dev),
+                                "dec": torch.empty(n, dtype=torch.complex64, device=dev),
+                                "taps": torch.empty(256, dtype=torch.float32, device=dev), "stream": h})
+        self._slot_n = n
+
+    def _free_slots(self):
+        for sl in self._slots:
+            lib.gpud_stream_destroy(sl["stream"])
+        self._slots, self._slot_n, self._d_in = [], 0, None
+
     def Close(self):
+        self._free_slots()
         if self._cr is not None:
             self._cr.close()
             self._cr = None
+
+
+@dataclass
+class ExtractJob:
+    """gpudemod.ExtractJob (batch.go:5-10)."""
+    OffsetHz: float
+    BW: float
+    OutRate: int
+    PhaseStart: float = 0.0
+
+
+@dataclass
+class ExtractResult:
+    """gpudemod.ExtractResult (batch.go:14-18)."""
+    IQ: np.ndarray
+    Rate: int
+    PhaseEnd: float
+
+
+def _go_round(x: float) -> int:
+    """math.Round for x >= 0: half away from zero (x - floor(x) is exact)."""
+    f = int(np.floor(x))
+    return f + 1 if x - f >= 0.5 else f
+
+
+def LowpassFIR(cutoff_hz: float, sample_rate: int, taps: int) -> np.ndarray:
+    """dsp.LowpassFIR (dsp/fir.go:6-28), float64, odd length."""
+    out = np.zeros((taps | 1) + 1, np.float64)
+    n = lib.gpud_lowpass_fir(float(cutoff_hz), int(sample_rate), int(taps),
+                             out.ctypes.data_as(C.POINTER(C.c_double)), out.size)
+    if n < 0:
+        raise ValueError(f"LowpassFIR({cutoff_hz}, {sample_rate}, {taps}) rejected: {n}")
+    return out[:n]
+
+
+class Engine:
+    """gpudemod.Engine (gpudemod.go:81-489): the single-signal shift / FIR /
+    decimate / demod engine, every stage on the device.
+
+    ShiftFilterDecimate and the front end of Demod give the results the
+    reference keeps: its CPU dsp chain (FreqShift from phase 0, incremented
+    before use; zero-history FIR with float64 accumulation; Decimate keeping
+    every D-th sample from index 0), here on the device through
+    gpud_shift_fir_decimate_cuda.  Demod's FIR taps are set on the first call
+    (101 taps of LowpassFIR(max(bw/2, 200))) and kept, as SetFIR keeps them;
+    the demodulators are the drop-in launchers: the discriminator, the AM
+    envelope without mean removal, and the BFO product whose phase advances
+    by 2*pi*bfo/sampleRate per decimated sample and carries across calls
+    (gpudemod.go:296-318)."""
+
+    def __init__(self, max_samples: int, sample_rate: int):
+        """gpudemod.New (gpudemod.go:103-150)."""
+        if max_samples <= 0:
+            raise ValueError("invalid maxSamples")
+        if sample_rate <= 0:
+            raise ValueError("invalid sampleRate")
+        if not Available():
+            raise ErrUnavailable("cuda device not available")
+        import torch
+        self.maxSamples, self.sampleRate = int(max_samples), int(sample_rate)
+        self.phase = 0.0
+        self.bfoPhase = 0.0
+        self.firTaps = None
+        self._dev = torch.device("cuda", torch.cuda.current_device())
+        self._in = torch.empty(self.maxSamples, dtype=torch.complex64, device=self._dev)
+        self._sh = torch.empty_like(self._in)
+        self._dec = torch.empty_like(self._in)
+        self._audio = torch.empty(self.maxSamples, dtype=torch.float32, device=self._dev)
+        self._taps = torch.empty(256, dtype=torch.float64, device=self._dev)
+        self.cudaReady = True
+        self._last_shift = self._last_demod = False
+
+    def SetFIR(self, taps):
+        """gpudemod.go:152-164: at most 256 float32 taps, uploaded to the
+        launchers' constant taps as well."""
+        t = np.asarray(taps, np.float32)[:256]
+        if t.size == 0:
+            self.firTaps = None
+            return
+        self.firTaps = t.copy()
+        if self.cudaReady:
+            lib.gpud_upload_fir_taps_cuda(self.firTaps.ctypes.data, self.firTaps.size)
+
+    def LastShiftUsedGPU(self) -> bool:
+        return self._last_shift
+
+    def LastDemodUsedGPU(self) -> bool:
+        return self._last_demod
+
+    def _front(self, iq, offset_hz: float, taps64: np.ndarray, decim: int):
+        """Shift, FIR and decimate on the device; returns the count."""
+        import torch
+        x = torch.as_tensor(np.ascontiguousarray(iq, np.complex64))
+        n = x.numel()
+        if n > self.maxSamples:
+            raise ValueError("sample count exceeds engine capacity")
+        self._in[:n].copy_(x)
+        self._taps[:taps64.size].copy_(torch.from_numpy(np.ascontiguousarray(taps64, np.float64)))
+        cnt = C.c_int()
+        rc = lib.gpud_shift_fir_decimate_cuda(self._in.data_ptr(), n, self.sampleRate, float(offset_hz),
+                                              self._taps.data_ptr(), taps64.size, int(decim), self._sh.data_ptr(),
+                                              self._dec.data_ptr(), self.maxSamples, C.byref(cnt), None)
+        if rc != 0:
+            raise GPUDError(rc, "shift/FIR/decimate launch failed")
+        return cnt.value
+
+    def ShiftFilterDecimate(self, iq, offset_hz: float, bw: float, out_rate: int):
+        """gpudemod.go:325-350: (IQ, rate) with cutoff BW/2 clamped to
+        [200, fs/2 - 1], 101 taps, decimation round(fs / out_rate)."""
+        if len(iq) == 0:
+            return None, 0
+        if out_rate <= 0:
+            raise ValueError("invalid output sample rate")
+        cutoff = min(max(bw / 2, 200.0), self.sampleRate / 2 - 1)
+        decim = max(1, _go_round(self.sampleRate / out_rate))
+        n = self._front(iq, offset_hz, LowpassFIR(cutoff, self.sampleRate, 101), decim)
+        self._last_shift = True
+        import torch
+        torch.cuda.synchronize(self._dev)
+        return self._dec[:n].cpu().numpy(), self.sampleRate // decim
+
+    def Demod(self, iq, offset_hz: float, bw: float, mode: int):
+        """gpudemod.go:356-461: (audio, demod input rate)."""
+        if not self.cudaReady:
+            raise RuntimeError("cuda demod engine is not initialized")
+        if len(iq) == 0:
+            return None, 0
+        if len(iq) > self.maxSamples:
+            raise ValueError("sample count exceeds engine capacity")
+        if mode in (DemodNFM, DemodAM, DemodUSB, DemodLSB, DemodCW):
+            out_rate = 48000
+        elif mode == DemodWFM:
+            out_rate = 192000
+        else:
+            raise ValueError("unsupported demod type")
+        if self.firTaps is None:
+            self.SetFIR(LowpassFIR(max(bw / 2, 200.0), self.sampleRate, 101).astype(np.float32))
+        decim = max(1, _go_round(self.sampleRate / out_rate))
+        m = self._front(iq, offset_hz, self.firTaps.astype(np.float64), decim)
+        self.phase += -2.0 * np.pi * offset_hz / self.sampleRate * len(iq)
+        self._last_shift = True
+        rate = self.sampleRate // decim
+        dec, audio = self._dec.data_ptr(), self._audio.data_ptr()
+        if mode in (DemodNFM, DemodWFM):
+            rc, cnt = lib.gpud_launch_fm_discrim_cuda(dec, audio, m), max(0, m - 1)
+        elif mode == DemodAM:
+            rc, cnt = lib.gpud_launch_am_envelope_cuda(dec, audio, m), m
+        else:
+            bfo = -700.0 if mode == DemodLSB else 700.0
+            inc = 2.0 * np.pi * bfo / self.sampleRate
+            rc, cnt = lib.gpud_launch_ssb_product_cuda(dec, audio, m, inc, self.bfoPhase), m
+            self.bfoPhase += inc * m
+        if rc != 0:
+            raise GPUDError(rc, "demod launch failed")
+        self._last_demod = True
+        import torch
+        torch.cuda.synchronize(self._dev)
+        return self._audio[:cnt].cpu().numpy(), rate
+
+    DemodFused = Demod  # gpudemod.go:352-354
+
+    def ShiftFilterDecimateBatch(self, iq, jobs):
+        """batch.go:20-32: ShiftFilterDecimate per job."""
+        outs, rates = [], []
+        for job in jobs:
+            o, r = self.ShiftFilterDecimate(iq, job.OffsetHz, job.BW, job.OutRate)
+            outs.append(o)
+            rates.append(r)
+        return outs, rates
+
+    def ShiftFilterDecimateBatchWithPhase(self, iq, jobs):
+        """batch.go:36-50: PhaseEnd = PhaseStart + inc * len(iq)."""
+        res = []
+        for job in jobs:
+            o, r = self.ShiftFilterDecimate(iq, job.OffsetHz, job.BW, job.OutRate)
+            inc = -2.0 * np.pi * job.OffsetHz / self.sampleRate
+            res.append(ExtractResult(o, r, job.PhaseStart + inc * len(iq)))
+        return res
+
+    def Close(self):
+        self._in = self._sh = self._dec = self._audio = self._taps = None
+        self.firTaps = None
+        self.cudaReady = False
 
 
 def NewBatchRunner(max_samples: int, sample_rate: int) -> BatchRunner:

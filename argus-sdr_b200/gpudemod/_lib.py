@@ -147,6 +147,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
             i, [P, i, P, P, i, i, i, P, P, i, pi, pi, pd, d, P, i, pi]),
         "gpud_launch_streaming_polyphase_stateful_noalloc_cuda": (
             i, [P, i, P, i, i, i, P, i, pi, pi, pd, d, P, i, pi]),
+        # engine front end
+        "gpud_lowpass_fir": (i, [d, i, i, pd, i]),
+        "gpud_shift_fir_decimate_cuda": (i, [P, i, i, d, P, i, i, P, P, i, pi, P]),
         # runner
         "gpud_runner_create": (i, [i, i, i, i, C.c_uint64, C.POINTER(P)]),
         "gpud_runner_destroy": (i, [P]),

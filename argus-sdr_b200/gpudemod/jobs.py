@@ -19,7 +19,7 @@ import math
 from dataclasses import dataclass
 
 from . import (CH_AUDIO48K, CH_RDS, MODE_AM, MODE_CW, MODE_LSB, MODE_NFM, MODE_USB, MODE_WFM, MODE_WFM_STEREO,
-               ExactIntegerDecimation, StreamingConfigHash, StreamingExtractJob)
+               ExactIntegerDecimation, ExtractJob, StreamingConfigHash, StreamingExtractJob)
 
 WFM_STREAM_OUT_RATE = 512_000   # helpers.go:279
 WFM_STREAM_MIN_BW = 250_000.0   # helpers.go:280
@@ -53,15 +53,6 @@ class ExtractionConfig:
     extraction bandwidth multiplier (<= 0: 1)."""
     firTaps: int = 0
     bwMult: float = 0.0
-
-
-@dataclass
-class ExtractJob:
-    """gpudemod.ExtractJob (batch.go:5-10)."""
-    OffsetHz: float
-    BW: float
-    OutRate: int
-    PhaseStart: float = 0.0
 
 
 def is_wfm(sig: Signal) -> bool:

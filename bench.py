@@ -384,7 +384,7 @@ def stage_key(name):
 # the kernel on the same workload (cold cache, serialised); None where no
 # capture exists.
 NCU_TRAFFIC = {("fm_band", "extract_gemm"): 8.73e6,
-               ("fm_band", "pll_newton"): 10.57e6,
+               ("fm_band", "pll"): 10.58e6,
                # k_extract_mod captured at 512 headroom channels (10.5 MB read, 42.2 MB
                # of partial sums written), scaled by the channel count to 2048
                ("headroom", "extract_mod"): 52.6e6 * 2048 / 512}

@@ -569,6 +569,33 @@ GPUD_API int GPUD_CALL gpud_spectrum_welch(gpud_spectrum *s, const gpud_float2 *
                                            double overlap, int hann, gpud_stream_handle stream, double *out_db,
                                            int *n_out);
 
+/* ======================================================================
+ * Part 8 -- the single-signal Engine's front end on the device
+ * (internal/demod/gpudemod/gpudemod.go:325-427).  The reference runs these
+ * stages with its CPU dsp functions; these entry points give the same
+ * results on the device so Engine.ShiftFilterDecimate / Engine.Demod and the
+ * legacy batch paths need no CPU stage.
+ * ====================================================================== */
+
+/* dsp.LowpassFIR (internal/dsp/fir.go:6-28): Hann-windowed sinc taps of
+ * odd length (taps | 1) into out (host, out_cap entries).  Returns the length
+ * or GPUD_E_ARG. */
+GPUD_API int GPUD_CALL gpud_lowpass_fir(double cutoff_hz, int sample_rate, int taps, double *out, int out_cap);
+
+/* dsp.Decimate(dsp.ApplyFIR(dsp.FreqShift(in, sample_rate, offset_hz), taps), decim)
+ * (gpudemod.go:336-350; dsp/freqshift.go:6-23, dsp/fir.go:31-95): the shift's
+ * phase restarts at 0 and is incremented before use by the reference's exact
+ * sequence of float64 additions; the FIR (num_taps <= 4096 float64 taps,
+ * device) has zero history and a float64 accumulator and is evaluated at the
+ * kept samples only; *n_out = ceil(n / decim) samples, every decim-th from
+ * index 0.  in, shifted_tmp (n samples), out (out_cap) and taps are device
+ * pointers; n_out is a host pointer.  Returns 0, GPUD_E_ARG or GPUD_E_CUDA;
+ * n <= 0 is a no-op. */
+GPUD_API int GPUD_CALL gpud_shift_fir_decimate_cuda(const gpud_float2 *in, int n, int sample_rate, double offset_hz,
+                                                    const double *taps, int num_taps, int decim,
+                                                    gpud_float2 *shifted_tmp, gpud_float2 *out, int out_cap,
+                                                    int *n_out /*host*/, gpud_stream_handle stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1963,3 +1963,192 @@ int or_snippet_decim(int64_t snip_rate, int64_t demod_rate, int wfm) {
     if (wfm && d > 2 && snip_rate / 2 >= 200000) d = 2;
     return (int)d;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The single-signal Engine (internal/demod/gpudemod/gpudemod.go, Linux) and */
+/* the legacy GPU batch slot (batch_runner_windows.go:142-182)               */
+/* ------------------------------------------------------------------------ */
+
+/* dsp.FreqShift (dsp/freqshift.go:6-23): phase from 0, incremented before
+ * use, float64 cos/sin, products rounded once per component; a copy when the
+ * offset is 0. */
+static void freq_shift_go(const cf32 *iq, int n, int fs, double offset, cf32 *out) {
+    if (n <= 0) return;
+    if (fs <= 0 || offset == 0) {
+        memcpy(out, iq, sizeof(cf32) * (size_t)n);
+        return;
+    }
+    double phase = 0.0;
+    double inc = -2 * OR_PI * offset / (double)fs;
+    for (int i = 0; i < n; i++) {
+        phase += inc;
+        double re = cos(phase), im = sin(phase);
+        double vr = iq[i].re, vi = iq[i].im;
+        out[i].re = (float)(vr * re - vi * im);
+        out[i].im = (float)(vr * im + vi * re);
+    }
+}
+
+/* dsp.Decimate(dsp.ApplyFIR(dsp.FreqShift(iq, fs, offset), taps), decim)
+ * (gpudemod.go:336-350; dsp/fir.go:31-95): zero-history FIR with float64
+ * accumulation, every decim-th output from index 0 (ceil(n/decim) of them;
+ * all n when decim <= 1).  Returns the count. */
+int or_shift_filter_decimate(const cf32 *iq, int n, int fs, double offset, const double *taps, int nt, int decim,
+                             cf32 *out) {
+    if (n <= 0 || nt <= 0) return 0;
+    if (decim < 1) decim = 1;
+    cf32 *sh = (cf32 *)malloc(sizeof(cf32) * (size_t)n);
+    freq_shift_go(iq, n, fs, offset, sh);
+    int cnt = 0;
+    for (int i = 0; i < n; i += decim) {
+        double ar = 0, ai = 0;
+        for (int k = 0; k < nt; k++) {
+            int idx = i - k;
+            if (idx < 0) break;
+            ar += (double)sh[idx].re * taps[k];
+            ai += (double)sh[idx].im * taps[k];
+        }
+        out[cnt].re = (float)ar;
+        out[cnt].im = (float)ai;
+        cnt++;
+    }
+    free(sh);
+    return cnt;
+}
+
+/* Engine.ShiftFilterDecimate (gpudemod.go:325-350): cutoff = BW/2 clamped to
+ * [200, fs/2 - 1], 101-tap LowpassFIR, decimation round(fs / out_rate) >= 1.
+ * Returns the count (-1 for a non-positive out rate); *rate = fs / decim. */
+int or_engine_shift_filter_decimate(const cf32 *iq, int n, int fs, double offset, double bw, int out_rate,
+                                    cf32 *out, int *rate) {
+    *rate = 0;
+    if (n <= 0) return 0;
+    if (out_rate <= 0) return -1;
+    double cutoff = bw / 2;
+    if (cutoff < 200) cutoff = 200;
+    if (cutoff > (double)fs / 2 - 1) cutoff = (double)fs / 2 - 1;
+    double taps[101];
+    or_lowpass_fir(cutoff, fs, 101, taps);
+    int decim = (int)round((double)fs / (double)out_rate);
+    if (decim < 1) decim = 1;
+    *rate = fs / decim;
+    return or_shift_filter_decimate(iq, n, fs, offset, taps, 101, decim, out);
+}
+
+/* Engine state across Demod calls (gpudemod.go:81-100): the FIR taps set on
+ * the first call (float32, at most 256) and the BFO phase of the SSB/CW
+ * product. */
+typedef struct {
+    int fs;
+    int nfir;
+    float fir[256];
+    double bfo_phase;
+} or_engine;
+
+size_t or_engine_size(void) { return sizeof(or_engine); }
+void or_engine_init(or_engine *e, int fs) {
+    memset(e, 0, sizeof *e);
+    e->fs = fs;
+}
+
+/* Engine.Demod (gpudemod.go:352-461) with the CUDA engine ready.  The shift,
+ * FIR and decimation stages take the results the reference keeps after its
+ * CPU comparison (ValidateFreqShift / ValidateFIR / ValidateDecimate,
+ * gpudemod.go:368-427): dsp.FreqShift from phase 0, the FIR with the first
+ * call's float32 taps (LowpassFIR(max(BW/2, 200), fs, 101)) accumulated in
+ * float64, dsp.Decimate by round(fs / rate), rate 192000 for WFM and 48000
+ * otherwise.  The demodulator is the GPU launcher the reference returns
+ * unchecked: the discriminator (n-1 outputs; float64 products and atan2 as
+ * the CPU path), the AM envelope without mean removal (exports.cu K6), the
+ * BFO product re*cos - im*sin with phase bfo_phase + i*inc and inc =
+ * 2 pi bfo / fs at the engine's full rate (gpudemod.go:296-318; BFO +700 Hz
+ * for USB and CW, -700 Hz for LSB), bfo_phase advanced by inc * count.
+ * mode: 0 NFM, 1 WFM, 2 AM, 3 USB, 4 LSB, 5 CW (DemodType).  Returns the
+ * audio count, *rate the demod input rate; -1 for an unknown mode. */
+int or_engine_demod(or_engine *e, const cf32 *iq, int n, double offset, double bw, int mode, float *audio,
+                    int *rate) {
+    *rate = 0;
+    if (n <= 0) return 0;
+    if (mode < 0 || mode > 5) return -1;
+    int out_rate = mode == 1 ? 192000 : 48000;
+    double cutoff = bw / 2;
+    if (cutoff < 200) cutoff = 200;
+    if (e->nfir == 0) {
+        double t64[101];
+        or_lowpass_fir(cutoff, e->fs, 101, t64);
+        for (int k = 0; k < 101; k++) e->fir[k] = (float)t64[k];
+        e->nfir = 101;
+    }
+    double taps[256];
+    for (int k = 0; k < e->nfir; k++) taps[k] = (double)e->fir[k];
+    int decim = (int)round((double)e->fs / (double)out_rate);
+    if (decim < 1) decim = 1;
+    int m = (n + decim - 1) / decim;
+    cf32 *dec = (cf32 *)malloc(sizeof(cf32) * (size_t)m);
+    m = or_shift_filter_decimate(iq, n, e->fs, offset, taps, e->nfir, decim, dec);
+    *rate = e->fs / decim;
+    int cnt = 0;
+    if (mode == 0 || mode == 1) {
+        if (m >= 2) cnt = or_fm_discrim(dec, m, audio);
+    } else if (mode == 2) {
+        for (int i = 0; i < m; i++) {
+            double x = dec[i].re, y = dec[i].im;
+            audio[i] = (float)sqrt(x * x + y * y);
+        }
+        cnt = m;
+    } else {
+        double bfo = mode == 4 ? -700.0 : 700.0;
+        double inc = 2.0 * OR_PI * bfo / (double)e->fs;
+        for (int i = 0; i < m; i++) {
+            double ph = e->bfo_phase + inc * (double)i;
+            ph -= rint(ph / 6.283185307179586) * 6.283185307179586;
+            audio[i] = (float)((double)dec[i].re * cos(ph) - (double)dec[i].im * sin(ph));
+        }
+        e->bfo_phase += inc * (double)m;
+        cnt = m;
+    }
+    free(dec);
+    return cnt;
+}
+
+/* One slot of the legacy GPU batch (batch_runner_windows.go:142-182,
+ * shiftFilterDecimateSlotParallel): 101-tap LowpassFIR(max(BW/2, 200), fs)
+ * as float32, exact integer decimation, the shift K1 with phase
+ * phase_start + i*inc (inc = -2 pi offset / fs, no pre-increment), the
+ * zero-history FIR K5 and the decimation K3: n / decim outputs,
+ * out[j] = filtered[j*decim].  Returns the count, -1 when fs / out_rate is
+ * not an integer, -2 when no output remains; *rate = fs / decim; *phase_end
+ * = phase_start + inc * n (batch_runner.go:83-88). */
+int or_batch_slot(const cf32 *iq, int n, int fs, double offset, double bw, int out_rate, double phase_start,
+                  cf32 *out, int *rate, double *phase_end) {
+    double cutoff = bw / 2;
+    if (cutoff < 200) cutoff = 200;
+    double t64[101];
+    or_lowpass_fir(cutoff, fs, 101, t64);
+    double taps[101];
+    for (int k = 0; k < 101; k++) taps[k] = (double)(float)t64[k];
+    if (fs <= 0 || out_rate <= 0 || fs % out_rate != 0) return -1;
+    int decim = fs / out_rate;
+    int nout = n / decim;
+    if (nout <= 0) return -2;
+    double inc = -2.0 * OR_PI * offset / (double)fs;
+    *rate = fs / decim;
+    *phase_end = phase_start + inc * (double)n;
+    for (int j = 0; j < nout; j++) {
+        int i = j * decim;
+        double ar = 0, ai = 0;
+        for (int k = 0; k < 101 && i - k >= 0; k++) {
+            int idx = i - k;
+            double ph = phase_start + inc * (double)idx;
+            ph -= rint(ph / 6.283185307179586) * 6.283185307179586;
+            double c = cos(ph), s = sin(ph);
+            double vr = iq[idx].re, vi = iq[idx].im;
+            float sr = (float)(vr * c - vi * s), si = (float)(vr * s + vi * c);
+            ar += (double)sr * taps[k];
+            ai += (double)si * taps[k];
+        }
+        out[j].re = (float)ar;
+        out[j].im = (float)ai;
+    }
+    return nout;
+}

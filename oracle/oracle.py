@@ -77,6 +77,12 @@ def _load() -> C.CDLL:
         "or_batch_extract_job": (None, [C.c_int64, d, d, d, i, P, P, P]),
         "or_rds_job_out_rate": (C.c_int64, [C.c_int64]),
         "or_snippet_decim": (i, [C.c_int64, C.c_int64, i]),
+        "or_shift_filter_decimate": (i, [P, i, i, d, P, i, i, P]),
+        "or_engine_shift_filter_decimate": (i, [P, i, i, d, d, i, P, P]),
+        "or_engine_size": (C.c_size_t, []),
+        "or_engine_init": (None, [P, i]),
+        "or_engine_demod": (i, [P, P, i, d, d, i, P, P]),
+        "or_batch_slot": (i, [P, i, i, d, d, i, d, P, P, P]),
         "or_decim_fir_size": (C.c_size_t, []),
         "or_decim_fir_init": (i, [P, P, i, i]),
         "or_decim_fir_process": (i, [P, P, i, P]),
@@ -670,3 +676,51 @@ def rds_job_out_rate(ring_rate: int) -> int:
 def snippet_decim(snip_rate: int, demod_rate: int, wfm: bool) -> int:
     """recorder/streamer.go:1098-1113."""
     return int(_lib.or_snippet_decim(snip_rate, demod_rate, int(wfm)))
+
+
+# --------------------------------------------------------------------------
+# the single-signal Engine and the legacy GPU batch slot
+# --------------------------------------------------------------------------
+def engine_shift_filter_decimate(iq, sample_rate: int, offset_hz: float, bw: float, out_rate: int):
+    """Engine.ShiftFilterDecimate (gpudemod.go:325-350): (IQ, rate)."""
+    x = _c64(iq)
+    out = np.zeros(x.size + 1, np.complex64)
+    rate = C.c_int()
+    n = _lib.or_engine_shift_filter_decimate(_p(x), x.size, sample_rate, offset_hz, bw, out_rate, _p(out),
+                                             C.byref(rate))
+    if n < 0:
+        raise ValueError("invalid output sample rate")
+    return out[:n], rate.value
+
+
+class Engine:
+    """Engine.Demod state (gpudemod.go:81-100): first-call FIR taps and the
+    BFO phase.  mode is the DemodType (0 NFM .. 5 CW)."""
+
+    def __init__(self, sample_rate: int):
+        self._st = np.zeros(_lib.or_engine_size(), np.uint8)
+        _lib.or_engine_init(_p(self._st), sample_rate)
+
+    def demod(self, iq, offset_hz: float, bw: float, mode: int):
+        x = _c64(iq)
+        out = np.zeros(x.size + 1, np.float32)
+        rate = C.c_int()
+        n = _lib.or_engine_demod(_p(self._st), _p(x), x.size, offset_hz, bw, mode, _p(out), C.byref(rate))
+        if n < 0:
+            raise ValueError("unsupported demod type")
+        return out[:n], rate.value
+
+
+def batch_slot(iq, sample_rate: int, offset_hz: float, bw: float, out_rate: int, phase_start: float = 0.0):
+    """One legacy GPU batch slot (batch_runner_windows.go:142-182):
+    (IQ, rate, phase_end)."""
+    x = _c64(iq)
+    out = np.zeros(x.size + 1, np.complex64)
+    rate, pe = C.c_int(), C.c_double()
+    n = _lib.or_batch_slot(_p(x), x.size, sample_rate, offset_hz, bw, out_rate, phase_start, _p(out), C.byref(rate),
+                           C.byref(pe))
+    if n == -1:
+        raise ValueError("non-integer decimation")
+    if n == -2:
+        raise ValueError("not enough output samples after decimation")
+    return out[:n], rate.value, pe.value
