@@ -1282,17 +1282,18 @@ struct PllEval {
     float iphi, qphi;       // I/Q rows' d/dphase (diagonals are 1 - lpa)
 };
 
-__device__ __forceinline__ void pll_angle(const PllK &k, int t, double dphi, float &s, float &c) {
-    const uint64_t q = k.q0 + (uint64_t)t * k.qf;
+// q: the ramp phase phase0 + t*freq0 of step t in Q0.64 turns (callers carry
+// it by adding k.qf per step: the same integer as k.q0 + t*k.qf).
+__device__ __forceinline__ void pll_angle(uint64_t q, double dphi, float &s, float &c) {
     const float h = (float)(int32_t)(q >> 32) * 4.656612873077393e-10f + (float)(dphi * (1.0 / GPUD_PI));
     __sincosf(h * 3.14159265358979f, &s, &c);  // |angle| <= pi + |dphi|
 }
 
 template <bool kJac>
-__device__ __forceinline__ void pll_step(int t, double dphi, double df, float I, float Q, float p, const PllK &k,
+__device__ __forceinline__ void pll_step(uint64_t q, double dphi, double df, float I, float Q, float p, const PllK &k,
                                          PllEval &o) {
     float sn, cs;
-    pll_angle(k, t, dphi, sn, cs);
+    pll_angle(q, dphi, sn, cs);
     o.I1 = fmaf(k.lpa, fmaf(p, cs, -I), I);
     o.Q1 = fmaf(k.lpa, fmaf(p, -sn, -Q), Q);
     const float e = atan2f(o.Q1, o.I1);
@@ -1309,8 +1310,10 @@ __device__ __forceinline__ void pll_step(int t, double dphi, double df, float I,
     o.df1 = d;
     o.dphi1 = dphi + d + k.alpha * (double)e;
     if (kJac) {
+        // the Jacobian sets the convergence rate only, not the fixed point:
+        // an approximate reciprocal is enough
         const float r2 = fmaf(o.I1, o.I1, o.Q1 * o.Q1);
-        const float inv = r2 > 0.f ? __frcp_rn(r2) : 0.f;
+        const float inv = r2 > 0.f ? __fdividef(1.f, r2) : 0.f;
         const float gI = -o.Q1 * inv, gQ = o.I1 * inv;
         const float dIphi = -k.lpa * p * sn;  // d/dphase of lpa*p*cos(phase)
         const float dQphi = -k.lpa * p * cs;  // d/dphase of -lpa*p*sin(phase)
@@ -1352,9 +1355,10 @@ __device__ __forceinline__ double pll_phase_at(const PllK &k, int t, double dphi
     return ph;
 }
 
-// 2*sin(2*phase) of the loop phase after t steps, float32 (lr = bpf * that).
-__device__ __forceinline__ float pll_two_sin2(const PllK &k, int t, double dphi) {
-    const uint64_t q2 = 2 * (k.q0 + (uint64_t)t * k.qf);
+// 2*sin(2*phase) of the loop phase, float32 (lr = bpf * that); q is the ramp
+// phase of the same step in Q0.64 turns.
+__device__ __forceinline__ float pll_two_sin2(uint64_t q, double dphi) {
+    const uint64_t q2 = 2 * q;
     const float h = (float)(int32_t)(q2 >> 32) * 4.656612873077393e-10f + (float)(dphi * (2.0 / GPUD_PI));
     return 2.0f * sinpif(h);
 }
@@ -1448,15 +1452,17 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
                 float *th = s_th[c & 1];
                 const int base = c * kPllChunk;
                 const int len = min(kPllChunk, n - base);
+                uint64_t qr = k.q0 + (uint64_t)base * k.qf;
                 for (int q = 0; q < len; ++q) {
                     PllEval o;
-                    pll_step<false>(base + q, dphi, df, I, Q, sp[q], k, o);
+                    pll_step<false>(qr, dphi, df, I, Q, sp[q], k, o);
+                    qr += k.qf;
                     dphi = o.dphi1;
                     df = o.df1;
                     I = o.I1;
                     Q = o.Q1;
                     es += fabs((double)o.e);
-                    th[q] = pll_two_sin2(k, base + q + 1, dphi);
+                    th[q] = pll_two_sin2(qr, dphi);
                 }
             }
         } else {
@@ -1617,7 +1623,15 @@ struct SegState {
 };
 
 // One channel-block per cluster of `gridDim.x / count` CTAs; the block's steps
-// are split into one contiguous segment per thread of the cluster.
+// are split into one contiguous segment per thread of the cluster.  With
+// segments of at most kPllStageS steps (blocks of up to 32768 composite
+// samples) each CTA first stages its span of the pilot band in shared memory,
+// transposed (step i of thread j's segment at [i][j], conflict-free), so every
+// Newton sweep reads it from there; the output sweep writes 2 sin(2 phase)
+// back into the same cells and the CTA then writes the L-R products with
+// coalesced stores.
+constexpr int kPllStageS = 16;
+
 __global__ void __launch_bounds__(kNewtonThreads, 3)
 k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
              const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
@@ -1629,8 +1643,10 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     __shared__ float s_cta[2][20];       // CTA total, double-buffered across iterations
     __shared__ float s_max[kNW][4];
     __shared__ float s_cmax[2][4];       // CTA max |d|, double-buffered
+    __shared__ float s_dcta[4];          // d at this CTA's first segment
     __shared__ SegState s_first[kNW];    // each warp's first segment start (lane 0)
     __shared__ float s_jac[16][kNewtonThreads];  // each segment's Jacobian, kept for chord steps
+    __shared__ float s_seg[kPllStageS][kNewtonThreads + 1];  // staged pilot band / 2 sin(2 phase)
     __shared__ double s_sum[kNW][2];
     __shared__ double s_csum[2];
     const int csize = (int)cl.num_blocks();
@@ -1657,6 +1673,17 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     const int g = crank * kNewtonThreads + (int)threadIdx.x;
     const int t0 = min(n, g * S), t1 = min(n, t0 + S);
     const bool has_next = t1 < n;  // the next thread's segment is not empty
+    const bool staged = S <= kPllStageS;  // uniform
+    const int cbase = min(n, crank * kNewtonThreads * S);
+    const int cend = min(n, cbase + kNewtonThreads * S);
+    if (staged) {
+        for (int t = cbase + (int)threadIdx.x; t < cend; t += kNewtonThreads) {
+            const int r = t - cbase;
+            s_seg[r % S][r / S] = __ldg(pil + t);
+        }
+        __syncthreads();
+    }
+    auto pilot = [&](int t) -> float { return staged ? s_seg[t - t0][threadIdx.x] : __ldg(pil + t); };
     SegState x0{0.0, 0.0, I0, Q0};  // this segment's start: the free-running guess
     bool converged = false, bad = true;
     float prev_m0 = 1e30f;  // last iteration's largest phase correction (uniform in the cluster)
@@ -1689,25 +1716,23 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
         aff_identity(m);
         SegState x = x0;
         if (t0 < t1) {
-            float pt = __ldg(pil + t0);
+            uint64_t qr = k.q0 + (uint64_t)t0 * k.qf;
             if (jac) {
                 for (int t = t0; t < t1; ++t) {
-                    const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
                     PllEval o;
-                    pll_step<true>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                    pll_step<true>(qr, x.dphi, x.df, x.I, x.Q, pilot(t), k, o);
+                    qr += k.qf;
                     mat_push(m.a, o, om);
                     x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
-                    pt = pn;
                 }
 #pragma unroll
                 for (int i = 0; i < 16; ++i) s_jac[i][threadIdx.x] = m.a[i];
             } else {
                 for (int t = t0; t < t1; ++t) {
-                    const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
                     PllEval o;
-                    pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                    pll_step<false>(qr, x.dphi, x.df, x.I, x.Q, pilot(t), k, o);
+                    qr += k.qf;
                     x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
-                    pt = pn;
                 }
 #pragma unroll
                 for (int i = 0; i < 16; ++i) m.a[i] = s_jac[i][threadIdx.x];
@@ -1749,17 +1774,28 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             if (lane == kNW - 1) aff_store(s_cta[pb], wv);
         }
         cl.sync();  // CTA totals of the whole cluster are visible
-        float dcta[4] = {0.f, 0.f, 0.f, 0.f};  // d at this CTA's first segment
-        for (int r = 0; r < crank; ++r) {
-            Aff rm;
-            aff_load(rm, cl.map_shared_rank(&s_cta[pb][0], r));
-            float tmp[4];
-            aff_apply(tmp, rm, dcta);
-            dcta[0] = tmp[0];
-            dcta[1] = tmp[1];
-            dcta[2] = tmp[2];
-            dcta[3] = tmp[3];
+        // d at this CTA's first segment: the CTA totals before it, composed by
+        // a scan across warp 0's lanes (lane r holds CTA r's total) and
+        // applied to a zero correction
+        if (warp == 0) {
+            Aff tv;
+            if (lane < crank) aff_load(tv, cl.map_shared_rank(&s_cta[pb][0], lane));
+            else aff_identity(tv);
+#pragma unroll
+            for (int d = 1; d < kNewtonMaxCluster; d <<= 1) {
+                Aff o;
+                aff_shfl_up(o, tv, d);
+                if (lane >= d) aff_compose(tv, tv, o);
+            }
+            const int src = crank > 0 ? crank - 1 : 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float v = __shfl_sync(0xffffffffu, tv.b[i], src);
+                if (lane == 0) s_dcta[i] = crank > 0 ? v : 0.f;
+            }
         }
+        __syncthreads();
+        const float dcta[4] = {s_dcta[0], s_dcta[1], s_dcta[2], s_dcta[3]};
         float dl[4];
         {
             Aff wx;
@@ -1845,18 +1881,30 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     SegState x = x0;
     if (t0 < t1) {
         const bool out = g < gstar;
-        float pt = __ldg(pil + t0);
+        uint64_t qr = k.q0 + (uint64_t)t0 * k.qf;
         for (int t = t0; t < t1; ++t) {
-            const float pn = (t + 1 < t1) ? __ldg(pil + t + 1) : 0.f;
+            const float pt = pilot(t);
             pp += (double)pt * (double)pt;
             if (out) {
                 PllEval o;
-                pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                pll_step<false>(qr, x.dphi, x.df, x.I, x.Q, pt, k, o);
+                qr += k.qf;
                 x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
                 es += fabs((double)o.e);
-                lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x.dphi);
+                const float th = pll_two_sin2(qr, x.dphi);
+                if (staged)
+                    s_seg[t - t0][threadIdx.x] = th;  // this thread's own cell, already read
+                else
+                    lr[t] = bpf[t] * th;
             }
-            pt = pn;
+        }
+    }
+    if (staged) {
+        // the L-R products of this CTA's output segments, coalesced
+        __syncthreads();
+        for (int t = cbase + (int)threadIdx.x; t < cend; t += kNewtonThreads) {
+            const int r = t - cbase;
+            if (crank * kNewtonThreads + r / S < gstar) lr[t] = bpf[t] * s_seg[r % S][r / S];
         }
     }
 #pragma unroll
@@ -1894,14 +1942,16 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     if (g != owner) return;
     if (!converged) {
         // serial loop from the exact start of segment gstar to the block end
+        uint64_t qr = k.q0 + (uint64_t)t0 * k.qf;
         float pt = __ldg(pil + t0);
         for (int t = t0; t < n; ++t) {
             const float pn = (t + 1 < n) ? __ldg(pil + t + 1) : 0.f;
             PllEval o;
-            pll_step<false>(t, x.dphi, x.df, x.I, x.Q, pt, k, o);
+            pll_step<false>(qr, x.dphi, x.df, x.I, x.Q, pt, k, o);
+            qr += k.qf;
             x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
             es_all += fabs((double)o.e);
-            lr[t] = bpf[t] * pll_two_sin2(k, t + 1, x.dphi);
+            lr[t] = bpf[t] * pll_two_sin2(qr, x.dphi);
             pt = pn;
         }
     }

@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--plan-only", action="store_true",
                     help="form the process world and print the channel shards (no GPU work)")
     ap.add_argument("--no-serving", action="store_true", help="fm_band: leave out the serving phases")
+    ap.add_argument("--no-autotune", action="store_true", help="mixed: keep the runner's static form rule")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu (no baselines)")
     ap.add_argument("--workload", default="fm_band", choices=["fm_band", "mixed", "serving", "headroom"],
                     help="fm_band: the FM band batch (headline); mixed: the mixed-mode uneven batch; "
@@ -265,7 +266,7 @@ def gemm_grouped(chans, n_in=BLOCK):
         T, D = c["T"], c["D"]
         fm = c["kind"] in ("NFM", "WFM")
         precise = fm and c.get("bw") is not None and c["out_rate"] >= 4 * max(c["bw"], 400.0)
-        if extraction_form(T, D) != "extract_dense" or D % 4 or precise or n_in // D <= 256:
+        if (c.get("form") or extraction_form(T, D)) != "extract_dense" or D % 4 or precise or n_in // D <= 256:
             continue
         classes.setdefault((T, D), []).append(i)
     grouped, tensor_flop = set(), 0
@@ -324,7 +325,7 @@ def algorithmic_work(chans, n_in=BLOCK):
             fw["flop"] += f - f0
             fw["bytes"] += b - 8 * 256
         else:
-            fw = forms.setdefault(extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
+            fw = forms.setdefault(c.get("form") or extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
             fw["flop"] += f
             fw["bytes"] += b
         w["demod"]["flop"] += per_out[c["kind"]] * n_out
@@ -814,8 +815,24 @@ def run_mixed(args, world, rank, local):
         out_rate, taps, bw = synth.MODE_TABLE[kind]
         chans.append(dict(kind=kind, T=taps, D=FS // out_rate, out_rate=out_rate, bw=bw, off=off))
 
+    # extraction forms per (taps, decimation) class chosen by the autotuner,
+    # measured on this GPU before anything is timed
+    tune = None
+    if not args.no_autotune:
+        from gpudemod import autotune
+        classes = sorted({(c["T"], c["D"]) for c in chans})
+        table, report = autotune.tune(FS, BLOCK, classes)
+        names = {G.FORM_DENSE: "dense", G.FORM_WIDE: "wide", G.FORM_GROUP: "group", G.FORM_MOD: "mod"}
+        tune = {"table": table,
+                "chosen": {f"T{T}_D{D}": f"{names[f]}" + (f"/pg{pg}" if pg else "") for T, D, f, pg in table},
+                "candidates_ms": {f"T{T}_D{D}": {names[f] + (f"/pg{pg}" if pg else ""): round(ms, 4)
+                                                 for (f, pg), ms in times.items()}
+                                  for (T, D), times in report.items()}}
+
     def make_runner():
         r = G.ChannelRunner(FS, BLOCK, max_channels=128, max_taps=1024)
+        if tune is not None:
+            r.set_autotune_table(tune["table"])
         for i, c in enumerate(chans):
             r.admit(i, c["off"], c["bw"], c["out_rate"], c["T"], mode[c["kind"]], G.CH_AUDIO48K)
         return r
@@ -840,6 +857,10 @@ def run_mixed(args, world, rank, local):
                 "sample": f"{len(oc)} channels x {nb} blocks of 2^20 through the oracle chain ({dt:.1f} s wall)"}
 
     runner = make_runner()
+    form_key = {G.FORM_DENSE: "extract_dense", G.FORM_WIDE: "extract_wide", G.FORM_GROUP: "extract_group",
+                G.FORM_MOD: "extract_mod"}
+    for i, c in enumerate(chans):  # the runner's own form per channel (slots in admission order)
+        c["form"] = form_key[runner.channel_form(i)[0]]
     res = measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, "mixed", make_runner,
                         cpu_baseline)
     runner.close()
@@ -847,6 +868,8 @@ def run_mixed(args, world, rank, local):
         return None
     line = {"metric": "aggregate channel-MS/s on 1 B200, mixed-mode uneven batch", "unit": "channel-MS/s"}
     line.update(res)
+    if tune is not None:
+        line["autotune"] = {k: v for k, v in tune.items() if k != "table"}
     line["config"] = {"workload": MIXED_WORKLOAD, "channels": len(chans), "block": BLOCK,
                       "inputs": f"{n_scene} consecutive 8 MiB blocks resident in HBM ({n_scene * 8} MiB > L2)",
                       "parallelism": f"channel shards, {world} GPU(s), no data-path collective"}
