@@ -1761,8 +1761,9 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
             Aff wv;
             if (lane < kNW) aff_load(wv, s_tot[lane]);
             else aff_identity(wv);
+            // only lanes 0..kNW-1 carry warp totals: log2(kNW) rounds
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
+            for (int d = 1; d < kNW; d <<= 1) {
                 Aff o;
                 aff_shfl_up(o, wv, d);
                 if (lane >= d) aff_compose(wv, wv, o);
@@ -2424,7 +2425,8 @@ __global__ void __launch_bounds__(kAudOutThreads)
 k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
               const RsBank *__restrict__ banks, AudState *__restrict__ aud, const float *__restrict__ audio,
               const float *__restrict__ rs_out, int16_t *__restrict__ pcm) {
-    __shared__ double s_a[kAudOutThreads], s_b[2][kAudOutThreads];
+    constexpr int kWarps = kAudOutThreads / 32;
+    __shared__ double s_wa[kWarps], s_wb[2][kWarps];  // warp totals, then exclusive warp prefixes
     const SlotBlock sb = sbt[list[blockIdx.x]];
     const ChanParams &cp = prm[sb.slot];
     AudState &as = aud[sb.slot];
@@ -2447,33 +2449,59 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
             B0 = __dadd_rn(__dmul_rn(a, B0), __dmul_rn(1.0 - a, (double)r[o * C]));
             if (C == 2) B1 = __dadd_rn(__dmul_rn(a, B1), __dmul_rn(1.0 - a, (double)r[o * 2 + 1]));
         }
-        s_a[threadIdx.x] = A;
-        s_b[0][threadIdx.x] = B0;
-        s_b[1][threadIdx.x] = B1;
+        // inclusive scan of the maps across the warp (a later run applied
+        // after an earlier one), then across the warps' totals
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double pa = __shfl_up_sync(0xffffffffu, A, d);
+            const double pb0 = __shfl_up_sync(0xffffffffu, B0, d);
+            const double pb1 = __shfl_up_sync(0xffffffffu, B1, d);
+            if (lane >= d) {
+                B0 = A * pb0 + B0;
+                B1 = A * pb1 + B1;
+                A = A * pa;
+            }
+        }
+        if (lane == 31) {
+            s_wa[warp] = A;
+            s_wb[0][warp] = B0;
+            s_wb[1][warp] = B1;
+        }
         __syncthreads();
-        // inclusive scan of the maps (a later run applied after an earlier one)
-        for (int d = 1; d < kAudOutThreads; d <<= 1) {
-            double pa = 1.0, pb0 = 0.0, pb1 = 0.0;
-            const bool take = (int)threadIdx.x >= d;
-            if (take) {
-                pa = s_a[threadIdx.x - d];
-                pb0 = s_b[0][threadIdx.x - d];
-                pb1 = s_b[1][threadIdx.x - d];
+        if (warp == 0) {
+            double wa = lane < kWarps ? s_wa[lane] : 1.0;
+            double wb0 = lane < kWarps ? s_wb[0][lane] : 0.0, wb1 = lane < kWarps ? s_wb[1][lane] : 0.0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const double pa = __shfl_up_sync(0xffffffffu, wa, d);
+                const double pb0 = __shfl_up_sync(0xffffffffu, wb0, d);
+                const double pb1 = __shfl_up_sync(0xffffffffu, wb1, d);
+                if (lane >= d) {
+                    wb0 = wa * pb0 + wb0;
+                    wb1 = wa * pb1 + wb1;
+                    wa = wa * pa;
+                }
             }
-            __syncthreads();
-            if (take) {
-                const double ca = s_a[threadIdx.x];
-                s_b[0][threadIdx.x] = ca * pb0 + s_b[0][threadIdx.x];
-                s_b[1][threadIdx.x] = ca * pb1 + s_b[1][threadIdx.x];
-                s_a[threadIdx.x] = ca * pa;
+            // exclusive: the warps before this one
+            const double ea = __shfl_up_sync(0xffffffffu, wa, 1);
+            const double eb0 = __shfl_up_sync(0xffffffffu, wb0, 1);
+            const double eb1 = __shfl_up_sync(0xffffffffu, wb1, 1);
+            if (lane < kWarps) {
+                s_wa[lane] = lane ? ea : 1.0;
+                s_wb[0][lane] = lane ? eb0 : 0.0;
+                s_wb[1][lane] = lane ? eb1 : 0.0;
             }
-            __syncthreads();
         }
-        if (threadIdx.x > 0) {
-            const double pa = s_a[threadIdx.x - 1];
-            y0 = pa * as.y[0] + s_b[0][threadIdx.x - 1];
-            y1 = pa * as.y[1] + s_b[1][threadIdx.x - 1];
-        }
+        __syncthreads();
+        // this run's start: the warps before it, then the lanes before it
+        const double la = __shfl_up_sync(0xffffffffu, A, 1);
+        const double lb0 = __shfl_up_sync(0xffffffffu, B0, 1);
+        const double lb1 = __shfl_up_sync(0xffffffffu, B1, 1);
+        const double ws0 = s_wa[warp] * as.y[0] + s_wb[0][warp];
+        const double ws1 = s_wa[warp] * as.y[1] + s_wb[1][warp];
+        y0 = lane ? la * ws0 + lb0 : ws0;
+        y1 = lane ? la * ws1 + lb1 : ws1;
     }
     for (int o = o0; o < o1; ++o) {
         for (int c = 0; c < C; ++c) {

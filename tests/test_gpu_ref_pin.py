@@ -246,7 +246,12 @@ def test_legacy_batch_chain_pinned(ref, fs, jobs):
     import torch
 
     import gpudemod as G
-    x = make_tone_noise_iq(1 << 18, 0.9)
+    # a tone 1 kHz inside each job's passband, plus the noise-like mix
+    t = np.arange(1 << 18, dtype=np.float64)
+    x = 0.1 * make_tone_noise_iq(t.size, 0.9).astype(np.complex128)
+    for off, _, _, _ in jobs:
+        x += np.exp(2j * np.pi * (off + 1000.0) / fs * t)
+    x = x.astype(np.complex64)
     br = G.NewBatchRunner(x.size, fs)
     try:
         outs, rates = br.ShiftFilterDecimateBatch(x, [G.ExtractJob(o, b, r, p) for o, b, r, p in jobs])
