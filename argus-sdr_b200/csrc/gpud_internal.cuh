@@ -164,7 +164,7 @@ struct SlotBlock {
     int32_t ng;
     int32_t pg;
     int32_t part_off;
-    int32_t pad_sb;
+    int32_t wide_end;  // > 0: the warp-per-output kernel computes only outputs before it (the rest: a bank)
 };
 
 // Channel group extracted on the tensor cores (gemm_extract.cu): channels of
@@ -179,6 +179,20 @@ struct GemmGroup {
     int32_t mem_off;
     int32_t ns;      // taps stages in shared memory
     int32_t na;      // TMEM accumulators (arm u accumulates into u % na; summed in the epilogue)
+};
+
+// Short-arm channel bank (bank_extract.cu): channels of one decimation D, tap
+// count T <= 4D and phase count pc share the input grid; every output from
+// jt0 on is computed for all members from one staging of the input windows.
+struct BankGroup {
+    int32_t nmem;    // channels (members[mem_off .. mem_off + nmem): SlotBlock rows)
+    int32_t cpad;    // channel columns of the packed taps (a multiple of 32)
+    int32_t D, T, pc;
+    int32_t n_out;   // outputs of every member this block
+    int32_t jt0;     // first output of the bank tiles (earlier ones: the warp-per-output kernel)
+    int32_t mem_off;
+    int32_t g_off;   // float2 offset of the packed modulated taps (T x cpad) in the frame's buffer
+    int32_t r;       // outputs per lane of a work item (1, 2 or 4): 8r outputs per item
 };
 
 // Rational polyphase resampler bank (dsp/resample.go:45-93) for one input rate.

@@ -49,6 +49,14 @@ cudaError_t launch_extract_gemm(int grid, int smem, cudaStream_t sm, const int2 
                                 const float2 *x, int n, const float *gb, float2 *ext, unsigned *fault);
 int gemm_smem_bytes_host(int D, int L, int N, int ns);
 int gemm_tile();
+cudaError_t launch_bank_pack(int ngroups, int max_total, cudaStream_t sm, const BankGroup *groups,
+                             const int *members, const SlotBlock *sbt, const ChanParams *prm, const float *taps,
+                             float2 *gtab);
+cudaError_t launch_extract_bank(int grid, cudaStream_t sm, const int2 *work, const BankGroup *groups,
+                                const int *members, const SlotBlock *sbt, const ChanParams *prm, const ChanState *st,
+                                const float2 *x, const float2 *gtab, float2 *ext);
+int bank_lanes();
+int bank_warps();
 size_t gemm_pack_bytes_host(int D, int L, int N);
 cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                 const ChanParams *prm, const ChanState *st, const float2 *x, int n,
@@ -125,6 +133,12 @@ constexpr int kDensePipeSmemCap = 220 * 1024;  // what the pipelined dense kerne
 constexpr int kGemmMinChannels = 4;           // smaller groups stay on the dense kernel
 constexpr int kGemmSmemCap = 220 * 1024;
 constexpr int kGemmFirstOutput = 256;         // outputs before it (history) stay on the dense kernel
+#ifndef GPUD_BANK_EXTRACT
+#define GPUD_BANK_EXTRACT 1  // 0: no short-arm channel banks
+#endif
+constexpr int kBankMinChannels = 4;           // smaller classes keep their own form
+constexpr int kBankMaxL = 4;                  // arms of at most four taps (T <= 4D)
+constexpr int kWideTile = 32;                 // outputs per work item of the warp-per-output kernel
 #ifndef GPUD_DENSE_PIPE
 #define GPUD_DENSE_PIPE 2  // most consumer groups of the pipelined dense kernel (0: one-tile-per-CTA kernel only)
 #endif
@@ -250,6 +264,12 @@ struct BlockPlan {
     std::vector<int2> w_gemm;             // (group, 128-output tile from kGemmFirstOutput)
     int gemm_smem = 0, gemm_max_l = 0;
     size_t gemm_b_bytes = 0;              // packed taps of all groups
+    // short-arm channel banks (bank_extract.cu)
+    std::vector<BankGroup> banks;
+    std::vector<int> bmembers;            // SlotBlock rows of the banks' channels
+    std::vector<int2> w_bank;             // (bank, tile * chunks + chunk)
+    int64_t bank_g = 0;                   // float2 entries of the packed modulated taps
+    int bank_max_total = 0;               // largest T x cpad of a bank
     std::vector<int2> w_wide;
     int wide_smem = 0;
     std::vector<int2> w_group, w_gsum;  // (entry, tile*ng + group), (entry, 256-output tile)
@@ -300,9 +320,12 @@ struct Frame {
     int64_t rs_cap = 0;
     double2 *d_part = nullptr;  // phase-group partial sums (double2 slots)
     int64_t part_cap = 0;
+    float2 *d_bank = nullptr;   // packed modulated taps of the short-arm channel banks
+    int64_t bank_cap = 0;
     float *d_gb = nullptr;      // packed taps of the tensor-core channel groups
     size_t gb_cap = 0;
     std::vector<uint64_t> gb_key;  // the groups and member versions d_gb was packed for
+    std::vector<uint64_t> bank_key;  // the banks and member versions d_bank was packed for
     BlockPlan plan;
     std::vector<SlotAfter> after;
     std::vector<int> row_of_slot;
@@ -882,6 +905,68 @@ static std::vector<char> plan_gemm_groups(gpud_runner *r, BlockPlan &pl) {
     return grouped;
 }
 
+// Short-arm channel banks of a block: channels of the warp-per-output or the
+// modulated short-arm form (T <= 4D), not float64-summed, that share the
+// decimation, tap count and phase count, and are not in a tensor-core group,
+// form a bank when there are at least kBankMinChannels of them.  A bank takes
+// every output from jt0 on: the first output whose window lies inside the
+// block; the warp-per-output kernel keeps the outputs before it (they reach
+// into the carried history).  A bank's work items hold 8r outputs, r = 4
+// unless the bank then gives fewer than two items per SM.  Returns the first
+// banked output of every row (-1: not banked).
+static std::vector<int> plan_bank_groups(gpud_runner *r, BlockPlan &pl, const std::vector<char> &grouped) {
+    pl.banks.clear();
+    pl.bmembers.clear();
+    pl.w_bank.clear();
+    pl.bank_g = 0;
+    pl.bank_max_total = 0;
+    std::vector<int> first(pl.sbs.size(), -1);
+    if (!GPUD_BANK_EXTRACT || !r->channel_groups) return first;
+    std::map<std::tuple<int, int, int>, std::vector<int>> by_key;
+    for (int i = 0; i < (int)pl.sbs.size(); ++i) {
+        const SlotBlock &sb = pl.sbs[(size_t)i];
+        const Slot &s = r->slots[(size_t)sb.slot];
+        if (grouped[(size_t)i] || (s.ext_kind != 1 && s.ext_kind != 3) || precise_sum(s.spec) || s.L > kBankMaxL)
+            continue;
+        by_key[std::make_tuple(s.D, s.T, sb.pc)].push_back(i);
+    }
+    for (auto &kv : by_key) {
+        const std::vector<int> &rows = kv.second;
+        if ((int)rows.size() < kBankMinChannels) continue;
+        const int D = std::get<0>(kv.first), T = std::get<1>(kv.first), pc = std::get<2>(kv.first);
+        const int s0 = D - pc - 1;
+        // first output j with s0 + j*D - (T-1) >= 0, rounded up to a wide tile
+        const int jb = T - 1 > s0 ? (T - 1 - s0 + D - 1) / D : 0;
+        const int n_out = pl.sbs[(size_t)rows[0]].n_out;
+        if (n_out <= jb) continue;
+        BankGroup b{};
+        b.nmem = (int)rows.size();
+        b.cpad = (b.nmem + bank_lanes() - 1) / bank_lanes() * bank_lanes();
+        b.D = D;
+        b.T = T;
+        b.pc = pc;
+        b.n_out = n_out;
+        b.jt0 = jb;
+        b.mem_off = (int)pl.bmembers.size();
+        b.g_off = (int)pl.bank_g;
+        const int nch = b.cpad / bank_lanes();
+        b.r = 4;
+        while (b.r > 1 && (int64_t)(n_out - jb + 8 * b.r - 1) / (8 * b.r) * nch < 2 * r->num_sms) b.r >>= 1;
+        pl.bank_g += ((int64_t)T * b.cpad + 63) & ~63;
+        pl.bank_max_total = std::max(pl.bank_max_total, T * b.cpad);
+        const int bi = (int)pl.banks.size();
+        for (int row : rows) {
+            pl.bmembers.push_back(row);
+            first[(size_t)row] = jb;
+        }
+        const int tile = bank_warps() * b.r;
+        for (int t = 0; jb + t * tile < n_out; ++t)
+            for (int c = 0; c < nch; ++c) pl.w_bank.push_back(make_int2(bi, t * nch + c));
+        pl.banks.push_back(b);
+    }
+    return first;
+}
+
 static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     int64_t ext = 0;
     pl.tot_emit_ext = 0;
@@ -960,10 +1045,18 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.batch_stereo = false;
     pl.rds_smem = 0;
     std::vector<char> grouped = plan_gemm_groups(r, pl);
+    const std::vector<int> banked = plan_bank_groups(r, pl, grouped);
     for (int i = 0; i < (int)pl.sbs.size(); ++i) {
         const SlotBlock &sb = pl.sbs[(size_t)i];
         Slot &s = r->slots[(size_t)sb.slot];
-        if (sb.n_out > 0) {
+        if (sb.n_out > 0 && banked[(size_t)i] >= 0) {
+            // a banked channel keeps only the outputs before its bank's first one here
+            pl.sbs[(size_t)i].wide_end = std::max(1, banked[(size_t)i]);
+            if (banked[(size_t)i] > 0) {
+                for (int t = 0; t * kWideTile < banked[(size_t)i]; ++t) pl.w_wide.push_back(make_int2(i, t));
+                pl.wide_smem = std::max(pl.wide_smem, wide_smem_bytes_host(s.T));
+            }
+        } else if (sb.n_out > 0) {
             if (s.ext_kind == 0) {
                 // a grouped channel keeps only the outputs before kGemmFirstOutput here
                 const int n_dense = grouped[(size_t)i] ? kGemmFirstOutput : sb.n_out;
@@ -984,7 +1077,7 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
                     for (int t = 0; t * 256 < sb.n_out; ++t) pl.w_gsum.push_back(make_int2(i, t));
                 }
             } else {
-                for (int t = 0; t * 32 < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));
+                for (int t = 0; t * kWideTile < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));
                 pl.wide_smem = std::max(pl.wide_smem, wide_smem_bytes_host(s.T));
             }
         }
@@ -1055,10 +1148,19 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
           pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() + pl.w_gsum.size() +
-          pl.w_mod.size() + pl.w_free.size() + pl.w_gemm.size();
+          pl.w_mod.size() + pl.w_free.size() + pl.w_gemm.size() + pl.w_bank.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) +
-                   align256(pl.groups.size() * sizeof(GemmGroup)) + align256(pl.gmembers.size() * 4) + 4096;
+                   align256(pl.groups.size() * sizeof(GemmGroup)) + align256(pl.gmembers.size() * 4) +
+                   align256(pl.banks.size() * sizeof(BankGroup)) + align256(pl.bmembers.size() * 4) + 4096;
+    if (pl.bank_g > f.bank_cap) {
+        cudaFree(f.d_bank);
+        f.d_bank = nullptr;
+        int64_t cap = pl.bank_g * 5 / 4 + 1024;
+        CK(dalloc(&f.d_bank, (size_t)cap));
+        f.bank_cap = cap;
+        f.bank_key.clear();  // a new buffer holds no packed taps
+    }
     if (pl.gemm_b_bytes > f.gb_cap) {
         cudaFree(f.d_gb);
         f.d_gb = nullptr;
@@ -1161,7 +1263,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
            o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec),
            o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod), o_free = put(pl.w_free),
-           o_gemm = put(pl.w_gemm);
+           o_gemm = put(pl.w_gemm), o_bank = put(pl.w_bank);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
     size_t o_aud = o_pll + align256(pl.pll_list.size() * 4);
@@ -1170,7 +1272,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     std::memcpy(hd + o_ggr, pl.groups.data(), pl.groups.size() * sizeof(GemmGroup));
     size_t o_gmem = o_ggr + align256(pl.groups.size() * sizeof(GemmGroup));
     std::memcpy(hd + o_gmem, pl.gmembers.data(), pl.gmembers.size() * 4);
-    size_t dbytes = o_gmem + pl.gmembers.size() * 4;
+    size_t o_bgr = o_gmem + align256(pl.gmembers.size() * 4);
+    std::memcpy(hd + o_bgr, pl.banks.data(), pl.banks.size() * sizeof(BankGroup));
+    size_t o_bmem = o_bgr + align256(pl.banks.size() * sizeof(BankGroup));
+    std::memcpy(hd + o_bmem, pl.bmembers.data(), pl.bmembers.size() * 4);
+    size_t dbytes = o_bmem + pl.bmembers.size() * 4;
     CK(cudaMemcpyAsync(f.d_desc, hd, dbytes, cudaMemcpyHostToDevice, f.s));
     f.h2d += dbytes;
     const SlotBlock *d_sb = (const SlotBlock *)(f.d_desc + o_sb);
@@ -1179,6 +1285,8 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     const int *d_aud_list = (const int *)(f.d_desc + o_aud);
     const GemmGroup *d_groups = (const GemmGroup *)(f.d_desc + o_ggr);
     const int *d_gmem = (const int *)(f.d_desc + o_gmem);
+    const BankGroup *d_banks = (const BankGroup *)(f.d_desc + o_bgr);
+    const int *d_bmem = (const int *)(f.d_desc + o_bmem);
 
     // output arena: results | PCM | RDS | audio (host part, then device part) | IQ (emitted part first)
     f.off_res = 0;
@@ -1251,6 +1359,31 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         prof_mark(r, f, "extract_gemm");
         CK(launch_extract_gemm((int)pl.w_gemm.size(), pl.gemm_smem, f.s, d_w + o_gemm, d_groups, d_gmem, d_sb,
                                r->d_prm, r->d_st, x_dev, n, f.d_gb, d_ext, r->d_fault));
+        nl++;
+    }
+    if (!pl.w_bank.empty()) {
+        // the packed modulated taps depend on the bank layout and on each
+        // member's taps and NCO increment: repack only when one changed
+        std::vector<uint64_t> key;
+        key.reserve(pl.banks.size() * 3 + pl.bmembers.size());
+        for (const BankGroup &b : pl.banks) {
+            key.push_back(((uint64_t)(uint32_t)b.nmem << 32) | (uint32_t)b.cpad);
+            key.push_back(((uint64_t)(uint32_t)b.T << 32) | (uint32_t)b.g_off);
+        }
+        for (int row : pl.bmembers) {
+            const int slot = pl.sbs[(size_t)row].slot;
+            key.push_back(((uint64_t)(uint32_t)slot << 40) ^ r->slots[(size_t)slot].pver);
+        }
+        if (key != f.bank_key) {
+            prof_mark(r, f, "bank_pack");
+            CK(launch_bank_pack((int)pl.banks.size(), pl.bank_max_total, f.s, d_banks, d_bmem, d_sb, r->d_prm,
+                                r->d_taps, f.d_bank));
+            f.bank_key = std::move(key);
+            nl++;
+        }
+        prof_mark(r, f, "extract_bank");
+        CK(launch_extract_bank((int)pl.w_bank.size(), f.s, d_w + o_bank, d_banks, d_bmem, d_sb, r->d_prm, r->d_st,
+                               x_dev, f.d_bank, d_ext));
         nl++;
     }
     if (!pl.w_group.empty()) {
@@ -1490,11 +1623,16 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
         one.n = n;
         int slot = full.sbs[k].slot;
         Slot &s = r->slots[(size_t)slot];
+        plan_slot(r, one, slot, n);
+        finish_plan(r, one);
+        // a channel alone can need buffers the whole set does not (it takes
+        // no bank, so e.g. its phase-group partial sums): size the frame for
+        // this plan too (the previous channel's work has completed)
+        rc = ensure_frame(r, f, one);
+        if (rc) return rc;
         const float2 *x = nullptr;
         rc = stage_input(r, f, iq, n, on_device, &x);  // the reference copies the whole block per signal
         if (rc) return rc;
-        plan_slot(r, one, slot, n);
-        finish_plan(r, one);
         rc = enqueue_block(r, f, nullptr, one, x, n);
         if (rc) return rc;
         CK(cudaStreamSynchronize(f.s));
@@ -1632,6 +1770,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_rs);
         cudaFree(f.d_part);
         cudaFree(f.d_gb);
+        cudaFree(f.d_bank);
         if (f.h_desc) cudaFreeHost(f.h_desc);
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);

@@ -687,7 +687,9 @@ k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const int j0 = w.y * kWideOT;
-    if (j0 >= sb.n_out) return;
+    // a banked channel: only the outputs before its bank's first one
+    const int n_end = sb.wide_end > 0 ? min(sb.wide_end, sb.n_out) : sb.n_out;
+    if (j0 >= n_end) return;
     const ChanParams &cp = prm[sb.slot];
     const int T = cp.ntaps, D = cp.decim;
     const uint64_t u0 = st[sb.slot].nco_q;
@@ -706,8 +708,8 @@ k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
     const int H = sb.hist_len;
     const int jw = j0 + warp * kWideOPW;
-    if (jw >= sb.n_out) return;
-    const int no = min(kWideOPW, sb.n_out - jw);
+    if (jw >= n_end) return;
+    const int no = min(kWideOPW, n_end - jw);
     float ar[kWideOPW], ai[kWideOPW], br[kWideOPW], bi[kWideOPW];
 #pragma unroll
     for (int o = 0; o < kWideOPW; ++o) ar[o] = ai[o] = br[o] = bi[o] = 0.f;

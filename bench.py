@@ -292,6 +292,33 @@ def gemm_grouped(chans, n_in=BLOCK):
     return grouped, tensor_flop
 
 
+def bank_grouped(chans, n_in=BLOCK, grouped=()):
+    """Channels the runner extracts as short-arm channel banks (host
+    plan_bank_groups): warp-per-output or modulated-form channels with at
+    most four taps per arm, not float64-summed, not in a tensor-core group,
+    in (taps, decimation) classes of at least 4 (the workloads admit every
+    channel together, so they share the phase count).  Returns {index: first
+    banked output}."""
+    classes = {}
+    for i, c in enumerate(chans):
+        T, D = c["T"], c["D"]
+        fm = c["kind"] in ("NFM", "WFM")
+        precise = fm and c.get("bw") is not None and c["out_rate"] >= 4 * max(c["bw"], 400.0)
+        form = c.get("form") or extraction_form(T, D)
+        if i in grouped or form not in ("extract_wide", "extract_mod") or precise or -(-T // D) > 4:
+            continue
+        classes.setdefault((T, D), []).append(i)
+    out = {}
+    for (T, D), idx in classes.items():
+        if len(idx) < 4:
+            continue
+        s0 = D - 1  # phase count 0 at the first block; every block here is a multiple of D or close to it
+        jb = -(-(T - 1 - s0) // D) if T - 1 > s0 else 0
+        if n_in // D > jb:
+            out.update({i: jb for i in idx})
+    return out
+
+
 def algorithmic_work(chans, n_in=BLOCK):
     """Algorithmic work per block, summed over channels: extraction
     4*T*n_out + min(6*n_in, 4*T*n_out) flop (complex x real taps, plus the
@@ -307,6 +334,7 @@ def algorithmic_work(chans, n_in=BLOCK):
     forms = {}  # the same extraction work split by the kernel that does it
     per_out = {"WFM": 6, "NFM": 6, "AM": 5, "USB": 3, "LSB": 3, "CW": 1}
     grouped, tensor_flop = gemm_grouped(chans, n_in)
+    banked = bank_grouped(chans, n_in, grouped)
     bmin = 8 * n_in  # the wideband block, read once for all channels
     for i, c in enumerate(chans):
         T, D = c["T"], c["D"]
@@ -324,6 +352,15 @@ def algorithmic_work(chans, n_in=BLOCK):
             fw = forms.setdefault("extract_gemm", {"flop": 0, "bytes": 8 * n_in, "tensor_flop": tensor_flop})
             fw["flop"] += f - f0
             fw["bytes"] += b - 8 * 256
+        elif i in banked:
+            # outputs before the bank's first tile (the carried history) on the warp-per-output kernel
+            f0 = f * banked[i] / n_out
+            fw = forms.setdefault("extract_wide", {"flop": 0, "bytes": 8 * n_in})
+            fw["flop"] += f0
+            fw["bytes"] += 8 * banked[i]
+            fw = forms.setdefault("extract_bank", {"flop": 0, "bytes": 8 * n_in})
+            fw["flop"] += f - f0
+            fw["bytes"] += b - 8 * banked[i]
         else:
             fw = forms.setdefault(c.get("form") or extraction_form(T, D), {"flop": 0, "bytes": 8 * n_in})
             fw["flop"] += f
@@ -370,6 +407,8 @@ def stage_key(name):
         return "extract_dense"
     if name in ("extract_group", "group_sum"):
         return "extract_group"
+    if name in ("extract_bank", "bank_pack"):
+        return "extract_bank"
     if name.startswith("extract"):
         return name
     if name.startswith("pll"):
