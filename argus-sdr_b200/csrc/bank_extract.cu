@@ -85,6 +85,7 @@ k_extract_bank(const int2 *__restrict__ work, const BankGroup *__restrict__ grou
         const int kn = min(kBankKC, T - kc);
         // windows: output o's samples n_o - kc - kk (inside the block: the
         // bank starts at the first output whose window does)
+#pragma unroll 4
         for (int i = tid; i < J * kBankKC; i += kBankThreads) {
             const int o = i / kBankKC, kk = i - o * kBankKC;
             const int j = j0 + o;
@@ -93,6 +94,7 @@ k_extract_bank(const int2 *__restrict__ work, const BankGroup *__restrict__ grou
             s_x2[i] = v;
         }
         // taps of this chunk's channels (padding channels and taps: zero)
+#pragma unroll 4
         for (int i = tid; i < kBankKC * kBankLanes; i += kBankThreads) {
             const int kk = i / kBankLanes, c = i - kk * kBankLanes;
             const float2 v = kk < kn ? gtab[b.g_off + (kc + kk) * b.cpad + c0 + c] : make_float2(0.f, 0.f);
@@ -101,6 +103,7 @@ k_extract_bank(const int2 *__restrict__ work, const BankGroup *__restrict__ grou
         __syncthreads();
         const float4 *xw = s_x + (warp * R) * (kBankKC / 2);
         const int nq = (kn + 1) >> 1;
+#pragma unroll 4
         for (int q = 0; q < nq; ++q) {
             const float4 g = s_g[q * kBankLanes + lane];
 #pragma unroll
