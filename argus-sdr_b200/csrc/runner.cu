@@ -85,9 +85,11 @@ cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const Sl
 cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                        const ChanParams *prm, const ChanState *st, const WfmTaps *taps, const BinadeTable *tabs,
                        const float *wk, const float2 *rds_dl, float2 *rds_out);
+cudaError_t launch_post_extract(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                                const float2 *x, int n, float2 *hist, DevResult *res);
 cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
-                              const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
-                              float2 *rds_dl, const BinadeTable *tabs, float2 *d1hist, DevResult *res);
+                              const float2 *ext, const float *wk, float *comp_dl, float2 *rds_dl,
+                              const BinadeTable *tabs, float2 *d1hist, DevResult *res);
 cudaError_t launch_decim2(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                           const double *d1taps, const float2 *d1hist, float2 *ext);
 int decim2_tile();
@@ -304,6 +306,7 @@ struct PendingOp {
 struct Frame {
     cudaStream_t s = nullptr;
     cudaEvent_t ev_front = nullptr, ev_back = nullptr, ev_done = nullptr, ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_ext = nullptr;  // the block's extraction state (history, NCO phase) is carried
     cudaStream_t s2 = nullptr;  // side stream: dense classes beside the channel-group kernel
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     char *d_desc = nullptr, *h_desc = nullptr;
@@ -1414,6 +1417,19 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         CK(cudaEventRecord(f.ev_join, f.s2));
         CK(cudaStreamWaitEvent(f.s, f.ev_join, 0));
     }
+    // the extraction state is carried at once, so the next block's extraction
+    // overlaps this block's later front-half stages
+    prof_mark(r, f, "post_extract");
+    CK(launch_post_extract((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_res));
+    nl++;
+    CK(cudaEventRecord(f.ev_ext, f.s));
+    // the later front-half stages carry state across blocks too (bridge
+    // sample, decimator, composite and RDS delay lines): after the previous
+    // block's front half
+    if (prev) {
+        prof_mark(r, f, "wait_prev_front");
+        CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
+    }
     if (!pl.w_dec.empty()) {
         prof_mark(r, f, "decim2");
         CK(launch_decim2((int)pl.w_dec.size(), f.s, d_w + o_wdec, d_sb, r->d_prm, r->d_d1taps, r->d_d1hist, d_ext));
@@ -1442,8 +1458,8 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     }
     if (!pl.sbs.empty()) {
         prof_mark(r, f, "post_front");
-        CK(launch_post_front((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_ext, f.d_wk,
-                             r->d_comp_dl, r->d_rds_dl, r->d_tabs, r->d_d1hist, d_res));
+        CK(launch_post_front((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, d_ext, f.d_wk, r->d_comp_dl,
+                             r->d_rds_dl, r->d_tabs, r->d_d1hist, d_res));
         nl++;
     }
     CK(cudaEventRecord(f.ev_front, f.s));
@@ -1563,10 +1579,11 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
     const float2 *x = nullptr;
     rc = stage_input(r, f, iq, n, on_device, &x);
     if (rc) return rc;
-    // parameter updates and the front half wait for the previous front half
+    // parameter updates and the extraction wait for the previous block's
+    // extraction state (the later stages wait inside enqueue_block)
     if (prev) {
-        prof_mark(r, f, "wait_prev_front");
-        CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
+        prof_mark(r, f, "wait_prev_ext");
+        CK(cudaStreamWaitEvent(f.s, prev->ev_ext, 0));
     }
     rc = apply_pending(r, f);
     if (rc) return rc;
@@ -1574,6 +1591,12 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
         rc = enqueue_block(r, f, prev, pl, x, n);
         if (rc) return rc;
     } else {
+        // no channels: the chains of the block before pass through unchanged
+        if (prev) {
+            CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
+            CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
+        }
+        CK(cudaEventRecord(f.ev_ext, f.s));
         CK(cudaEventRecord(f.ev_front, f.s));
         CK(cudaEventRecord(f.ev_back, f.s));
         f.off_res = f.off_audio = f.off_rds = f.off_ext = f.out_bytes = 0;
@@ -1724,6 +1747,7 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     for (auto &f : r->fr) {
         CKC(cudaStreamCreateWithFlags(&f.s, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_front, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&f.ev_ext, cudaEventDisableTiming));
         CKC(cudaStreamCreateWithFlags(&f.s2, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_fork, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&f.ev_join, cudaEventDisableTiming));
@@ -1775,7 +1799,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);
         if (f.h_in) cudaFreeHost(f.h_in);
-        for (auto e : {f.ev_front, f.ev_back, f.ev_done, f.ev0, f.ev1, f.ev_fork, f.ev_join})
+        for (auto e : {f.ev_front, f.ev_ext, f.ev_back, f.ev_done, f.ev0, f.ev1, f.ev_fork, f.ev_join})
             if (e) cudaEventDestroy(e);
         for (auto e : f.prof_ev) cudaEventDestroy(e);
         if (f.s2) {
@@ -2037,9 +2061,9 @@ GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot) {
 }
 
 // The new taps / parameters are written on the next block's stream once the
-// block before it has passed its front half.  That block's back half may
-// still be reading ChanParams; of what an update changes (NCO increment,
-// taps) the back half reads nothing.
+// block before it has carried its extraction state.  That block's later
+// stages may still be reading ChanParams; of what an update changes (NCO
+// increment, taps, the float64-sum flag) only the extraction reads anything.
 GPUD_API int GPUD_CALL gpud_runner_update(gpud_runner *r, int slot, double offset_hz, double bandwidth) {
     if (!r) return GPUD_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(r->mu);

@@ -1218,6 +1218,7 @@ k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
           const WfmTaps *__restrict__ taps, float *__restrict__ wk, int W, const float *__restrict__ comp_dl) {
     __shared__ float win[padi(kFirOT + kWfmTapsPad) + 8];
     __shared__ float4 tp[kWfmTapsPad];
+    __shared__ float s_out[3 * (kFirOT + kFirOT / 32)];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const ChanParams &cp = prm[sb.slot];
@@ -1251,15 +1252,24 @@ k_wfm_fir(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
             }
         }
     }
-    float *lpr = wk + 1 * W + sb.comp_off, *bpf = wk + 2 * W + sb.comp_off, *pil = wk + 3 * W + sb.comp_off;
+    // outputs through shared memory (index i + i/32: conflict-free both
+    // ways), then coalesced stores of the three arrays
+    constexpr int kS = kFirOT + kFirOT / 32;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-        int q = q0 + 8 * t + r;
-        if (q < sb.n_disc) {
-            lpr[q] = a[r];
-            bpf[q] = b[r];
-            pil[q] = c[r];
-        }
+        const int i = 8 * t + r, j = i + (i >> 5);
+        s_out[j] = a[r];
+        s_out[kS + j] = b[r];
+        s_out[2 * kS + j] = c[r];
+    }
+    __syncthreads();
+    float *lpr = wk + 1 * W + sb.comp_off, *bpf = wk + 2 * W + sb.comp_off, *pil = wk + 3 * W + sb.comp_off;
+    const int nq = min(kFirOT, sb.n_disc - q0);
+    for (int i = t; i < nq; i += kFirThreads) {
+        const int j = i + (i >> 5);
+        lpr[q0 + i] = s_out[j];
+        bpf[q0 + i] = s_out[kS + j];
+        pil[q0 + i] = s_out[2 * kS + j];
     }
 }
 
@@ -1524,8 +1534,14 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
 // thread runs the serial loop over the rest.  No trajectory is stored: a last
 // pass integrates each segment from its converged start and writes the
 // outputs.
+#ifndef GPUD_PLL_CLUSTER
+#define GPUD_PLL_CLUSTER 8  // CTAs per channel at most: segment length max(16, n / (256 * this))
+#endif
+#ifndef GPUD_PLL_JAC_SWEEPS
+#define GPUD_PLL_JAC_SWEEPS 2  // sweeps that evaluate the segment Jacobians before chord steps may start
+#endif
 constexpr int kNewtonThreads = 256;
-constexpr int kNewtonMaxCluster = 8;
+constexpr int kNewtonMaxCluster = GPUD_PLL_CLUSTER;
 constexpr int kNewtonMinSeg = 16;
 
 // Steps per segment (per thread) for a block of n loop steps.
@@ -1713,7 +1729,7 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
         // Close to the solution (the last corrections below 1e-2 rad) the
         // segment Jacobians barely move: they are kept from the last full
         // evaluation (chord steps), which converge as fast as Newton there.
-        const bool jac = it < 2 || prev_m0 > 1e-2f;
+        const bool jac = it < GPUD_PLL_JAC_SWEEPS || prev_m0 > 1e-2f;
         Aff m;
         aff_identity(m);
         SegState x = x0;
@@ -2011,6 +2027,7 @@ k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
           const float *__restrict__ lr_dl, const float *__restrict__ audio_dl, float *__restrict__ audio) {
     __shared__ float win[padi(kFirOT + kWfmTapsPad) + 8];
     __shared__ float tp[kWfmTapsPad];
+    __shared__ float s_out[kFirOT + kFirOT / 32];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const ChanParams &cp = prm[sb.slot];
@@ -2055,32 +2072,31 @@ k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
             for (int r = 0; r < 8; ++r) a[r] = fmaf(h, ring[(r - kk + 8) & 7], a[r]);
         }
     }
-    float *dst = audio + sb.audio_off;
-    if (cp.mode == 2) {
+    // the tile's filter outputs through shared memory (index i + i/32: the
+    // stores of a register row and the reads of consecutive outputs are both
+    // conflict-free), then coalesced reads of L+R and stores of (L, R) pairs
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            int q = q0 + 8 * t + r;
-            if (q < sb.n_disc) dst[q] = a[r];
-        }
+    for (int r = 0; r < 8; ++r) {
+        const int i = 8 * t + r;
+        s_out[i + (i >> 5)] = a[r];
+    }
+    __syncthreads();
+    float *dst = audio + sb.audio_off;
+    const int nq = min(kFirOT, sb.n_disc - q0);
+    if (cp.mode == 2) {
+        for (int i = t; i < nq; i += kFirThreads) dst[q0 + i] = s_out[i + (i >> 5)];
     } else if (stereo) {
         const float *lpr = wk + 1 * W + sb.comp_off;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            int q = q0 + 8 * t + r;
-            if (q < sb.n_disc) {
-                float l = lpr[q];
-                dst[2 * q] = 0.5f * (l + a[r]);
-                dst[2 * q + 1] = 0.5f * (l - a[r]);
-            }
+        float2 *d2 = reinterpret_cast<float2 *>(dst);
+        for (int i = t; i < nq; i += kFirThreads) {
+            const float v = s_out[i + (i >> 5)], l = lpr[q0 + i];
+            d2[q0 + i] = make_float2(0.5f * (l + v), 0.5f * (l - v));
         }
     } else {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            int q = q0 + 8 * t + r;
-            if (q < sb.n_disc) {
-                dst[2 * q] = a[r];
-                dst[2 * q + 1] = a[r];
-            }
+        float2 *d2 = reinterpret_cast<float2 *>(dst);
+        for (int i = t; i < nq; i += kFirThreads) {
+            const float v = s_out[i + (i >> 5)];
+            d2[q0 + i] = make_float2(v, v);
         }
     }
 }
@@ -2198,9 +2214,9 @@ __device__ void shift_delay_line(float *dl, const float *__restrict__ src, int n
 // so the next block's front half can overlap this block's PLL.
 __global__ void __launch_bounds__(128)
 k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
-             const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, const float2 *__restrict__ ext,
-             const float *__restrict__ wk, float *__restrict__ comp_dl, float2 *__restrict__ rds_dl,
-             const BinadeTable *__restrict__ tabs, float2 *__restrict__ d1hist, DevResult *__restrict__ res) {
+             const float2 *__restrict__ ext, const float *__restrict__ wk, float *__restrict__ comp_dl,
+             float2 *__restrict__ rds_dl, const BinadeTable *__restrict__ tabs, float2 *__restrict__ d1hist,
+             DevResult *__restrict__ res) {
     const SlotBlock sb = sbt[blockIdx.x];
     const ChanParams &cp = prm[sb.slot];
     ChanState &s = st[sb.slot];
@@ -2216,20 +2232,6 @@ k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ p
         for (int i = threadIdx.x; i < kWfmHist; i += blockDim.x) dh[i] = dtmp[i];
         __syncthreads();
     }
-    const uint64_t u0 = s.nco_q;
-    // extraction history: last min(T-1, H+n) samples of (history ++ shifted block)
-    {
-        const int keep = cp.ntaps - 1;
-        const int H = sb.hist_len;
-        const int newH = min(keep, H + n);
-        const float2 *hold = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
-        float2 *hnew = hist_arena + cp.hist_off + (1 - sb.hist_sel) * cp.hcap;
-        for (int q = threadIdx.x; q < newH; q += blockDim.x) {
-            int g = H + n - newH + q;
-            hnew[q] = g < H ? hold[g] : cmulf(__ldg(x + (g - H)), q64_phasor(u0 + (uint64_t)(g - H) * cp.inc_q));
-        }
-    }
-    __syncthreads();
     if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
         const float *comp = wk + sb.comp_off;
         // RDS shifted history: the last 100 values of cplx over the stream
@@ -2259,7 +2261,6 @@ k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ p
         shift_delay_line(comp_dl + cp.wfm_idx * kWfmHist, comp, sb.n_disc);
     }
     if (threadIdx.x == 0) {
-        s.nco_q = u0 + (uint64_t)n * cp.inc_q;
         if (sb.n_dem > 0) {
             s.last_iq = ext[sb.dem_off + sb.n_dem - 1];
             s.has_last = 1;
@@ -2268,6 +2269,32 @@ k_post_front(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ p
             s.rds_count += sb.n_disc;
             s.rds_hist_len = (int)min((int64_t)kWfmHist, s.rds_count);
         }
+    }
+}
+
+// Extraction state of a block, carried as soon as the block's extraction
+// kernels are done (the next block's extraction waits only for this): the
+// last min(T-1, H+n) samples of (history ++ shifted block) into the other
+// history buffer, and the NCO phase advanced by the block.
+__global__ void __launch_bounds__(128)
+k_post_extract(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm, ChanState *__restrict__ st,
+               const float2 *__restrict__ x, int n, float2 *__restrict__ hist_arena, DevResult *__restrict__ res) {
+    const SlotBlock sb = sbt[blockIdx.x];
+    const ChanParams &cp = prm[sb.slot];
+    ChanState &s = st[sb.slot];
+    const uint64_t u0 = s.nco_q;
+    const int keep = cp.ntaps - 1;
+    const int H = sb.hist_len;
+    const int newH = min(keep, H + n);
+    const float2 *hold = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
+    float2 *hnew = hist_arena + cp.hist_off + (1 - sb.hist_sel) * cp.hcap;
+    for (int q = threadIdx.x; q < newH; q += blockDim.x) {
+        int g = H + n - newH + q;
+        hnew[q] = g < H ? hold[g] : cmulf(__ldg(x + (g - H)), q64_phasor(u0 + (uint64_t)(g - H) * cp.inc_q));
+    }
+    __syncthreads();  // every thread has read the block-start phase
+    if (threadIdx.x == 0) {
+        s.nco_q = u0 + (uint64_t)n * cp.inc_q;
         res[sb.res_idx].nco_phase = q64_to_rad(s.nco_q);
     }
 }
@@ -2754,9 +2781,9 @@ cudaError_t launch_decim2(int grid, cudaStream_t sm, const int2 *work, const Slo
 int decim2_tile() { return kDecOT; }
 
 cudaError_t launch_post_front(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
-                              const float2 *x, int n, float2 *hist, const float2 *ext, const float *wk, float *comp_dl,
-                              float2 *rds_dl, const BinadeTable *tabs, float2 *d1hist, DevResult *res) {
-    k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, ext, wk, comp_dl, rds_dl, tabs, d1hist, res);
+                              const float2 *ext, const float *wk, float *comp_dl, float2 *rds_dl,
+                              const BinadeTable *tabs, float2 *d1hist, DevResult *res) {
+    k_post_front<<<grid, 128, 0, sm>>>(sbt, prm, st, ext, wk, comp_dl, rds_dl, tabs, d1hist, res);
     return cudaGetLastError();
 }
 
@@ -2773,6 +2800,12 @@ cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *
 }
 
 int audio48_tile() { return kAudOT; }
+
+cudaError_t launch_post_extract(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
+                                const float2 *x, int n, float2 *hist, DevResult *res) {
+    k_post_extract<<<grid, 128, 0, sm>>>(sbt, prm, st, x, n, hist, res);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_post_back(int grid, cudaStream_t sm, const SlotBlock *sbt, const ChanParams *prm, ChanState *st,
                              const float *wk, int W, float *lr_dl, float *audio_dl, DevResult *res) {
