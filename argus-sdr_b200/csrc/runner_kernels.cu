@@ -2351,7 +2351,7 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
 constexpr int kAudThreads = 256;
 constexpr int kAudOT = 256;  // resampled frames per CTA in k_audio48_rs
 
-constexpr int kAudWin = 4096;     // staged input frames per channel and CTA
+constexpr int kAudWin = 2048;     // staged input frames per channel and CTA (256 outputs at M/L <= 7.8)
 constexpr int kAudBank = 4096;    // staged bank coefficients (doubles)
 
 __global__ void __launch_bounds__(kAudThreads)
@@ -2368,9 +2368,8 @@ k_audio48_rs(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, c
     const RsBank &bk = banks[cp.rs_bank];
     const int C = cp.aud_ch, L = bk.L, M = bk.M, K = bk.K;
     const float *in = audio + sb.audio_off;
-    const int o = oa + (int)threadIdx.x;
     if (L == M) {
-        if (o < ob)
+        for (int o = oa + (int)threadIdx.x; o < ob; o += kAudThreads)
             for (int c = 0; c < C; ++c) rs_out[sb.pcm_off + o * C + c] = in[o * C + c];
         return;
     }
@@ -2417,38 +2416,40 @@ k_audio48_rs(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, c
         }
         __syncthreads();
     }
-    if (o >= ob) return;
-    const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
-    const int64_t cc = T / L;  // T >= 0
-    const int ph = (int)(T - cc * L);
-    double acc0 = 0.0, acc1 = 0.0;
-    if (staged) {
-        const double *arm = s_bank + ph * K;
-        const float *x0 = s_in + (cc - 1 - lo), *x1 = s_in + kAudWin + (cc - 1 - lo);
-        for (int k = 0; k < K; ++k) {
-            const double h = arm[k];
-            acc0 = __dadd_rn(acc0, __dmul_rn((double)x0[-k], h));
-            if (C == 2) acc1 = __dadd_rn(acc1, __dmul_rn((double)x1[-k], h));
-        }
-    } else {
-        const double *arm = bk.arm + ph * K;
-        for (int k = 0; k < K; ++k) {
-            const int64_t i = cc - 1 - k;
-            const double h = arm[k];
-            const float v0 = i >= 0 ? in[i * C] : as.dl[0][-1 - i];
-            acc0 = __dadd_rn(acc0, __dmul_rn((double)v0, h));
-            if (C == 2) {
-                const float v1 = i >= 0 ? in[i * 2 + 1] : as.dl[1][-1 - i];
-                acc1 = __dadd_rn(acc1, __dmul_rn((double)v1, h));
+    for (int o = oa + (int)threadIdx.x; o < ob; o += kAudThreads) {
+        const int64_t T = (int64_t)sb.rs_t0 + (int64_t)o * M;
+        const int64_t cc = T / L;  // T >= 0
+        const int ph = (int)(T - cc * L);
+        double acc0 = 0.0, acc1 = 0.0;
+        if (staged) {
+            const double *arm = s_bank + ph * K;
+            const float *x0 = s_in + (cc - 1 - lo), *x1 = s_in + kAudWin + (cc - 1 - lo);
+            for (int k = 0; k < K; ++k) {
+                const double h = arm[k];
+                acc0 = __dadd_rn(acc0, __dmul_rn((double)x0[-k], h));
+                if (C == 2) acc1 = __dadd_rn(acc1, __dmul_rn((double)x1[-k], h));
+            }
+        } else {
+            const double *arm = bk.arm + ph * K;
+            for (int k = 0; k < K; ++k) {
+                const int64_t i = cc - 1 - k;
+                const double h = arm[k];
+                const float v0 = i >= 0 ? in[i * C] : as.dl[0][-1 - i];
+                acc0 = __dadd_rn(acc0, __dmul_rn((double)v0, h));
+                if (C == 2) {
+                    const float v1 = i >= 0 ? in[i * 2 + 1] : as.dl[1][-1 - i];
+                    acc1 = __dadd_rn(acc1, __dmul_rn((double)v1, h));
+                }
             }
         }
+        float *dst = rs_out + sb.pcm_off + o * C;
+        dst[0] = (float)acc0;
+        if (C == 2) dst[1] = (float)acc1;
     }
-    float *dst = rs_out + sb.pcm_off + o * C;
-    dst[0] = (float)acc0;
-    if (C == 2) dst[1] = (float)acc1;
 }
 
 constexpr int kAudOutThreads = 1024;  // one CTA per channel: short serial runs
+constexpr int kAudOutStage = 16384;   // resampled samples of a channel staged in shared memory (64 KB)
 
 __global__ void __launch_bounds__(kAudOutThreads)
 k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
@@ -2456,6 +2457,7 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
               const float *__restrict__ rs_out, int16_t *__restrict__ pcm) {
     constexpr int kWarps = kAudOutThreads / 32;
     __shared__ double s_wa[kWarps], s_wb[2][kWarps];  // warp totals, then exclusive warp prefixes
+    extern __shared__ float s_rs[];  // the channel's resampled block (when it fits), then its output samples
     const SlotBlock sb = sbt[list[blockIdx.x]];
     const ChanParams &cp = prm[sb.slot];
     AudState &as = aud[sb.slot];
@@ -2463,7 +2465,15 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
     const int n = sb.rs_frames, nout = sb.rs_nout;
     if (n <= 0) return;
     const RsBank &bk = banks[cp.rs_bank];
-    const float *r = rs_out + sb.pcm_off;
+    // each thread takes a run of consecutive frames: the block is staged with
+    // coalesced loads and the PCM written back coalesced
+    const bool staged = nout * C <= kAudOutStage;
+    if (staged) {
+        const float *src = rs_out + sb.pcm_off;
+        for (int i = threadIdx.x; i < nout * C; i += kAudOutThreads) s_rs[i] = src[i];
+        __syncthreads();
+    }
+    const float *r = staged ? s_rs : rs_out + sb.pcm_off;
     const int per = (nout + kAudOutThreads - 1) / kAudOutThreads;
     const int o0 = min(nout, (int)threadIdx.x * per), o1 = min(nout, o0 + per);
     const bool wfm = cp.mode == 2 || cp.mode == 3;
@@ -2541,12 +2551,27 @@ k_audio48_out(const int *__restrict__ list, const SlotBlock *__restrict__ sbt, c
                 s = (float)y;
             }
             if (wfm) s = s * 0.35f;
-            if (cp.flags & kChPcmF32) {
+            if (staged) {
+                s_rs[o * C + c] = s;  // this thread's own cell, already read
+            } else if (cp.flags & kChPcmF32) {
                 reinterpret_cast<float *>(pcm + sb.pcm_off)[o * C + c] = s;
             } else {
                 float v = s * 32767.0f;
                 v = fminf(fmaxf(v, -32768.0f), 32767.0f);
                 pcm[sb.pcm_off + o * C + c] = (int16_t)v;
+            }
+        }
+    }
+    if (staged) {
+        __syncthreads();
+        if (cp.flags & kChPcmF32) {
+            float *dst = reinterpret_cast<float *>(pcm + sb.pcm_off);
+            for (int i = threadIdx.x; i < nout * C; i += kAudOutThreads) dst[i] = s_rs[i];
+        } else {
+            for (int i = threadIdx.x; i < nout * C; i += kAudOutThreads) {
+                float v = s_rs[i] * 32767.0f;
+                v = fminf(fmaxf(v, -32768.0f), 32767.0f);
+                pcm[sb.pcm_off + i] = (int16_t)v;
             }
         }
     }
@@ -2795,7 +2820,10 @@ cudaError_t launch_audio48(int grid_rs, int count, cudaStream_t sm, const int2 *
     cudaError_t e = smem_optin_once(optin, (const void *)k_audio48_rs, smem);
     if (e != cudaSuccess) return e;
     if (grid_rs > 0) k_audio48_rs<<<grid_rs, kAudThreads, smem, sm>>>(work, sbt, prm, banks, aud, audio, rs_buf);
-    k_audio48_out<<<count, kAudOutThreads, 0, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
+    static std::atomic<uint64_t> optin_out{0};
+    e = smem_optin_once(optin_out, (const void *)k_audio48_out, kAudOutStage * 4);
+    if (e != cudaSuccess) return e;
+    k_audio48_out<<<count, kAudOutThreads, kAudOutStage * 4, sm>>>(list, sbt, prm, banks, aud, audio, rs_buf, pcm);
     return cudaGetLastError();
 }
 
