@@ -152,6 +152,7 @@ constexpr int kPllMaxIters = 64;
 #define GPUD_FRAMES 3
 #endif
 constexpr int kFrames = GPUD_FRAMES;  // blocks in flight
+constexpr int kInRing = kFrames + 1;  // input ring slots: one more than frames, so a copy can start before a frame is free
 constexpr int kMaxRsClasses = 16;  // 48 kHz resampler banks (one per demod rate)
 
 // ---------------------------------------------------------------------------
@@ -307,6 +308,8 @@ struct Frame {
     cudaStream_t s = nullptr;
     cudaEvent_t ev_front = nullptr, ev_back = nullptr, ev_done = nullptr, ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_ext = nullptr;  // the block's extraction state (history, NCO phase) is carried
+    int ring = -1;                 // input ring slot the block reads (-1: device input or the frame's own buffer)
+    cudaEvent_t ev_start = nullptr;  // where the block's latency starts (ev0, or its ring copy's start)
     cudaStream_t s2 = nullptr;  // side stream: dense classes beside the channel-group kernel
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     char *d_desc = nullptr, *h_desc = nullptr;
@@ -340,7 +343,20 @@ struct Frame {
     std::vector<cudaEvent_t> prof_ev;
     std::vector<std::string> prof_names;
     int prof_n = 0;
+    // the block's launch sequence, captured from the frame's streams and
+    // replayed as one graph (updated in place while its shape holds)
+    cudaGraphExec_t gexec = nullptr;
+    bool capturing = false;
 };
+
+// Events that order one frame's work against another frame's, or against the
+// copy stream: inside a capture they become the graph's external event nodes.
+static cudaError_t record_x(const Frame &f, cudaEvent_t e, cudaStream_t s) {
+    return f.capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
+}
+static cudaError_t wait_x(const Frame &f, cudaStream_t s, cudaEvent_t e) {
+    return cudaStreamWaitEvent(s, e, f.capturing ? cudaEventWaitExternal : 0);
+}
 
 }  // namespace gpud
 
@@ -352,6 +368,14 @@ struct gpud_runner {
     int schedule = GPUD_SCHED_BATCHED;
     cudaStream_t stream = nullptr;  // joins every block: work recorded here follows all submitted blocks
     cudaStream_t admin = nullptr;   // admission copies into slots no block in flight uses
+    // input ring: a block from pinned host memory is copied into the next
+    // slot on its own stream as soon as it is submitted, before the submit
+    // waits for a free frame; a slot is refilled once the block that read it
+    // has carried its extraction state (every reader of the input is done)
+    cudaStream_t in_s = nullptr;
+    float2 *d_ring[kInRing] = {};
+    cudaEvent_t ring_t0[kInRing] = {}, ring_copied[kInRing] = {}, ring_free[kInRing] = {};
+    int ring_next = 0;
     std::string err;
     std::recursive_mutex mu;
 
@@ -379,6 +403,7 @@ struct gpud_runner {
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
     bool channel_groups = true;  // tensor-core channel groups (gpud_runner_set_channel_groups)
+    bool graphs = true;          // per-block launch sequences replayed as graphs (gpud_runner_set_graphs)
     // fault word the pipelined extraction kernel writes when a bounded wait
     // gives up (page-locked, mapped into the device)
     unsigned *h_fault = nullptr, *d_fault = nullptr;
@@ -392,7 +417,7 @@ struct gpud_runner {
     // stats
     uint64_t blocks = 0, launches = 0;
     uint64_t pver_seq = 0;  // source of Slot::pver
-    int graph_rebuilds = 0;
+    int graph_rebuilds = 0;  // instantiations of the frames' executable graphs
     std::vector<float> lat_ms;
     size_t lat_pos = 0;
     double last_ms = 0;
@@ -447,6 +472,14 @@ static void prof_collect(gpud_runner *r, Frame &f) {
         cudaEventElapsedTime(&ms, f.prof_ev[(size_t)i], f.prof_ev[(size_t)i + 1]);
         gpud_stage_time t{};
         std::snprintf(t.name, sizeof t.name, "%s", f.prof_names[(size_t)i].c_str());
+        t.ms = ms;
+        r->stage_times.push_back(t);
+    }
+    if (f.ring >= 0) {  // the block's copy into the input ring, on the copy stream
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r->ring_t0[f.ring], r->ring_copied[f.ring]);
+        gpud_stage_time t{};
+        std::snprintf(t.name, sizeof t.name, "%s", "h2d_ring");
         t.ms = ms;
         r->stage_times.push_back(t);
     }
@@ -716,7 +749,7 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 // ---------------------------------------------------------------------------
 static void record_latency(gpud_runner *r, Frame &f) {
     float ms = 0;
-    cudaEventElapsedTime(&ms, f.ev0, f.ev1);
+    cudaEventElapsedTime(&ms, f.ev_start ? f.ev_start : f.ev0, f.ev1);
     r->last_ms = ms;
     r->lat_ms[r->lat_pos % r->lat_ms.size()] = ms;
     r->lat_pos++;
@@ -1117,7 +1150,6 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         int64_t cap = std::max<int64_t>(W * 5 / 4, 1 << 16);
         CK(dalloc(&f.d_wk, (size_t)cap * 5));
         f.wk_cap = cap;
-        r->graph_rebuilds++;
     }
     if (pl.tot_part > f.part_cap) {
         cudaFree(f.d_part);
@@ -1145,7 +1177,6 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         CK(cudaMalloc((void **)&f.d_out, cap));
         CK(cudaMallocHost((void **)&f.h_out, cap));
         f.out_cap = cap;
-        r->graph_rebuilds++;
     }
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
@@ -1422,13 +1453,14 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     prof_mark(r, f, "post_extract");
     CK(launch_post_extract((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_res));
     nl++;
-    CK(cudaEventRecord(f.ev_ext, f.s));
+    CK(record_x(f, f.ev_ext, f.s));
+    if (f.ring >= 0) CK(record_x(f, r->ring_free[f.ring], f.s));  // the input ring slot may be refilled
     // the later front-half stages carry state across blocks too (bridge
     // sample, decimator, composite and RDS delay lines): after the previous
     // block's front half
     if (prev) {
         prof_mark(r, f, "wait_prev_front");
-        CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
+        CK(wait_x(f, f.s, prev->ev_front));
     }
     if (!pl.w_dec.empty()) {
         prof_mark(r, f, "decim2");
@@ -1462,11 +1494,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                              r->d_rds_dl, r->d_tabs, r->d_d1hist, d_res));
         nl++;
     }
-    CK(cudaEventRecord(f.ev_front, f.s));
+    CK(record_x(f, f.ev_front, f.s));
     // ---- back half: after the previous block's back half ----
     if (prev) {
         prof_mark(r, f, "wait_prev_back");
-        CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
+        CK(wait_x(f, f.s, prev->ev_back));
     }
     if (!pl.w_free.empty()) {
         prof_mark(r, f, "free_stereo");
@@ -1512,7 +1544,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                             d_res));
         nl++;
     }
-    CK(cudaEventRecord(f.ev_back, f.s));
+    CK(record_x(f, f.ev_back, f.s));
     prof_mark(r, f, "d2h");
     r->launches += (uint64_t)nl;
     gpud_count_launch(nl);
@@ -1555,7 +1587,45 @@ static void build_rows(gpud_runner *r, Frame &f) {
     for (size_t i = 0; i < f.plan.sbs.size(); ++i) f.row_of_slot[(size_t)f.plan.sbs[i].slot] = (int)i;
 }
 
+// Replays a captured block on the frame's stream: the frame's executable graph
+// takes the new block's parameters in place when the launch sequence kept its
+// shape, and is instantiated again when it did not.
+static int launch_block_graph(gpud_runner *r, Frame &f, cudaGraph_t g) {
+    if (f.gexec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(f.gexec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(f.gexec);
+            f.gexec = nullptr;
+        }
+    }
+    if (!f.gexec) {
+        CK(cudaGraphInstantiate(&f.gexec, g, 0));
+        r->graph_rebuilds++;
+    }
+    CK(cudaGraphLaunch(f.gexec, f.s));
+    return 0;
+}
+
+static bool host_pinned(const void *p) {
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return pinned;
+}
+
 static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_device) {
+    // a block in pinned host memory starts its copy into the input ring now,
+    // before this submit waits for a free frame
+    int ring = -1;
+    if (!on_device && n > 0 && iq && host_pinned(iq)) {
+        ring = r->ring_next;
+        r->ring_next = (ring + 1) % kInRing;
+        CK(cudaStreamWaitEvent(r->in_s, r->ring_free[ring], 0));  // its previous block's readers are done
+        CK(cudaEventRecord(r->ring_t0[ring], r->in_s));
+        CK(cudaMemcpyAsync(r->d_ring[ring], iq, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, r->in_s));
+        CK(cudaEventRecord(r->ring_copied[ring], r->in_s));
+    }
     const int fi = r->nxt;
     Frame &f = r->fr[fi];
     if (f.inflight) {
@@ -1577,8 +1647,16 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
     CK(cudaEventRecord(f.ev0, f.s));
     prof_mark(r, f, "h2d");
     const float2 *x = nullptr;
-    rc = stage_input(r, f, iq, n, on_device, &x);
-    if (rc) return rc;
+    f.ring = ring;
+    f.ev_start = ring >= 0 ? r->ring_t0[ring] : f.ev0;
+    if (ring >= 0) {
+        CK(cudaStreamWaitEvent(f.s, r->ring_copied[ring], 0));
+        f.h2d += (uint64_t)n * sizeof(float2);
+        x = r->d_ring[ring];
+    } else {
+        rc = stage_input(r, f, iq, n, on_device, &x);
+        if (rc) return rc;
+    }
     // parameter updates and the extraction wait for the previous block's
     // extraction state (the later stages wait inside enqueue_block)
     if (prev) {
@@ -1588,7 +1666,23 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
     rc = apply_pending(r, f);
     if (rc) return rc;
     if (!pl.sbs.empty()) {
+        // the block's launches go to the device as one graph: a single
+        // submission instead of one per kernel, copy and event, whose fetches
+        // would otherwise queue behind the input copies on the host link
+        const bool graph = r->graphs && !r->profiling;
+        if (graph) {
+            CK(cudaStreamBeginCapture(f.s, cudaStreamCaptureModeRelaxed));
+            f.capturing = true;
+        }
         rc = enqueue_block(r, f, prev, pl, x, n);
+        if (graph) {
+            f.capturing = false;
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(f.s, &g);
+            if (!rc && ce != cudaSuccess) rc = set_err(r, GPUD_E_CUDA, "block capture", ce);
+            if (!rc) rc = launch_block_graph(r, f, g);
+            if (g) cudaGraphDestroy(g);
+        }
         if (rc) return rc;
     } else {
         // no channels: the chains of the block before pass through unchanged
@@ -1597,6 +1691,7 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
             CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
         }
         CK(cudaEventRecord(f.ev_ext, f.s));
+        if (f.ring >= 0) CK(cudaEventRecord(r->ring_free[f.ring], f.s));
         CK(cudaEventRecord(f.ev_front, f.s));
         CK(cudaEventRecord(f.ev_back, f.s));
         f.off_res = f.off_audio = f.off_rds = f.off_ext = f.out_bytes = 0;
@@ -1631,6 +1726,8 @@ static int run_plain(gpud_runner *r, const gpud_float2 *iq, int n, int on_device
     if (rc) return rc;
     f.h2d = f.d2h = 0;
     f.prof_n = 0;
+    f.ring = -1;  // the plain schedule copies the block per signal, not through the input ring
+    f.ev_start = f.ev0;
     std::vector<char> gathered;
     // the batched arena layout: results | PCM | RDS | audio | IQ
     size_t res_b = align256(full.sbs.size() * sizeof(DevResult));
@@ -1758,6 +1855,13 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
         CKC(dalloc(&f.d_block, (size_t)max_block));
         CKC(cudaMallocHost((void **)&f.h_in, (size_t)max_block * sizeof(float2)));
     }
+    CKC(cudaStreamCreateWithFlags(&r->in_s, cudaStreamNonBlocking));
+    for (int i = 0; i < kInRing; ++i) {
+        CKC(dalloc(&r->d_ring[i], (size_t)max_block));
+        CKC(cudaEventCreate(&r->ring_t0[i]));
+        CKC(cudaEventCreate(&r->ring_copied[i]));
+        CKC(cudaEventCreateWithFlags(&r->ring_free[i], cudaEventDisableTiming));
+    }
     size_t M = (size_t)max_channels;
     CKC(dalloc(&r->d_prm, M));
     CKC(dalloc(&r->d_st, M));
@@ -1774,7 +1878,7 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
     CKC(dalloc(&r->d_d1hist, M * kWfmHist));
     CKC(dalloc(&r->d_banks, (size_t)kMaxRsClasses));
 #undef CKC
-    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 8 * kFrames + sizeof(RsBank) * kMaxRsClasses;
+    r->used = slot_state_bytes(r) * M + (uint64_t)max_block * 8 * (kFrames + kInRing) + sizeof(RsBank) * kMaxRsClasses;
     *out = r;
     return 0;
 }
@@ -1786,7 +1890,17 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
     }
     if (r->stream) cudaStreamSynchronize(r->stream);
     if (r->admin) cudaStreamSynchronize(r->admin);
+    if (r->in_s) {
+        cudaStreamSynchronize(r->in_s);
+        cudaStreamDestroy(r->in_s);
+    }
+    for (int i = 0; i < kInRing; ++i) {
+        cudaFree(r->d_ring[i]);
+        for (auto e : {r->ring_t0[i], r->ring_copied[i], r->ring_free[i]})
+            if (e) cudaEventDestroy(e);
+    }
     for (auto &f : r->fr) {
+        if (f.gexec) cudaGraphExecDestroy(f.gexec);
         cudaFree(f.d_desc);
         cudaFree(f.d_out);
         cudaFree(f.d_wk);
@@ -2624,6 +2738,13 @@ GPUD_API int GPUD_CALL gpud_runner_set_channel_groups(gpud_runner *r, int enable
     if (!r) return GPUD_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(r->mu);
     r->channel_groups = enable != 0;
+    return 0;
+}
+
+GPUD_API int GPUD_CALL gpud_runner_set_graphs(gpud_runner *r, int enable) {
+    if (!r) return GPUD_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(r->mu);
+    r->graphs = enable != 0;
     return 0;
 }
 
