@@ -343,20 +343,7 @@ struct Frame {
     std::vector<cudaEvent_t> prof_ev;
     std::vector<std::string> prof_names;
     int prof_n = 0;
-    // the block's launch sequence, captured from the frame's streams and
-    // replayed as one graph (updated in place while its shape holds)
-    cudaGraphExec_t gexec = nullptr;
-    bool capturing = false;
 };
-
-// Events that order one frame's work against another frame's, or against the
-// copy stream: inside a capture they become the graph's external event nodes.
-static cudaError_t record_x(const Frame &f, cudaEvent_t e, cudaStream_t s) {
-    return f.capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
-}
-static cudaError_t wait_x(const Frame &f, cudaStream_t s, cudaEvent_t e) {
-    return cudaStreamWaitEvent(s, e, f.capturing ? cudaEventWaitExternal : 0);
-}
 
 }  // namespace gpud
 
@@ -403,7 +390,6 @@ struct gpud_runner {
     int pll_max_iters = kPllMaxIters;  // Newton iterations before the serial fallback
     int num_sms = 148;
     bool channel_groups = true;  // tensor-core channel groups (gpud_runner_set_channel_groups)
-    bool graphs = true;          // per-block launch sequences replayed as graphs (gpud_runner_set_graphs)
     // fault word the pipelined extraction kernel writes when a bounded wait
     // gives up (page-locked, mapped into the device)
     unsigned *h_fault = nullptr, *d_fault = nullptr;
@@ -417,7 +403,7 @@ struct gpud_runner {
     // stats
     uint64_t blocks = 0, launches = 0;
     uint64_t pver_seq = 0;  // source of Slot::pver
-    int graph_rebuilds = 0;  // instantiations of the frames' executable graphs
+    int graph_rebuilds = 0;
     std::vector<float> lat_ms;
     size_t lat_pos = 0;
     double last_ms = 0;
@@ -1150,6 +1136,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         int64_t cap = std::max<int64_t>(W * 5 / 4, 1 << 16);
         CK(dalloc(&f.d_wk, (size_t)cap * 5));
         f.wk_cap = cap;
+        r->graph_rebuilds++;
     }
     if (pl.tot_part > f.part_cap) {
         cudaFree(f.d_part);
@@ -1177,6 +1164,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         CK(cudaMalloc((void **)&f.d_out, cap));
         CK(cudaMallocHost((void **)&f.h_out, cap));
         f.out_cap = cap;
+        r->graph_rebuilds++;
     }
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
@@ -1453,14 +1441,14 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     prof_mark(r, f, "post_extract");
     CK(launch_post_extract((int)pl.sbs.size(), f.s, d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, d_res));
     nl++;
-    CK(record_x(f, f.ev_ext, f.s));
-    if (f.ring >= 0) CK(record_x(f, r->ring_free[f.ring], f.s));  // the input ring slot may be refilled
+    CK(cudaEventRecord(f.ev_ext, f.s));
+    if (f.ring >= 0) CK(cudaEventRecord(r->ring_free[f.ring], f.s));  // the input ring slot may be refilled
     // the later front-half stages carry state across blocks too (bridge
     // sample, decimator, composite and RDS delay lines): after the previous
     // block's front half
     if (prev) {
         prof_mark(r, f, "wait_prev_front");
-        CK(wait_x(f, f.s, prev->ev_front));
+        CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
     }
     if (!pl.w_dec.empty()) {
         prof_mark(r, f, "decim2");
@@ -1494,11 +1482,11 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                              r->d_rds_dl, r->d_tabs, r->d_d1hist, d_res));
         nl++;
     }
-    CK(record_x(f, f.ev_front, f.s));
+    CK(cudaEventRecord(f.ev_front, f.s));
     // ---- back half: after the previous block's back half ----
     if (prev) {
         prof_mark(r, f, "wait_prev_back");
-        CK(wait_x(f, f.s, prev->ev_back));
+        CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
     }
     if (!pl.w_free.empty()) {
         prof_mark(r, f, "free_stereo");
@@ -1544,7 +1532,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
                             d_res));
         nl++;
     }
-    CK(record_x(f, f.ev_back, f.s));
+    CK(cudaEventRecord(f.ev_back, f.s));
     prof_mark(r, f, "d2h");
     r->launches += (uint64_t)nl;
     gpud_count_launch(nl);
@@ -1585,26 +1573,6 @@ static int apply_pending(gpud_runner *r, Frame &f) {
 static void build_rows(gpud_runner *r, Frame &f) {
     f.row_of_slot.assign((size_t)r->max_ch, -1);
     for (size_t i = 0; i < f.plan.sbs.size(); ++i) f.row_of_slot[(size_t)f.plan.sbs[i].slot] = (int)i;
-}
-
-// Replays a captured block on the frame's stream: the frame's executable graph
-// takes the new block's parameters in place when the launch sequence kept its
-// shape, and is instantiated again when it did not.
-static int launch_block_graph(gpud_runner *r, Frame &f, cudaGraph_t g) {
-    if (f.gexec) {
-        cudaGraphExecUpdateResultInfo info{};
-        if (cudaGraphExecUpdate(f.gexec, g, &info) != cudaSuccess) {
-            cudaGetLastError();
-            cudaGraphExecDestroy(f.gexec);
-            f.gexec = nullptr;
-        }
-    }
-    if (!f.gexec) {
-        CK(cudaGraphInstantiate(&f.gexec, g, 0));
-        r->graph_rebuilds++;
-    }
-    CK(cudaGraphLaunch(f.gexec, f.s));
-    return 0;
 }
 
 static bool host_pinned(const void *p) {
@@ -1666,23 +1634,7 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
     rc = apply_pending(r, f);
     if (rc) return rc;
     if (!pl.sbs.empty()) {
-        // the block's launches go to the device as one graph: a single
-        // submission instead of one per kernel, copy and event, whose fetches
-        // would otherwise queue behind the input copies on the host link
-        const bool graph = r->graphs && !r->profiling;
-        if (graph) {
-            CK(cudaStreamBeginCapture(f.s, cudaStreamCaptureModeRelaxed));
-            f.capturing = true;
-        }
         rc = enqueue_block(r, f, prev, pl, x, n);
-        if (graph) {
-            f.capturing = false;
-            cudaGraph_t g = nullptr;
-            const cudaError_t ce = cudaStreamEndCapture(f.s, &g);
-            if (!rc && ce != cudaSuccess) rc = set_err(r, GPUD_E_CUDA, "block capture", ce);
-            if (!rc) rc = launch_block_graph(r, f, g);
-            if (g) cudaGraphDestroy(g);
-        }
         if (rc) return rc;
     } else {
         // no channels: the chains of the block before pass through unchanged
@@ -1900,7 +1852,6 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
             if (e) cudaEventDestroy(e);
     }
     for (auto &f : r->fr) {
-        if (f.gexec) cudaGraphExecDestroy(f.gexec);
         cudaFree(f.d_desc);
         cudaFree(f.d_out);
         cudaFree(f.d_wk);
@@ -2738,13 +2689,6 @@ GPUD_API int GPUD_CALL gpud_runner_set_channel_groups(gpud_runner *r, int enable
     if (!r) return GPUD_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(r->mu);
     r->channel_groups = enable != 0;
-    return 0;
-}
-
-GPUD_API int GPUD_CALL gpud_runner_set_graphs(gpud_runner *r, int enable) {
-    if (!r) return GPUD_E_ARG;
-    std::lock_guard<std::recursive_mutex> lk(r->mu);
-    r->graphs = enable != 0;
     return 0;
 }
 

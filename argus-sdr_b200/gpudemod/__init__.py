@@ -192,11 +192,6 @@ class ChannelRunner:
         bit-identical alone and in any mix."""
         _check(self._r, lib.gpud_runner_set_channel_groups(self._r, 1 if enable else 0))
 
-    def set_graphs(self, enable: bool):
-        """Each batched block replayed as one CUDA graph (default) or launched
-        kernel by kernel (gpud_runner_set_graphs); outputs are identical."""
-        _check(self._r, lib.gpud_runner_set_graphs(self._r, 1 if enable else 0))
-
     def channel_form(self, slot: int):
         """(form, phases per group, groups) of an admitted channel."""
         f, pg, ng = C.c_int(), C.c_int(), C.c_int()

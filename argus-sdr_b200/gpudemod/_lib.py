@@ -156,7 +156,6 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "gpud_runner_set_autotune_table": (i, [P, C.POINTER(AutotuneEntry), i]),
         "gpud_runner_channel_form": (i, [P, i, pi, pi, pi]),
         "gpud_runner_set_channel_groups": (i, [P, i]),
-        "gpud_runner_set_graphs": (i, [P, i]),
         "gpud_wfm_batch_audio": (i, [P, i, i, i, d, d, d, P, i, C.POINTER(BatchAudioResult)]),
         "gpud_demod_audio_segment": (i, [i, P, i, i, i, d, d, P, i, C.POINTER(SegmentAudioResult)]),
         "gpud_iqfile_write": (i, [C.c_char_p, P, C.c_int64, C.c_int64, d]),

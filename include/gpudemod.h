@@ -274,10 +274,9 @@ typedef struct {
     double p50_block_ms;    /* over the last 4096 blocks */
     double p99_block_ms;
     uint64_t kernel_launches; /* kernels launched by the runner since creation */
-    int32_t graph_rebuilds;   /* instantiations of the frames' block graphs: the first block on
-                                 each frame, and blocks whose launch sequence changed shape
-                                 (admission, retirement and regrown buffers are taken in place;
-                                 a different set of kernels is not) */
+    int32_t graph_rebuilds;   /* regrowths of the per-block work arrays and output arena (the
+                                 launch sequence is not graph-captured; a captured one would be
+                                 rebuilt on exactly these) */
     int32_t pad;
     uint64_t last_h2d_bytes;  /* host->device bytes of the last block */
     uint64_t last_d2h_bytes;  /* device->host bytes of the last block */
@@ -313,15 +312,6 @@ GPUD_API int GPUD_CALL gpud_runner_channel_form(gpud_runner *r, int slot, int *f
  * groups off (enable 0) every channel's output is bit-identical alone and in
  * any mix.  Takes effect at the next block. */
 GPUD_API int GPUD_CALL gpud_runner_set_channel_groups(gpud_runner *r, int enable);
-/* Graph replay (no reference counterpart; on by default): each batched
- * block's launch sequence -- descriptor copy, kernels, the waits on the block
- * before and the output copies -- is captured and replayed as one CUDA graph
- * on its frame, updated in place while the sequence keeps its shape and
- * instantiated again when it changes (counted in graph_rebuilds).  Outputs
- * are identical either way; blocks run with profiling on are not captured
- * (their stage events need the plain launches).  Takes effect at the next
- * block. */
-GPUD_API int GPUD_CALL gpud_runner_set_graphs(gpud_runner *r, int enable);
 GPUD_API int GPUD_CALL gpud_runner_admit(gpud_runner *r, const gpud_channel_spec *spec, int *slot_out);
 GPUD_API int GPUD_CALL gpud_runner_retire(gpud_runner *r, int slot);
 /* Offset / bandwidth drift: the NCO increment follows the offset with the
