@@ -159,11 +159,10 @@ struct SlotBlock {
     int32_t dem_off;   // float2 offset of the demod input in the IQ region
     int32_t n_dem;     // demod input samples this block
     int32_t d1_phase;  // pre-demod decimator phase before the block
-    // phase-grouped extraction: ng groups of pg phases; partial sums at
-    // part_off (float2) when ng > 1
+    // phase-grouped extraction: ng groups of pg phases (one CTA per tile adds them)
     int32_t ng;
     int32_t pg;
-    int32_t part_off;
+    int32_t pad_pg;
     int32_t wide_end;  // > 0: the warp-per-output kernel computes only outputs before it (the rest: a bank)
 };
 

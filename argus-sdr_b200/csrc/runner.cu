@@ -109,12 +109,10 @@ int group_smem_bytes_host(int Pc, int L);
 int mod_smem_bytes_host(int Pc, int L);
 cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
-                                 const float2 *hist, const float *taps, float2 *ext, void *part);
+                                 const float2 *hist, const float *taps, float2 *ext);
 cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                const ChanParams *prm, const ChanState *st, const float2 *x, int n,
-                               const float2 *hist, const float *taps, float2 *ext, void *part);
-cudaError_t launch_group_sum(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
-                             const ChanParams *prm, const void *part, float2 *ext);
+                               const float2 *hist, const float *taps, float2 *ext);
 
 constexpr int kWfmTapsPadH = 104;
 struct WfmTapsHost {
@@ -275,11 +273,10 @@ struct BlockPlan {
     int bank_max_total = 0;               // largest T x cpad of a bank
     std::vector<int2> w_wide;
     int wide_smem = 0;
-    std::vector<int2> w_group, w_gsum;  // (entry, tile*ng + group), (entry, 256-output tile)
+    std::vector<int2> w_group;  // (entry, 256-output tile): one CTA takes the tile's phase groups in turn
     int group_smem = 0;
-    std::vector<int2> w_mod;            // (entry, tile*ng + group) of the modulated short-arm form
+    std::vector<int2> w_mod;    // (entry, 256-output tile) of the modulated short-arm form, likewise
     int mod_smem = 0;
-    int64_t tot_part = 0;               // double2 slots of partial sums of multi-group channels
     std::vector<int2> w_demod, w_am, w_fir, w_out, w_rds;
     int rds_smem = 0;
     std::vector<int> pll_list;
@@ -324,8 +321,6 @@ struct Frame {
     float2 *h_in = nullptr;
     float *d_rs = nullptr;  // resampled 48 kHz audio before de-emphasis
     int64_t rs_cap = 0;
-    double2 *d_part = nullptr;  // phase-group partial sums (double2 slots)
-    int64_t part_cap = 0;
     float2 *d_bank = nullptr;   // packed modulated taps of the short-arm channel banks
     int64_t bank_cap = 0;
     float *d_gb = nullptr;      // packed taps of the tensor-core channel groups
@@ -363,6 +358,8 @@ struct gpud_runner {
     float2 *d_ring[kInRing] = {};
     cudaEvent_t ring_t0[kInRing] = {}, ring_copied[kInRing] = {}, ring_free[kInRing] = {};
     int ring_next = 0;
+    double ring_ms = 0;       // device time of the ring copies since the last stats reset
+    uint64_t ring_copies = 0;
     std::string err;
     std::recursive_mutex mu;
 
@@ -762,6 +759,14 @@ static int finish_frame(gpud_runner *r, int fi, int timeout_ms) {
     if (f.ticket > r->completed) r->completed = f.ticket;
     r->done_frame = fi;
     record_latency(r, f);
+    if (f.ring >= 0) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, r->ring_t0[f.ring], r->ring_copied[f.ring]) == cudaSuccess) {
+            r->ring_ms += ms;
+            r->ring_copies++;
+        }
+        cudaGetLastError();
+    }
     prof_collect(r, f);
     if (r->h_fault && *(volatile unsigned *)r->h_fault != 0) {
         const unsigned code = *(volatile unsigned *)r->h_fault;
@@ -1052,11 +1057,9 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
     pl.w_wide.clear();
     pl.wide_smem = 0;
     pl.w_group.clear();
-    pl.w_gsum.clear();
     pl.group_smem = 0;
     pl.w_mod.clear();
     pl.mod_smem = 0;
-    pl.tot_part = 0;
     pl.w_demod.clear();
     pl.w_am.clear();
     pl.w_fir.clear();
@@ -1087,17 +1090,11 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
                 pl.dense_pmax[s.L] = std::max(pl.dense_pmax[s.L], s.P);
             } else if (s.ext_kind == 2 || s.ext_kind == 3) {
                 auto &wl = s.ext_kind == 2 ? pl.w_group : pl.w_mod;
-                for (int t = 0; t * dense_tile() < sb.n_out; ++t)
-                    for (int g = 0; g < s.ng; ++g) wl.push_back(make_int2(i, t * s.ng + g));
+                for (int t = 0; t * dense_tile() < sb.n_out; ++t) wl.push_back(make_int2(i, t));
                 if (s.ext_kind == 2)
                     pl.group_smem = std::max(pl.group_smem, group_smem_bytes_host(s.pg, s.L));
                 else
                     pl.mod_smem = std::max(pl.mod_smem, mod_smem_bytes_host(s.pg, s.L));
-                if (s.ng > 1) {
-                    pl.sbs[(size_t)i].part_off = (int)pl.tot_part;
-                    pl.tot_part += ((int64_t)s.ng * sb.n_out + 31) & ~31;
-                    for (int t = 0; t * 256 < sb.n_out; ++t) pl.w_gsum.push_back(make_int2(i, t));
-                }
             } else {
                 for (int t = 0; t * kWideTile < sb.n_out; ++t) pl.w_wide.push_back(make_int2(i, t));
                 pl.wide_smem = std::max(pl.wide_smem, wide_smem_bytes_host(s.T));
@@ -1126,6 +1123,16 @@ static void finish_plan(gpud_runner *r, BlockPlan &pl) {
             pl.rds_smem = std::max(pl.rds_smem, rds_smem_bytes(std::max(1, demod_rate(s) / 19000)));
         }
     }
+    // a phase-grouped tile costs its channel's phases x arm length: the
+    // longest go first, so that the short ones fill in behind them
+    auto longest_first = [&](std::vector<int2> &wl) {
+        std::stable_sort(wl.begin(), wl.end(), [&](int2 a, int2 b) {
+            const Slot &sa = r->slots[(size_t)pl.sbs[(size_t)a.x].slot], &sb = r->slots[(size_t)pl.sbs[(size_t)b.x].slot];
+            return (int64_t)sa.P * sa.L > (int64_t)sb.P * sb.L;
+        });
+    };
+    longest_first(pl.w_group);
+    longest_first(pl.w_mod);
 }
 
 static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
@@ -1137,13 +1144,6 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
         CK(dalloc(&f.d_wk, (size_t)cap * 5));
         f.wk_cap = cap;
         r->graph_rebuilds++;
-    }
-    if (pl.tot_part > f.part_cap) {
-        cudaFree(f.d_part);
-        f.d_part = nullptr;
-        int64_t cap = std::max<int64_t>(pl.tot_part * 5 / 4, 1 << 16);
-        CK(dalloc(&f.d_part, (size_t)cap));
-        f.part_cap = cap;
     }
     if (pl.tot_pcm > f.rs_cap) {
         cudaFree(f.d_rs);
@@ -1169,7 +1169,7 @@ static int ensure_frame(gpud_runner *r, Frame &f, const BlockPlan &pl) {
     size_t nw = 0;
     for (int L = 0; L <= kDenseMaxL; ++L) nw += pl.w_dense[L].size();
     nw += pl.w_wide.size() + pl.w_demod.size() + pl.w_am.size() + pl.w_fir.size() + pl.w_out.size() +
-          pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() + pl.w_gsum.size() +
+          pl.w_rds.size() + pl.w_aud.size() + pl.w_dec.size() + pl.w_group.size() +
           pl.w_mod.size() + pl.w_free.size() + pl.w_gemm.size() + pl.w_bank.size();
     size_t dneed = align256(pl.sbs.size() * sizeof(SlotBlock)) + align256(nw * sizeof(int2)) +
                    align256(pl.pll_list.size() * 4) + align256(pl.aud_list.size() * 4) +
@@ -1284,7 +1284,7 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     };
     size_t o_wide = put(pl.w_wide), o_dem = put(pl.w_demod), o_am = put(pl.w_am), o_fir = put(pl.w_fir),
            o_out = put(pl.w_out), o_rds = put(pl.w_rds), o_waud = put(pl.w_aud), o_wdec = put(pl.w_dec),
-           o_grp = put(pl.w_group), o_gsum = put(pl.w_gsum), o_mod = put(pl.w_mod), o_free = put(pl.w_free),
+           o_grp = put(pl.w_group), o_mod = put(pl.w_mod), o_free = put(pl.w_free),
            o_gemm = put(pl.w_gemm), o_bank = put(pl.w_bank);
     size_t o_pll = o_w + align256(cnt * sizeof(int2));
     std::memcpy(hd + o_pll, pl.pll_list.data(), pl.pll_list.size() * 4);
@@ -1411,18 +1411,13 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     if (!pl.w_group.empty()) {
         prof_mark(r, f, "extract_group");
         CK(launch_extract_group((int)pl.w_group.size(), pl.group_smem, f.s, d_w + o_grp, d_sb, r->d_prm, r->d_st,
-                                x_dev, n, r->d_hist, r->d_taps, d_ext, f.d_part));
+                                x_dev, n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_mod.empty()) {
         prof_mark(r, f, "extract_mod");
         CK(launch_extract_mod((int)pl.w_mod.size(), pl.mod_smem, f.s, d_w + o_mod, d_sb, r->d_prm, r->d_st, x_dev,
-                              n, r->d_hist, r->d_taps, d_ext, f.d_part));
-        nl++;
-    }
-    if (!pl.w_gsum.empty()) {
-        prof_mark(r, f, "group_sum");
-        CK(launch_group_sum((int)pl.w_gsum.size(), f.s, d_w + o_gsum, d_sb, r->d_prm, f.d_part, d_ext));
+                              n, r->d_hist, r->d_taps, d_ext));
         nl++;
     }
     if (!pl.w_wide.empty()) {
@@ -1857,7 +1852,6 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         cudaFree(f.d_wk);
         cudaFree(f.d_block);
         cudaFree(f.d_rs);
-        cudaFree(f.d_part);
         cudaFree(f.d_gb);
         cudaFree(f.d_bank);
         if (f.h_desc) cudaFreeHost(f.h_desc);
@@ -2282,6 +2276,8 @@ GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *
     }
     out->kernel_launches = r->launches;
     out->graph_rebuilds = r->graph_rebuilds;
+    out->ring_copy_ms = r->ring_ms;
+    out->ring_copies = r->ring_copies;
     if (r->done_frame >= 0) {
         out->last_h2d_bytes = r->fr[r->done_frame].h2d;
         out->last_d2h_bytes = r->fr[r->done_frame].d2h;
@@ -2293,6 +2289,8 @@ GPUD_API int GPUD_CALL gpud_runner_reset_stats(gpud_runner *r) {
     if (!r) return GPUD_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(r->mu);
     r->lat_pos = 0;
+    r->ring_ms = 0;
+    r->ring_copies = 0;
     return 0;
 }
 

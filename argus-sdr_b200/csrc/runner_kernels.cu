@@ -764,9 +764,10 @@ k_extract_wide(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
 //     Z[pp][m] = s(s0 + (m_base + m)*D - (p_lo + pp)),
 // -- for each column m a contiguous run of Pc samples -- and computes the
 // group's share of the 256 outputs with the same warp/lane layout as the dense
-// form.  With one group the sums go to the extraction output; with several,
-// each group writes its partial sums and k_group_sum adds them in group order
-// (deterministic: the grouping depends on the channel only).
+// form.  One CTA takes all groups of its tile in turn, restaging shared memory
+// per group, and each thread adds its output's group shares in group order in
+// a register (deterministic: the grouping depends on the channel only), so no
+// partial sums leave the SM.
 // The rotation of sample cb(m) + r is A[m] * B[r], A[m] = exp(j phi(cb(m))),
 // B[r] = exp(j r inc), both exact from the Q0.64 phase.
 // ===========================================================================
@@ -860,24 +861,21 @@ __device__ __forceinline__ void group_stage(const GroupTile &gt, const SlotBlock
     __syncthreads();
 }
 
+static_assert(kDenseOT == kDenseThreads, "the phase-group kernels keep one output per thread");
+
 __global__ void __launch_bounds__(kDenseThreads, 2)
 k_extract_group(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
                 const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
                 const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
-                float2 *__restrict__ ext, void *__restrict__ part) {
+                float2 *__restrict__ ext) {
     extern __shared__ float4 smemg4[];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const ChanParams &cp = prm[sb.slot];
-    const int ng = sb.ng;
-    const int tile = w.y / ng;
     GroupTile gt;
-    gt.g = w.y - tile * ng;
-    gt.j0 = tile * kDenseOT;
+    gt.j0 = w.y * kDenseOT;
     if (gt.j0 >= sb.n_out) return;
     const int L = cp.plen;
-    gt.p_lo = gt.g * sb.pg;
-    gt.Pc = min(sb.pg, cp.nphase - gt.p_lo);
     gt.Le = group_Le(L);
     gt.M = kDenseOT + gt.Le - 1;
     gt.Mp = dense_row_stride(gt.Le);
@@ -888,7 +886,7 @@ k_extract_group(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
     float *tsm = reinterpret_cast<float *>(reinterpret_cast<char *>(smemg4) + zb);
     void *tabs = tsm + ((sb.pg * gt.Le + 3) & ~3);
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
-    group_stage(gt, sb, cp, st[sb.slot].nco_q, x, n, hist, taps_arena + cp.taps_off, Z, tsm, tabs);
+    const uint64_t u0 = st[sb.slot].nco_q;
 
     auto row = [&](int pp, int lane, float *ar, float *ai) {
         const float2 *zrow = Z + pp * gt.Mp;
@@ -903,23 +901,29 @@ k_extract_group(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
         }
     };
     const int nv = sb.n_out - gt.j0;
-    // one group: the extraction output; several: this group's partial sums
-    // (double2 slots from part_off; float2 view for non-precise channels)
-    const int64_t pbase = (int64_t)sb.part_off * 2 + (int64_t)gt.g * sb.n_out + gt.j0;
-    if (cp.precise_sum) {
-        double2 *p64 = reinterpret_cast<double2 *>(part) + (int64_t)sb.part_off + (int64_t)gt.g * sb.n_out + gt.j0;
-        float2 *e = ext + sb.ext_off + gt.j0;
-        tile_sum<true>(gt.Pc, row, Z, [&](int o, double2 v) {
-            if (o >= nv) return;
-            if (ng == 1) e[o] = make_float2((float)v.x, (float)v.y);
-            else p64[o] = v;
-        });
-    } else {
-        float2 *dst = ng == 1 ? ext + sb.ext_off + gt.j0 : reinterpret_cast<float2 *>(part) + pbase;
-        tile_sum<false>(gt.Pc, row, Z, [&](int o, float2 v) {
-            if (o < nv) dst[o] = v;
-        });
+    const int o = (int)threadIdx.x;  // this thread's output of the tile
+    double2 acc64 = make_double2(0.0, 0.0);
+    float2 acc = make_float2(0.f, 0.f);
+    for (int g = 0; g < sb.ng; ++g) {
+        gt.g = g;
+        gt.p_lo = g * sb.pg;
+        gt.Pc = min(sb.pg, cp.nphase - gt.p_lo);
+        if (g) __syncthreads();  // the last group's reduction has read Z
+        group_stage(gt, sb, cp, u0, x, n, hist, taps_arena + cp.taps_off, Z, tsm, tabs);
+        if (cp.precise_sum) {
+            tile_sum<true>(gt.Pc, row, Z, [&](int, double2 v) {
+                acc64.x += v.x;
+                acc64.y += v.y;
+            });
+        } else {
+            tile_sum<false>(gt.Pc, row, Z, [&](int, float2 v) {
+                acc.x += v.x;
+                acc.y += v.y;
+            });
+        }
     }
+    if (o < nv)
+        ext[sb.ext_off + gt.j0 + o] = cp.precise_sum ? make_float2((float)acc64.x, (float)acc64.y) : acc;
 }
 
 // Short arms (L <= 4) in phase groups with the NCO folded into the taps: with
@@ -965,19 +969,14 @@ __global__ void __launch_bounds__(kDenseThreads, 3)
 k_extract_mod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
               const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
               const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
-              float2 *__restrict__ ext, void *__restrict__ part) {
+              float2 *__restrict__ ext) {
     extern __shared__ float4 smemm4[];
     const int2 w = work[blockIdx.x];
     const SlotBlock sb = sbt[w.x];
     const ChanParams &cp = prm[sb.slot];
-    const int ng = sb.ng;
-    const int tile = w.y / ng;
-    const int g = w.y - tile * ng;
-    const int j0 = tile * kDenseOT;
+    const int j0 = w.y * kDenseOT;
     if (j0 >= sb.n_out) return;
     const int L = cp.plen, D = cp.decim;
-    const int p_lo = g * sb.pg;
-    const int Pc = min(sb.pg, cp.nphase - p_lo);
     const int M = kDenseOT + L - 1;
     const int Mp = dense_row_stride(L);
     int zb = (sb.pg * Mp * 8 + 15) & ~15;
@@ -987,32 +986,9 @@ k_extract_mod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, 
     const uint64_t u0 = st[sb.slot].nco_q;
     const uint64_t inc = cp.inc_q;
     const float *tg = taps_arena + cp.taps_off;
-    for (int i = threadIdx.x; i < Pc * L; i += kDenseThreads) {
-        const int pp = i / L, u = i - pp * L;
-        const int k = p_lo + pp + u * D;
-        const float h = tg[(p_lo + pp) * L + u];
-        const float2 ph = q64_phasor((uint64_t)0 - (uint64_t)k * inc);
-        hc[i] = make_float2(h * ph.x, h * ph.y);
-    }
-    // raw samples: Z[pp][m] = x(cb0 + m*D + r), pp = Pc-1-r
     const int s0 = D - sb.pc - 1;
-    const int cb0 = s0 + (j0 - (L - 1)) * D - p_lo - Pc + 1;
     const float2 *hist = hist_arena + cp.hist_off + sb.hist_sel * cp.hcap;
     const int H = sb.hist_len;
-    const bool interior = cb0 >= 0 && cb0 + (M - 1) * D + Pc <= n;
-    if (interior) {
-        stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) { return __ldg(x + i); });
-    } else {
-        stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) {
-            if (i >= n) return make_float2(0.f, 0.f);
-            if (i >= 0) return __ldg(x + i);
-            const int hi = H + i;
-            // a carried sample is shifted already: undo its rotation
-            return hi >= 0 ? cmulf(hist[hi], q64_phasor((uint64_t)0 - (u0 + (uint64_t)(int64_t)i * inc)))
-                           : make_float2(0.f, 0.f);
-        });
-    }
-    __syncthreads();
     auto row = [&](int pp, int lane, float *ar, float *ai) {
         const float2 *zrow = Z + pp * Mp;
         const float2 *hrow = hc + pp * L;
@@ -1024,55 +1000,52 @@ k_extract_mod(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, 
         }
     };
     const int nv = sb.n_out - j0;
-    auto phase_out = [&](int o) { return q64_phasor(u0 + (uint64_t)(int64_t)(s0 + (j0 + o) * D) * inc); };
-    if (cp.precise_sum) {
-        double2 *p64 = reinterpret_cast<double2 *>(part) + (int64_t)sb.part_off + (int64_t)g * sb.n_out + j0;
-        float2 *e = ext + sb.ext_off + j0;
-        tile_sum<true>(Pc, row, Z, [&](int o, double2 v) {
-            if (o >= nv) return;
-            const float2 ph = phase_out(o);
-            const double yr = v.x * (double)ph.x - v.y * (double)ph.y;
-            const double yi = v.x * (double)ph.y + v.y * (double)ph.x;
-            if (ng == 1) e[o] = make_float2((float)yr, (float)yi);
-            else p64[o] = make_double2(yr, yi);
-        });
-    } else {
-        float2 *dst = ng == 1 ? ext + sb.ext_off + j0
-                              : reinterpret_cast<float2 *>(part) + (int64_t)sb.part_off * 2 + (int64_t)g * sb.n_out + j0;
-        tile_sum<false>(Pc, row, Z, [&](int o, float2 v) {
-            if (o < nv) dst[o] = cmulf(v, phase_out(o));
-        });
-    }
-}
-
-// Sum of the phase groups' partial outputs, in group order (float64 for
-// precise channels, rounded once).
-__global__ void __launch_bounds__(256)
-k_group_sum(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
-            const void *__restrict__ part, float2 *__restrict__ ext) {
-    const int2 w = work[blockIdx.x];
-    const SlotBlock sb = sbt[w.x];
-    const int j = w.y * 256 + (int)threadIdx.x;
-    if (j >= sb.n_out) return;
-    if (prm[sb.slot].precise_sum) {
-        const double2 *p = reinterpret_cast<const double2 *>(part) + sb.part_off + j;
-        double2 sum = make_double2(0.0, 0.0);
-        for (int g = 0; g < sb.ng; ++g) {
-            const double2 v = p[(int64_t)g * sb.n_out];
-            sum.x += v.x;
-            sum.y += v.y;
+    const int o = (int)threadIdx.x;  // this thread's output of the tile
+    // its rotation exp(j phi(n_j)), taken by every group's share
+    const float2 ph = q64_phasor(u0 + (uint64_t)(int64_t)(s0 + (j0 + o) * D) * inc);
+    double2 acc64 = make_double2(0.0, 0.0);
+    float2 acc = make_float2(0.f, 0.f);
+    for (int g = 0; g < sb.ng; ++g) {
+        const int p_lo = g * sb.pg;
+        const int Pc = min(sb.pg, cp.nphase - p_lo);
+        if (g) __syncthreads();  // the last group's reduction has read Z and its rows hc
+        for (int i = threadIdx.x; i < Pc * L; i += kDenseThreads) {
+            const int pp = i / L, u = i - pp * L;
+            const int k = p_lo + pp + u * D;
+            const float h = tg[(p_lo + pp) * L + u];
+            const float2 t = q64_phasor((uint64_t)0 - (uint64_t)k * inc);
+            hc[i] = make_float2(h * t.x, h * t.y);
         }
-        ext[sb.ext_off + j] = make_float2((float)sum.x, (float)sum.y);
-    } else {
-        const float2 *p = reinterpret_cast<const float2 *>(part) + (int64_t)sb.part_off * 2 + j;
-        float2 sum = make_float2(0.f, 0.f);
-        for (int g = 0; g < sb.ng; ++g) {
-            const float2 v = p[(int64_t)g * sb.n_out];
-            sum.x += v.x;
-            sum.y += v.y;
+        // raw samples: Z[pp][m] = x(cb0 + m*D + r), pp = Pc-1-r
+        const int cb0 = s0 + (j0 - (L - 1)) * D - p_lo - Pc + 1;
+        const bool interior = cb0 >= 0 && cb0 + (M - 1) * D + Pc <= n;
+        if (interior) {
+            stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) { return __ldg(x + i); });
+        } else {
+            stage_columns(Pc, M, Mp, D, cb0, Z, [&](int i, int, int) {
+                if (i >= n) return make_float2(0.f, 0.f);
+                if (i >= 0) return __ldg(x + i);
+                const int hi = H + i;
+                // a carried sample is shifted already: undo its rotation
+                return hi >= 0 ? cmulf(hist[hi], q64_phasor((uint64_t)0 - (u0 + (uint64_t)(int64_t)i * inc)))
+                               : make_float2(0.f, 0.f);
+            });
         }
-        ext[sb.ext_off + j] = sum;
+        __syncthreads();
+        if (cp.precise_sum) {
+            tile_sum<true>(Pc, row, Z, [&](int, double2 v) {
+                acc64.x += v.x * (double)ph.x - v.y * (double)ph.y;
+                acc64.y += v.x * (double)ph.y + v.y * (double)ph.x;
+            });
+        } else {
+            tile_sum<false>(Pc, row, Z, [&](int, float2 v) {
+                const float2 y = cmulf(v, ph);
+                acc.x += y.x;
+                acc.y += y.y;
+            });
+        }
     }
+    if (o < nv) ext[sb.ext_off + j0 + o] = cp.precise_sum ? make_float2((float)acc64.x, (float)acc64.y) : acc;
 }
 
 // ===========================================================================
@@ -2678,27 +2651,21 @@ cudaError_t launch_extract_wide(int grid, int smem, cudaStream_t sm, const int2 
 
 cudaError_t launch_extract_group(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
-                                 const float2 *hist, const float *taps, float2 *ext, void *part) {
+                                 const float2 *hist, const float *taps, float2 *ext) {
     static std::atomic<uint64_t> optin{0};
     cudaError_t e = smem_optin_once(optin, (const void *)k_extract_group, 220 * 1024);
     if (e != cudaSuccess) return e;
-    k_extract_group<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
+    k_extract_group<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
     return cudaGetLastError();
 }
 
 cudaError_t launch_extract_mod(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                const ChanParams *prm, const ChanState *st, const float2 *x, int n,
-                               const float2 *hist, const float *taps, float2 *ext, void *part) {
+                               const float2 *hist, const float *taps, float2 *ext) {
     static std::atomic<uint64_t> optin{0};
     cudaError_t e = smem_optin_once(optin, (const void *)k_extract_mod, 220 * 1024);
     if (e != cudaSuccess) return e;
-    k_extract_mod<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext, part);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_group_sum(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
-                             const ChanParams *prm, const void *part, float2 *ext) {
-    k_group_sum<<<grid, 256, 0, sm>>>(work, sbt, prm, part, ext);
+    k_extract_mod<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
     return cudaGetLastError();
 }
 

@@ -147,8 +147,9 @@ class ChannelRunner:
     # -- lifecycle ---------------------------------------------------------
     def close(self):
         if self._r:
-            lib.gpud_runner_destroy(self._r)
+            lib.gpud_runner_destroy(self._r)  # waits for every block in flight
             self._r = C.c_void_p()
+        self._keep = ()  # the blocks in flight no longer need their inputs
 
     Close = close
 

@@ -118,6 +118,8 @@ class RunnerStats(C.Structure):
         ("pad", C.c_int32),
         ("last_h2d_bytes", C.c_uint64),
         ("last_d2h_bytes", C.c_uint64),
+        ("ring_copy_ms", C.c_double),
+        ("ring_copies", C.c_uint64),
     ]
 
 

@@ -23,7 +23,7 @@ from . import FORM_DENSE, FORM_GROUP, FORM_MOD, FORM_WIDE, GPUDError, MODE_IQ, C
 # every extraction stage, the channel-group taps packing included (a repack
 # runs only when the group or a member's taps change, so a steady trial
 # mostly sees the group kernel itself)
-_EXTRACT_STAGES = ("extract", "group_sum", "gemm_pack")
+_EXTRACT_STAGES = ("extract", "gemm_pack")
 
 
 def _candidates(T: int, D: int):

@@ -48,6 +48,7 @@ import numpy as np  # noqa: E402
 FS = 10_000_000
 BLOCK = 1 << 20
 N_CH = 40
+E2E_MIN_BLOCKS = 96  # e2e pass: blocks timed through the public API from pinned host memory
 TAPS = 256
 OUT_RATE = 312_500
 BW = 250_000.0
@@ -405,7 +406,7 @@ def stage_key(name):
     """Work group of a runner stage name (extraction by kernel form)."""
     if name.startswith("extract_dense"):
         return "extract_dense"
-    if name in ("extract_group", "group_sum"):
+    if name == "extract_group":
         return "extract_group"
     if name in ("extract_bank", "bank_pack"):
         return "extract_bank"
@@ -425,9 +426,12 @@ def stage_key(name):
 # capture exists.
 NCU_TRAFFIC = {("fm_band", "extract_gemm"): 8.73e6,
                ("fm_band", "pll"): 10.58e6,
-               # k_extract_mod captured at 512 headroom channels (10.5 MB read, 42.2 MB
-               # of partial sums written), scaled by the channel count to 2048
-               ("headroom", "extract_mod"): 52.6e6 * 2048 / 512}
+               }
+# Headroom stress, captured at 512 channels (the 2048-channel launch was not
+# captured): the phase-group kernels read the L2-resident block once and write
+# nothing to DRAM during the launch, so their traffic does not grow with the
+# channel count and is reported as measured, not scaled.
+NCU_TRAFFIC_HEADROOM_512 = {"extract_mod": 10.23e6, "extract_group": 9.70e6}
 
 
 def kernel_roofline(name, ms, work, fp32, hbm_peak, peak_kind, wl, tf32=None):
@@ -461,12 +465,16 @@ def kernel_roofline(name, ms, work, fp32, hbm_peak, peak_kind, wl, tf32=None):
     return roof
 
 
-def h2d_rate(block, stream):
+def h2d_rate(block):
     """Host-to-device copy rate (GB/s) of one pinned input block, timed
-    alone on the runner's stream: the bound of any e2e number whose every
-    block crosses the host link."""
+    alone on a stream of its own (not the runner's: torch's pinned-memory
+    allocator records every stream a pinned block was copied on, and records
+    an event there when the block is freed, which may be after the runner
+    has gone): the bound of any e2e number whose every block crosses the
+    host link."""
     import torch
     dst = torch.empty_like(block, device="cuda")
+    stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         for _ in range(2):
             dst.copy_(block, non_blocking=True)
@@ -654,7 +662,9 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     # the e2e pass's blocks (the stream after the value pass's) in pinned host
     # memory, prepared up front so that the GPU does not idle between the passes
     first = args.warmup + args.steps
-    pinned = [blocks[(first + b) % n_scene].cpu().pin_memory() for b in range(args.warmup + args.steps)]
+    e2e_steps = max(args.steps, E2E_MIN_BLOCKS)
+    pool = [blocks[(first + b) % n_scene].cpu().pin_memory() for b in range(min(n_scene, args.warmup + e2e_steps))]
+    pinned = [pool[b % len(pool)] for b in range(args.warmup + e2e_steps)]
 
     # ---- value: inputs resident in HBM, outputs kept on the device ----------
     runner.set_host_outputs(False)
@@ -695,10 +705,17 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
     clk.__exit__(None, None, None)
     clocks = clk.summary()
     st = runner.stats()
-    e2e = world * n_ch * BLOCK * args.steps / e2e_s / 1e6
+    e2e = world * n_ch * BLOCK * e2e_steps / e2e_s / 1e6
     h2d, d2h = st["last_h2d_bytes"], st["last_d2h_bytes"]
-    h2d_gbs = h2d_rate(pinned[0], stream)
-    del pinned
+    # the host link during the pass: every block's copy into the input ring
+    # is timed on the copy stream
+    ring_ms = st["ring_copy_ms"] / max(1, st["ring_copies"])
+    link = {"ring_copies": st["ring_copies"], "copy_ms_per_block": ring_ms,
+            "gbs_during_pass": (BLOCK * 8) / (ring_ms * 1e-3) / 1e9 if ring_ms > 0 else None,
+            "busy_frac": st["ring_copy_ms"] / (e2e_s * 1e3),
+            "bound": world * n_ch * BLOCK / (ring_ms * 1e-3) / 1e6 if ring_ms > 0 else None}
+    h2d_gbs = h2d_rate(pinned[0])
+    del pinned, pool
     if rank != 0:
         return None
 
@@ -762,8 +779,13 @@ def measure_batch(args, world, rank, local, runner, blocks, n_scene, chans, wl, 
         "e2e": {"value": e2e, "unit": "channel-MS/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "h2d_gbs": h2d_gbs,
                 "h2d_bound": world * n_ch * BLOCK / (h2d / (h2d_gbs * 1e9)) / 1e6,
+                "host_link_during_pass": link,
                 "p50_block_ms": st["p50_block_ms"], "p99_block_ms": st["p99_block_ms"],
-                "blocks_timed": args.steps},
+                "blocks_timed": e2e_steps,
+                "note": f"{e2e_steps} consecutive blocks (at least {E2E_MIN_BLOCKS}, so that the window is steady), "
+                        f"{args.depth} in flight, each copied from pinned host memory into the runner's input ring "
+                        f"and its outputs read back into pinned host memory; h2d_gbs is one block's copy timed "
+                        f"alone, host_link_during_pass the copies as they ran inside the pass"},
         "plain_runner": {"value": plain_v, "unit": "channel-MS/s",
                          "speedup_batched_vs_plain": (value / plain_v) if plain_v else None},
         "latency_ms": {"p50": st_value["p50_block_ms"], "p99": st_value["p99_block_ms"],
@@ -1199,7 +1221,8 @@ def run_headroom(args, world, rank, local):
     roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
             "peak_source": "FP32 FMA microbenchmark, measured in this run", "kernel": dom,
             "ms_per_launch": kern[dom], "algorithmic_flop": wdk["flop"],
-            "traffic": NCU_TRAFFIC.get(("headroom", dk)) if n_live == 2048 else None,
+            "traffic": NCU_TRAFFIC_HEADROOM_512.get(dk) if n_live == 512 else None,
+            "traffic_at_512_channels": NCU_TRAFFIC_HEADROOM_512.get(dk),
             "block": {"gflop": flop / args.steps / 1e9, "min_bytes": b_min, "roofline_ms": t_roof,
                       "measured_ms": block_ms, "frac": t_roof / block_ms,
                       "hbm_peak_gbs": hbm_peak, "hbm_peak_source": peak_kind}}

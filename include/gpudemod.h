@@ -280,6 +280,9 @@ typedef struct {
     int32_t pad;
     uint64_t last_h2d_bytes;  /* host->device bytes of the last block */
     uint64_t last_d2h_bytes;  /* device->host bytes of the last block */
+    double ring_copy_ms;      /* device time of the input-ring copies (blocks from pinned host
+                                 memory) completed since the last reset */
+    uint64_t ring_copies;     /* their count */
 } gpud_runner_stats;
 
 typedef struct gpud_runner gpud_runner;
@@ -343,7 +346,8 @@ GPUD_API int GPUD_CALL gpud_runner_wait(gpud_runner *r, uint64_t ticket, int tim
  * GPUD_E_TIMEOUT when blocks are in flight and none has completed since. */
 GPUD_API int GPUD_CALL gpud_runner_result(gpud_runner *r, int slot, gpud_channel_result *out);
 GPUD_API int GPUD_CALL gpud_runner_stats_get(gpud_runner *r, gpud_runner_stats *out);
-/* Clears the block-latency window behind p50_block_ms / p99_block_ms. */
+/* Clears the block-latency window behind p50_block_ms / p99_block_ms and the
+ * ring-copy totals. */
 GPUD_API int GPUD_CALL gpud_runner_reset_stats(gpud_runner *r);
 /* Stream that joins every submitted block: an event recorded on it after a
  * submit completes when that block and all earlier ones have completed (for
