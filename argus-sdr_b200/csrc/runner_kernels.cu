@@ -1931,24 +1931,52 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
         }
     }
     cl.sync();  // no shared memory of another CTA is read after this
-    if (g != owner) return;
-    if (!converged) {
-        // serial loop from the exact start of segment gstar to the block end
-        uint64_t qr = k.q0 + (uint64_t)t0 * k.qf;
-        float pt = __ldg(pil + t0);
-        for (int t = t0; t < n; ++t) {
-            const float pn = (t + 1 < n) ? __ldg(pil + t + 1) : 0.f;
-            PllEval o;
-            pll_step<false>(qr, x.dphi, x.df, x.I, x.Q, pt, k, o);
-            qr += k.qf;
-            x = SegState{o.dphi1, o.df1, o.I1, o.Q1};
-            es_all += fabs((double)o.e);
-            lr[t] = bpf[t] * pll_two_sin2(qr, x.dphi);
-            pt = pn;
-        }
+    if (converged) {
+        if (g != owner) return;
+        pll_finish(s, cp, n, pll_phase_at(k, n, x.dphi), s.pll_freq + x.df, (double)x.I, (double)x.Q, es_all,
+                   pp_all);
+        s.pll_path = 1;
+        s.pll_iters = iters;
+        return;
     }
-    pll_finish(s, cp, n, pll_phase_at(k, n, x.dphi), s.pll_freq + x.df, (double)x.I, (double)x.Q, es_all, pp_all);
-    s.pll_path = converged ? 1 : 2;
+    // Serial loop from the exact start of segment gstar to the block end, by
+    // the owner's whole warp: the lanes load the pilot band and the L-R band of
+    // the next 32 steps (coalesced, one chunk ahead), all of them evaluate the
+    // same recurrence (uniform values, so the loop never waits on a load), and
+    // lane i keeps step i's L-R product for one coalesced store per chunk.
+    if ((g >> 5) != (owner >> 5)) return;
+    const int ol = owner & 31;
+    SegState xs{__shfl_sync(0xffffffffu, x.dphi, ol), __shfl_sync(0xffffffffu, x.df, ol),
+                __shfl_sync(0xffffffffu, x.I, ol), __shfl_sync(0xffffffffu, x.Q, ol)};
+    const int ts = __shfl_sync(0xffffffffu, t0, ol);
+    double es_w = __shfl_sync(0xffffffffu, es_all, ol);
+    uint64_t qr = k.q0 + (uint64_t)ts * k.qf;
+    float pcur = ts + lane < n ? __ldg(pil + ts + lane) : 0.f;
+    float bcur = ts + lane < n ? bpf[ts + lane] : 0.f;
+    for (int c0 = ts; c0 < n; c0 += 32) {
+        const int cn = c0 + 32;
+        const float pnext = cn + lane < n ? __ldg(pil + cn + lane) : 0.f;
+        const float bnext = cn + lane < n ? bpf[cn + lane] : 0.f;
+        const int cnt = min(32, n - c0);  // uniform in the warp
+        float mine = 0.f;
+#pragma unroll 4
+        for (int i = 0; i < cnt; ++i) {
+            const float pt = __shfl_sync(0xffffffffu, pcur, i);
+            PllEval o;
+            pll_step<false>(qr, xs.dphi, xs.df, xs.I, xs.Q, pt, k, o);
+            qr += k.qf;
+            xs = SegState{o.dphi1, o.df1, o.I1, o.Q1};
+            es_w += fabs((double)o.e);
+            const float th = pll_two_sin2(qr, xs.dphi);
+            if (lane == i) mine = bcur * th;
+        }
+        if (lane < cnt) lr[c0 + lane] = mine;
+        pcur = pnext;
+        bcur = bnext;
+    }
+    if (lane != ol) return;
+    pll_finish(s, cp, n, pll_phase_at(k, n, xs.dphi), s.pll_freq + xs.df, (double)xs.I, (double)xs.Q, es_w, pp_all);
+    s.pll_path = 2;
     s.pll_iters = iters;
 }
 
