@@ -38,6 +38,9 @@ struct WfmTaps;
 cudaError_t launch_extract_dense(int L, int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                                  const ChanParams *prm, const ChanState *st, const float2 *x, int n,
                                  const float2 *hist, const float *taps, float2 *ext);
+cudaError_t launch_extract_dense_any(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                     const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                     const float2 *hist, const float *taps, float2 *ext);
 cudaError_t launch_extract_dense_pipe(int L, int ng, int ntiles, int grid, int pmax, cudaStream_t sm,
                                       const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                                       const ChanState *st, const float2 *x, int n, const float2 *hist,
@@ -1270,8 +1273,46 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     std::memcpy(hd + o_sb, pl.sbs.data(), pl.sbs.size() * sizeof(SlotBlock));
     int2 *hw = (int2 *)(hd + o_w);
     size_t cnt = 0;
-    size_t w_dense_off[kDenseMaxL + 1];
+    // Dense classes: the persistent kernel pays off with at least two tiles
+    // per SM; smaller classes (e.g. the history tiles of grouped channels)
+    // run one tile per CTA.  Such classes whose shared memory is within 2x of
+    // each other go out as one launch (their tiles laid out contiguously,
+    // largest footprint first), so that a dozen small classes fill the GPU
+    // together instead of one after another.
+    bool dense_pipe[kDenseMaxL + 1] = {};
+    int dense_ng[kDenseMaxL + 1] = {};
+    std::vector<int> tile_classes;
     for (int L = 0; L <= kDenseMaxL; ++L) {
+        if (pl.w_dense[L].empty()) continue;
+        const int ntiles = (int)pl.w_dense[L].size();
+        dense_ng[L] = std::min(GPUD_DENSE_PIPE, dense_pipe_groups_host(pl.dense_pmax[L], L, kDensePipeSmemCap));
+        dense_pipe[L] = dense_ng[L] > 0 && ntiles >= 2 * r->num_sms && r->d_fault && ((uintptr_t)x_dev & 15) == 0;
+        if (!dense_pipe[L]) tile_classes.push_back(L);
+    }
+    std::stable_sort(tile_classes.begin(), tile_classes.end(),
+                     [&](int a, int b) { return pl.dense_smem[a] > pl.dense_smem[b]; });
+    struct DenseBatch {
+        size_t off = 0, items = 0;
+        int smem = 0, classes = 0, L = 0;
+    };
+    std::vector<DenseBatch> batches;
+    size_t w_dense_off[kDenseMaxL + 1] = {};
+    for (int L : tile_classes) {
+        if (batches.empty() || 2 * pl.dense_smem[L] < batches.back().smem) {
+            batches.emplace_back();
+            batches.back().off = cnt;
+            batches.back().smem = pl.dense_smem[L];
+            batches.back().L = L;
+        }
+        DenseBatch &bt = batches.back();
+        w_dense_off[L] = cnt;
+        std::memcpy(hw + cnt, pl.w_dense[L].data(), pl.w_dense[L].size() * sizeof(int2));
+        cnt += pl.w_dense[L].size();
+        bt.items += pl.w_dense[L].size();
+        bt.classes++;
+    }
+    for (int L = 0; L <= kDenseMaxL; ++L) {
+        if (pl.w_dense[L].empty() || !dense_pipe[L]) continue;
         w_dense_off[L] = cnt;
         std::memcpy(hw + cnt, pl.w_dense[L].data(), pl.w_dense[L].size() * sizeof(int2));
         cnt += pl.w_dense[L].size();
@@ -1335,25 +1376,29 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
         CK(cudaEventRecord(f.ev_fork, f.s));
         CK(cudaStreamWaitEvent(f.s2, f.ev_fork, 0));
     }
+    auto dense_name = [](int L) {
+        return L < 10 ? std::string("extract_dense_L") + char('0' + L)
+                      : std::string("extract_dense_L1") + char('0' + L - 10);
+    };
+    for (const DenseBatch &bt : batches) {
+        // one tile per CTA; the smaller CTAs share SMs with the other blocks in flight
+        if (!side) prof_mark(r, f, bt.classes > 1 ? "extract_dense" : dense_name(bt.L).c_str());
+        if (bt.classes > 1)
+            CK(launch_extract_dense_any((int)bt.items, bt.smem, ds, d_w + bt.off, d_sb, r->d_prm, r->d_st, x_dev, n,
+                                        r->d_hist, r->d_taps, d_ext));
+        else
+            CK(launch_extract_dense(bt.L, (int)bt.items, bt.smem, ds, d_w + bt.off, d_sb, r->d_prm, r->d_st, x_dev,
+                                    n, r->d_hist, r->d_taps, d_ext));
+        nl++;
+    }
     for (int L = 0; L <= kDenseMaxL; ++L) {
-        if (pl.w_dense[L].empty()) continue;
-        if (!side)
-            prof_mark(r, f, L < 10 ? (std::string("extract_dense_L") + char('0' + L)).c_str()
-                                    : (std::string("extract_dense_L1") + char('0' + L - 10)).c_str());
-        const int ntiles = (int)pl.w_dense[L].size();
-        const int ng = std::min(GPUD_DENSE_PIPE, dense_pipe_groups_host(pl.dense_pmax[L], L, kDensePipeSmemCap));
-        // the persistent kernel pays off with at least two tiles per SM; a
-        // smaller class (e.g. the history tiles of grouped channels) runs one
-        // tile per CTA, whose smaller CTAs share SMs with the other blocks in flight
-        if (ng > 0 && ntiles >= 2 * r->num_sms && r->d_fault && ((uintptr_t)x_dev & 15) == 0) {
-            // persistent: one CTA per SM over contiguous runs of tiles
-            CK(launch_extract_dense_pipe(L, ng, ntiles, std::min(ntiles, r->num_sms), pl.dense_pmax[L], ds,
-                                         d_w + w_dense_off[L], d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist,
-                                         r->d_taps, d_ext, r->d_fault));
-        } else {
-            CK(launch_extract_dense(L, ntiles, pl.dense_smem[L], ds, d_w + w_dense_off[L], d_sb, r->d_prm,
-                                    r->d_st, x_dev, n, r->d_hist, r->d_taps, d_ext));
-        }
+        if (pl.w_dense[L].empty() || !dense_pipe[L]) continue;
+        if (!side) prof_mark(r, f, dense_name(L).c_str());
+        // persistent: one CTA per SM over contiguous runs of tiles
+        CK(launch_extract_dense_pipe(L, dense_ng[L], (int)pl.w_dense[L].size(),
+                                     std::min((int)pl.w_dense[L].size(), r->num_sms), pl.dense_pmax[L], ds,
+                                     d_w + w_dense_off[L], d_sb, r->d_prm, r->d_st, x_dev, n, r->d_hist, r->d_taps,
+                                     d_ext, r->d_fault));
         nl++;
     }
     if (!pl.w_gemm.empty()) {

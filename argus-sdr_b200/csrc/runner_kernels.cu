@@ -285,18 +285,14 @@ __device__ __forceinline__ void tile_sum(int rows, const Row &row, float2 *Z, co
     }
 }
 
+// One 256-output tile of the dense form (work item w), arm length L.
 template <int L>
-__global__ void __launch_bounds__(kDenseThreads, 2)
-k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
-                const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
-                const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
-                float2 *__restrict__ ext) {
-    extern __shared__ float4 smem4[];
-    const int2 w = work[blockIdx.x];
-    const SlotBlock sb = sbt[w.x];
+__device__ __forceinline__ void dense_tile(const int2 w, const SlotBlock &sb, const ChanParams &cp,
+                                           const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+                                           const float2 *__restrict__ hist_arena,
+                                           const float *__restrict__ taps_arena, float2 *__restrict__ ext,
+                                           float4 *smem4) {
     const int j0 = w.y * kDenseOT;
-    if (j0 >= sb.n_out) return;
-    const ChanParams &cp = prm[sb.slot];
     const int D = cp.decim;
     const int P = cp.nphase;
     const int M = kDenseOT + L - 1;
@@ -345,6 +341,41 @@ k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt
         tile_sum<false>(P, row, Z, [&](int o, float2 v) {
             if (o < nv) dst[o] = v;
         });
+}
+
+template <int L>
+__global__ void __launch_bounds__(kDenseThreads, 2)
+k_extract_dense(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
+                const ChanState *__restrict__ st, const float2 *__restrict__ x, int n,
+                const float2 *__restrict__ hist_arena, const float *__restrict__ taps_arena,
+                float2 *__restrict__ ext) {
+    extern __shared__ float4 smem4[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    if (w.y * kDenseOT >= sb.n_out) return;
+    dense_tile<L>(w, sb, prm[sb.slot], st, x, n, hist_arena, taps_arena, ext, smem4);
+}
+
+// Several dense classes in one launch (each too small to fill the GPU alone):
+// every CTA takes its tile's arm length from the channel.
+__global__ void __launch_bounds__(kDenseThreads, 2)
+k_extract_dense_any(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt,
+                    const ChanParams *__restrict__ prm, const ChanState *__restrict__ st,
+                    const float2 *__restrict__ x, int n, const float2 *__restrict__ hist_arena,
+                    const float *__restrict__ taps_arena, float2 *__restrict__ ext) {
+    extern __shared__ float4 smem4[];
+    const int2 w = work[blockIdx.x];
+    const SlotBlock sb = sbt[w.x];
+    if (w.y * kDenseOT >= sb.n_out) return;
+    const ChanParams &cp = prm[sb.slot];
+    switch (cp.plen) {  // uniform per CTA
+#define GPUD_ANY(LL) \
+    case LL: dense_tile<LL>(w, sb, cp, st, x, n, hist_arena, taps_arena, ext, smem4); break;
+        GPUD_ANY(2) GPUD_ANY(3) GPUD_ANY(4) GPUD_ANY(5) GPUD_ANY(6) GPUD_ANY(7) GPUD_ANY(8) GPUD_ANY(9)
+        GPUD_ANY(10) GPUD_ANY(11) GPUD_ANY(12) GPUD_ANY(13) GPUD_ANY(14) GPUD_ANY(15) GPUD_ANY(16)
+#undef GPUD_ANY
+    default: break;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2604,6 +2635,16 @@ static cudaError_t launch_dense_L(int grid, int smem, cudaStream_t sm, const int
     cudaError_t e = smem_optin_once(optin, (const void *)k_extract_dense<L>, 220 * 1024);
     if (e != cudaSuccess) return e;
     k_extract_dense<L><<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract_dense_any(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
+                                     const ChanParams *prm, const ChanState *st, const float2 *x, int n,
+                                     const float2 *hist, const float *taps, float2 *ext) {
+    static std::atomic<uint64_t> optin{0};
+    cudaError_t e = smem_optin_once(optin, (const void *)k_extract_dense_any, 220 * 1024);
+    if (e != cudaSuccess) return e;
+    k_extract_dense_any<<<grid, kDenseThreads, smem, sm>>>(work, sbt, prm, st, x, n, hist, taps, ext);
     return cudaGetLastError();
 }
 
