@@ -77,15 +77,14 @@ cudaError_t launch_seg_aa(cudaStream_t sm, const float *in, int C, const double 
 cudaError_t launch_comp_power(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt,
                               const ChanParams *prm, ChanState *st, const float *wk);
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W, DevResult *res);
+                       ChanState *st, float *wk, int W);
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
-                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters,
-                              DevResult *res);
+                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters);
 int pll_newton_threads();
 int pll_cluster_for(int max_n);
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
-                           const float *audio_dl, float *audio, const DevResult *res);
+                           const float *audio_dl, float *audio);
 cudaError_t launch_rds(int grid, int smem, cudaStream_t sm, const int2 *work, const SlotBlock *sbt,
                        const ChanParams *prm, const ChanState *st, const WfmTaps *taps, const BinadeTable *tabs,
                        const float *wk, const float2 *rds_dl, float2 *rds_out);
@@ -309,7 +308,6 @@ struct Frame {
     cudaStream_t s = nullptr;
     cudaEvent_t ev_front = nullptr, ev_back = nullptr, ev_done = nullptr, ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_ext = nullptr;  // the block's extraction state (history, NCO phase) is carried
-    cudaEvent_t ev_pll = nullptr;  // the block's pilot loop state is carried (the next block's loop may start)
     int ring = -1;                 // input ring slot the block reads (-1: device input or the frame's own buffer)
     cudaEvent_t ev_start = nullptr;  // where the block's latency starts (ev0, or its ring copy's start)
     cudaStream_t s2 = nullptr;  // side stream: dense classes beside the channel-group kernel
@@ -1527,11 +1525,8 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
     CK(cudaEventRecord(f.ev_front, f.s));
     // ---- back half: after the previous block's back half ----
     if (prev) {
-        // the loop stages carry only the pilot loop's state: the next block's
-        // loop starts as soon as this one's has finished, beside this block's
-        // stereo output and audio back end
-        prof_mark(r, f, "wait_prev_pll");
-        CK(cudaStreamWaitEvent(f.s, prev->ev_pll, 0));
+        prof_mark(r, f, "wait_prev_back");
+        CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
     }
     if (!pl.w_free.empty()) {
         prof_mark(r, f, "free_stereo");
@@ -1552,25 +1547,17 @@ static int enqueue_block(gpud_runner *r, Frame &f, const Frame *prev, BlockPlan 
             for (int i : pl.pll_list) max_n = std::max(max_n, pl.sbs[(size_t)i].n_disc);
             const int cluster = pll_cluster_for(max_n);
             prof_mark(r, f, "pll_newton");
-            CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->pll_max_iters,
-                                 d_res));
+            CK(launch_pll_newton(nch, cluster, f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, r->pll_max_iters));
         } else {
             prof_mark(r, f, "pll_serial");
-            CK(launch_pll((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W, d_res));
+            CK(launch_pll((int)pl.pll_list.size(), f.s, d_pll, d_sb, r->d_prm, r->d_st, f.d_wk, W));
         }
         nl++;
-    }
-    CK(cudaEventRecord(f.ev_pll, f.s));
-    if (prev) {
-        // stereo output, audio back end and state carry: after the previous
-        // block's (delay lines, resampler and de-emphasis state)
-        prof_mark(r, f, "wait_prev_back");
-        CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
     }
     if (!pl.w_out.empty()) {
         prof_mark(r, f, "wfm_out");
         CK(launch_wfm_out((int)pl.w_out.size(), f.s, d_w + o_out, d_sb, r->d_prm, r->d_st, wt, f.d_wk, W, r->d_lr_dl,
-                          r->d_audio_dl, d_audio, d_res));
+                          r->d_audio_dl, d_audio));
         nl++;
     }
     if (!pl.aud_list.empty()) {
@@ -1693,11 +1680,9 @@ static int submit_batched(gpud_runner *r, const gpud_float2 *iq, int n, int on_d
         // no channels: the chains of the block before pass through unchanged
         if (prev) {
             CK(cudaStreamWaitEvent(f.s, prev->ev_front, 0));
-            CK(cudaStreamWaitEvent(f.s, prev->ev_pll, 0));
             CK(cudaStreamWaitEvent(f.s, prev->ev_back, 0));
         }
         CK(cudaEventRecord(f.ev_ext, f.s));
-        CK(cudaEventRecord(f.ev_pll, f.s));
         if (f.ring >= 0) CK(cudaEventRecord(r->ring_free[f.ring], f.s));
         CK(cudaEventRecord(f.ev_front, f.s));
         CK(cudaEventRecord(f.ev_back, f.s));
@@ -1852,7 +1837,6 @@ GPUD_API int GPUD_CALL gpud_runner_create(int sample_rate, int max_block, int ma
         CKC(cudaStreamCreateWithFlags(&f.s, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_front, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&f.ev_ext, cudaEventDisableTiming));
-        CKC(cudaEventCreateWithFlags(&f.ev_pll, cudaEventDisableTiming));
         CKC(cudaStreamCreateWithFlags(&f.s2, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&f.ev_fork, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&f.ev_join, cudaEventDisableTiming));
@@ -1919,7 +1903,7 @@ GPUD_API int GPUD_CALL gpud_runner_destroy(gpud_runner *r) {
         if (f.h_out) cudaFreeHost(f.h_out);
         if (f.h_stage) cudaFreeHost(f.h_stage);
         if (f.h_in) cudaFreeHost(f.h_in);
-        for (auto e : {f.ev_front, f.ev_ext, f.ev_pll, f.ev_back, f.ev_done, f.ev0, f.ev1, f.ev_fork, f.ev_join})
+        for (auto e : {f.ev_front, f.ev_ext, f.ev_back, f.ev_done, f.ev0, f.ev1, f.ev_fork, f.ev_join})
             if (e) cudaEventDestroy(e);
         for (auto e : f.prof_ev) cudaEventDestroy(e);
         if (f.s2) {

@@ -1434,22 +1434,9 @@ __device__ void pll_finish(ChanState &s, const ChanParams &cp, int n, double ph,
 // (streamer.go:1363-1380, 1615-1635).
 constexpr int kPllChunk = 2048;
 
-// The block's loop outcome in its own results row, written by the PLL kernel:
-// the next block's PLL may update the channel state while this block's later
-// stages (stereo output, state carry) still run, so they read it from here.
-__device__ __forceinline__ void pll_result(DevResult &o, const ChanState &s) {
-    o.flags = (s.locked ? 1 : 0) | (s.enabled ? 2 : 0);
-    o.coherence = s.coherence;
-    o.pilot_hz = s.pilot_hz;
-    o.err_avg = s.last_err_avg;
-    o.status = s.pll_path;
-    o.pll_iters = s.pll_iters;
-}
-
 __global__ void __launch_bounds__(64)
 k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
-      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
-      DevResult *__restrict__ res) {
+      const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W) {
     __shared__ float s_pil[2][kPllChunk];
     __shared__ float s_th[2][kPllChunk];
     __shared__ double s_red[32];
@@ -1525,7 +1512,6 @@ k_pll(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt
     if (threadIdx.x != 0) return;
     pll_finish(s, cp, n, pll_phase_at(k, n, dphi), s.pll_freq + df, (double)I, (double)Q, es, s_red[0]);
     s.pll_path = 2;
-    pll_result(res[sb.res_idx], s);
 }
 
 
@@ -1671,7 +1657,7 @@ constexpr int kPllStageS = 16;
 __global__ void __launch_bounds__(kNewtonThreads, 3)
 k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restrict__ sbt,
              const ChanParams *__restrict__ prm, ChanState *__restrict__ st, float *__restrict__ wk, int W,
-             int max_iters, DevResult *__restrict__ res) {
+             int max_iters) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float s_tot[kNW][20];     // warp totals
@@ -1982,7 +1968,6 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
                    pp_all);
         s.pll_path = 1;
         s.pll_iters = iters;
-        pll_result(res[sb.res_idx], s);
         return;
     }
     // Serial loop from the exact start of segment gstar to the block end, by
@@ -2024,7 +2009,6 @@ k_pll_newton(const int *__restrict__ list, int count, const SlotBlock *__restric
     pll_finish(s, cp, n, pll_phase_at(k, n, xs.dphi), s.pll_freq + xs.df, (double)xs.I, (double)xs.Q, es_w, pp_all);
     s.pll_path = 2;
     s.pll_iters = iters;
-    pll_result(res[sb.res_idx], s);
 }
 
 // Sum of the block's composite squared for batch-stereo channels (the
@@ -2072,8 +2056,7 @@ k_free_stereo(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, 
 __global__ void __launch_bounds__(kFirThreads)
 k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ prm,
           const ChanState *__restrict__ st, const WfmTaps *__restrict__ taps, const float *__restrict__ wk, int W,
-          const float *__restrict__ lr_dl, const float *__restrict__ audio_dl, float *__restrict__ audio,
-          const DevResult *__restrict__ res) {
+          const float *__restrict__ lr_dl, const float *__restrict__ audio_dl, float *__restrict__ audio) {
     __shared__ float win[padi(kFirOT + kWfmTapsPad) + 8];
     __shared__ float tp[kWfmTapsPad];
     __shared__ float s_out[kFirOT + kFirOT / 32];
@@ -2082,9 +2065,7 @@ k_wfm_out(const int2 *__restrict__ work, const SlotBlock *__restrict__ sbt, cons
     const ChanParams &cp = prm[sb.slot];
     const int q0 = w.y * kFirOT;
     if (q0 >= sb.n_disc) return;
-    // a loop-decoded channel's stereo decision of this block is in its results
-    // row (the channel state may already hold the next block's)
-    const bool stereo = (cp.mode == 3) && ((cp.flags & kChFreeStereo) || (res[sb.res_idx].flags & 2));
+    const bool stereo = (cp.mode == 3) && (st[sb.slot].enabled || (cp.flags & kChFreeStereo));
     if (cp.mode == 3 && !stereo && (cp.flags & kChBatchStereo)) {
         // batch decoder not locked: the discriminator output itself on both
         // channels (wfm_batch_stereo.go:43-49)
@@ -2359,13 +2340,9 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
     const SlotBlock sb = sbt[blockIdx.x];
     const ChanParams &cp = prm[sb.slot];
     ChanState &s = st[sb.slot];
-    // loop-decoded channels: this block's decisions come from the results row
-    // the PLL kernel wrote (the channel state may already hold the next block's)
-    const bool pll_ch = cp.mode == 3 && sb.n_disc > 0 && !(cp.flags & kChFreeStereo);
-    const bool enabled = pll_ch ? (res[sb.res_idx].flags & 2) != 0 : (bool)s.enabled;
     if (cp.wfm_idx >= 0 && sb.n_disc > 0) {
         const float *comp = wk + sb.comp_off;
-        const bool fallback = (cp.mode == 2) || !enabled;
+        const bool fallback = (cp.mode == 2) || !s.enabled;
         if (fallback) {
             float *adl = audio_dl + cp.wfm_idx * kAudioDlStride;
             int valid = __float_as_int(adl[kWfmHist]);
@@ -2375,7 +2352,7 @@ k_post_back(const SlotBlock *__restrict__ sbt, const ChanParams *__restrict__ pr
         }
         if (cp.mode == 3) shift_delay_line(lr_dl + cp.wfm_idx * kWfmHist, wk + 4 * W + sb.comp_off, sb.n_disc);
     }
-    if (threadIdx.x == 0 && !pll_ch) {
+    if (threadIdx.x == 0) {
         DevResult &o = res[sb.res_idx];
         o.flags = (cp.mode == 3 && sb.n_disc > 0) ? ((s.locked ? 1 : 0) | (s.enabled ? 2 : 0))
                                                   : (s.enabled ? 2 : 0);
@@ -2818,14 +2795,13 @@ cudaError_t launch_wfm_fir(int grid, cudaStream_t sm, const int2 *work, const Sl
 }
 
 cudaError_t launch_pll(int count, cudaStream_t sm, const int *list, const SlotBlock *sbt, const ChanParams *prm,
-                       ChanState *st, float *wk, int W, DevResult *res) {
-    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W, res);
+                       ChanState *st, float *wk, int W) {
+    k_pll<<<count, 64, 0, sm>>>(list, count, sbt, prm, st, wk, W);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int *list, const SlotBlock *sbt,
-                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters,
-                              DevResult *res) {
+                              const ChanParams *prm, ChanState *st, float *wk, int W, int max_iters) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(count * cluster), 1, 1);
     cfg.blockDim = dim3(kNewtonThreads, 1, 1);
@@ -2838,15 +2814,15 @@ cudaError_t launch_pll_newton(int count, int cluster, cudaStream_t sm, const int
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_pll_newton, list, count, sbt, prm, st, wk, W, max_iters, res);
+    return cudaLaunchKernelEx(&cfg, k_pll_newton, list, count, sbt, prm, st, wk, W, max_iters);
 }
 
 int pll_newton_threads() { return kNewtonThreads; }
 
 cudaError_t launch_wfm_out(int grid, cudaStream_t sm, const int2 *work, const SlotBlock *sbt, const ChanParams *prm,
                            const ChanState *st, const WfmTaps *taps, const float *wk, int W, const float *lr_dl,
-                           const float *audio_dl, float *audio, const DevResult *res) {
-    k_wfm_out<<<grid, kFirThreads, 0, sm>>>(work, sbt, prm, st, taps, wk, W, lr_dl, audio_dl, audio, res);
+                           const float *audio_dl, float *audio) {
+    k_wfm_out<<<grid, kFirThreads, 0, sm>>>(work, sbt, prm, st, taps, wk, W, lr_dl, audio_dl, audio);
     return cudaGetLastError();
 }
 
