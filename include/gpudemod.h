@@ -335,9 +335,8 @@ GPUD_API int GPUD_CALL gpud_runner_process_block(gpud_runner *r, const gpud_floa
  * once the outputs of every block up to that ticket are in host memory
  * (GPUD_E_TIMEOUT after timeout_ms).  Three blocks may be in flight: block
  * k+1's extraction / demod / stereo FIR / RDS stages run while block k's pilot
- * PLL and stereo output finish, block k+1's PLL while block k's audio back end
- * finishes, and their copies overlap; a fourth submit first completes the
- * oldest block.  A block in pinned host memory starts its copy into one of the
+ * PLL and stereo output finish, and their copies overlap; a fourth submit
+ * first completes the oldest block.  A block in pinned host memory starts its copy into one of the
  * runner's four input-ring buffers when it is submitted, before that wait.
  * A pinned host iq buffer is read asynchronously and must stay unchanged until
  * its block completed; pageable buffers are copied before submit returns. */
