@@ -84,3 +84,56 @@ def test_ring_equals_frame_staging(cuda):
                 va, vb = a[sid][key], b[sid][key]
                 same = np.array_equal(va, vb) if isinstance(va, np.ndarray) else va == vb
                 assert same, (k, sid, key)
+
+
+def test_sources_interleaved_in_one_stream(cuda):
+    """Pinned (input ring), pageable (frame staging) and device-resident
+    blocks, and an empty block, alternating in one pipelined stream: the ring
+    slots advance only for pinned blocks, and every output equals the
+    one-block-at-a-time runner's on the same blocks."""
+    import torch
+    scene, _ = synth.mixed_scene(device="cuda", block=BLOCK, seed=SEED + 1)
+    lengths = [BLOCK, BLOCK - 3, 0, BLOCK, 150_001, BLOCK, BLOCK - 1024, BLOCK, BLOCK]
+    raw = [scene.next_block().cpu().numpy()[:n] for n in lengths]
+    kinds = ["pin", "page", "pin", "dev", "pin", "pin", "page", "dev", "pin"]
+    src = []
+    for x, kind in zip(raw, kinds):
+        if kind == "pin":
+            src.append(torch.from_numpy(x).pin_memory())
+        elif kind == "dev":
+            src.append(torch.from_numpy(x).to("cuda"))
+        else:
+            src.append(x)
+    specs = _specs()[:-1]
+
+    def runner():
+        r = G.ChannelRunner(FS, BLOCK, max_channels=64, max_taps=1024)
+        return r, {s[0]: r.admit(*s) for s in specs}
+
+    rs, ls = runner()
+    rp, lp = runner()
+    try:
+        want = []
+        for x in raw:
+            rs.process_block(x)
+            want.append({sid: rs.result(sl) for sid, sl in ls.items()})
+        got, tickets = [], []
+        for k, x in enumerate(src):
+            tickets.append(rp.submit(x))
+            if k >= 2:
+                rp.wait(tickets[k - 2])
+                got.append({sid: rp.result(sl) for sid, sl in lp.items()})
+        for k in range(len(src) - 2, len(src)):
+            rp.wait(tickets[k])
+            got.append({sid: rp.result(sl) for sid, sl in lp.items()})
+        assert len(got) == len(want)
+        for k, (a, b) in enumerate(zip(want, got)):
+            for sid in a:
+                for key in KEYS:
+                    va, vb = a[sid][key], b[sid][key]
+                    same = np.array_equal(va, vb) if isinstance(va, np.ndarray) else va == vb
+                    assert same, (k, kinds[k], sid, key)
+        assert rp.stats()["blocks"] == len(src)
+    finally:
+        rs.close()
+        rp.close()
