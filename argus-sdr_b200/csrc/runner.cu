@@ -2031,6 +2031,26 @@ static void choose_extraction(gpud_runner *r, Slot &s) {
     s.ext_kind = mod ? 3 : 2;
     s.ng = (s.P + pmax - 1) / pmax;
     s.pg = (s.P + s.ng - 1) / s.ng;
+    // The staging puts a group's phases on lanes (one pass per 32) and its
+    // rows on the 8 warps: groups of at most a multiple of 32 phases can keep
+    // the lanes full (100 phases as 4 x 25 rather than 3 x 34, whose second
+    // lane pass holds 2 of 32) at the price of more groups; take that split
+    // when the instructions per thread it needs are fewer.
+    if (pmax >= 64 || (pmax >= 32 && pmax % 32 != 0)) {
+        const int q = pmax / 32 * 32;
+        const int ng = (s.P + q - 1) / q, pg = (s.P + ng - 1) / ng;
+        const int Le = mod ? s.L : ((s.L > 16) ? (s.L + 7) & ~7 : s.L);
+        const int cols = 256 + Le - 1;
+        auto cost = [&](int groups, int phases) {
+            const int lane_passes = (phases + 31) / 32, row_rounds = (phases + 7) / 8;
+            const int row = 8 + 2 * Le - 1 + (mod ? 4 : 2) * 8 * Le;  // window + taps loads, FMAs of 8 outputs
+            return (int64_t)groups * (lane_passes * 14 * cols / 8 + row_rounds * row + 100);
+        };
+        if (cost(ng, pg) < cost(s.ng, s.pg)) {
+            s.ng = ng;
+            s.pg = pg;
+        }
+    }
 }
 
 static int admit_core(gpud_runner *r, const gpud_channel_spec *spec, int D, int T, double deemph_us,
