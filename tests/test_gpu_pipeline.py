@@ -10,7 +10,7 @@ from signals import max_abs, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-AUDIO_TOL = 1e-5   # relative L2 per block
+AUDIO_TOL = 1e-5   # relative L2 per block (the parity tolerance)
 RDS_TOL = 1e-5
 
 

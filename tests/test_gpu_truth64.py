@@ -1,7 +1,7 @@
 """Error against a float64 truth, per output: the GPU chain and the
 reference-precision restatement (the oracle), each against the same chain
 evaluated entirely in float64 (oracle/truth64.py).  Both must stay within the
-north-star tolerance (relative L2 <= 1e-5 per output stream); the GPU's error
+parity tolerance (relative L2 <= 1e-5 per output stream); the GPU's error
 is reported next to the oracle's.  With GPUD_PARITY_REPORT set to a path the
 table is written there as JSON."""
 import json
