@@ -18,7 +18,11 @@ which the test checks on the inputs it rebuilds):
     129, 511, 2000 and 6148 samples, every chunk's outputs and the carried
     history length, phase count and phase;
   * FM discriminator, gpud_launch_fm_discrim_cuda, on a tone-plus-tones input
-    and a two-tone deterministic input of 20000 samples each.
+    and a two-tone deterministic input of 20000 samples each;
+  * the legacy batch slot chain (batch_runner_windows.go:170-178): frequency
+    shift from the job's start phase, FIR v2 with the 101-tap low-pass of the
+    job's bandwidth, decimation, for two jobs at 2.4 MS/s and two at 10 MS/s
+    on 65536 samples (tones 1 kHz inside each passband over a noise-like mix).
 """
 import ctypes as C
 import hashlib
@@ -40,6 +44,19 @@ REF_PATH = os.path.join(ROOT, "oracle", "_ref", "libgpudemod_ref.so")
 FS = 4_000_000
 CHUNKS = [0, 1, 2, 17, 63, 64, 65, 129, 511, 2000, 6148]
 STATEFUL = [(65, 20, 12_500.0), (33, 40, -18_750.0), (129, 8, 300_000.0)]
+SLOT_N = 1 << 16
+SLOTS = [(2_400_000, [(300_000.0, 250_000.0, 300_000, 0.0), (-1_100_000.0, 12_500.0, 48_000, 2.5)]),
+         (10_000_000, [(4_300_000.0, 12_500.0, 25_000, -1.0), (1_234_567.0, 250_000.0, 312_500, 0.3)])]
+
+
+def slot_input(fs, jobs):
+    """The slot chain's input: a tone 1 kHz inside each job's passband plus
+    the noise-like mix (deterministic)."""
+    t = np.arange(SLOT_N, dtype=np.float64)
+    x = 0.1 * make_tone_noise_iq(t.size, 0.9).astype(np.complex128)
+    for off, _, _, _ in jobs:
+        x += np.exp(2j * np.pi * (off + 1000.0) / fs * t)
+    return x.astype(np.complex64)
 
 
 def _ref():
@@ -48,6 +65,12 @@ def _ref():
     pi, pd = C.POINTER(C.c_int), C.POINTER(C.c_double)
     r.gpud_stream_sync.restype, r.gpud_stream_sync.argtypes = i, [P]
     r.gpud_launch_fm_discrim_cuda.restype, r.gpud_launch_fm_discrim_cuda.argtypes = i, [P, P, i]
+    r.gpud_stream_create.restype, r.gpud_stream_create.argtypes = i, [P]
+    r.gpud_stream_destroy.restype, r.gpud_stream_destroy.argtypes = i, [P]
+    r.gpud_launch_freq_shift_stream_cuda.restype = i
+    r.gpud_launch_freq_shift_stream_cuda.argtypes = [P, P, i, d, d, P]
+    r.gpud_launch_fir_v2_stream_cuda.restype, r.gpud_launch_fir_v2_stream_cuda.argtypes = i, [P, P, P, i, i, P]
+    r.gpud_launch_decimate_stream_cuda.restype, r.gpud_launch_decimate_stream_cuda.argtypes = i, [P, P, i, i, P]
     f = r.gpud_launch_streaming_polyphase_stateful_cuda
     f.restype, f.argtypes = i, [P, i, P, P, i, i, i, P, P, i, pi, pi, pd, d, P, i, pi]
     return r
@@ -101,6 +124,24 @@ def main(out_path):
         assert r.gpud_stream_sync(None) == 0
         store[f"discrim{k}_in_sha256"] = _sha(xin)
         store[f"discrim{k}_out"] = d_out.cpu().numpy()[: xin.size - 1].copy()
+    for g, (fs, jobs) in enumerate(SLOTS):
+        x = slot_input(fs, jobs)
+        store[f"slot{g}_in_sha256"] = _sha(x)
+        d_in = dev(x)
+        for j, (off, bw, rate, p0) in enumerate(jobs):
+            taps = O.lowpass_fir(max(bw / 2, 200.0), fs, 101).astype(np.float32)
+            d_t = dev(taps)
+            decim = fs // rate
+            n_out = x.size // decim
+            sh, flt, dec = (empty(x.size, torch.complex64) for _ in range(3))
+            s = C.c_void_p()
+            assert r.gpud_stream_create(C.byref(s)) == 0
+            assert r.gpud_launch_freq_shift_stream_cuda(d_in.data_ptr(), sh.data_ptr(), x.size,
+                                                        -2.0 * math.pi * off / fs, p0, s) == 0
+            assert r.gpud_launch_fir_v2_stream_cuda(sh.data_ptr(), flt.data_ptr(), d_t.data_ptr(), x.size, 101, s) == 0
+            assert r.gpud_launch_decimate_stream_cuda(flt.data_ptr(), dec.data_ptr(), n_out, decim, s) == 0
+            assert r.gpud_stream_sync(s) == 0 and r.gpud_stream_destroy(s) == 0
+            store[f"slot{g}_job{j}_out"] = dec.cpu().numpy()[:n_out].copy()
     np.savez_compressed(out_path, **store)
     print("wrote", out_path, os.path.getsize(out_path), "bytes")
 

@@ -5,8 +5,10 @@ run once by tests/golden/make_ref_golden.py) on deterministic inputs.  The
 oracle's streaming polyphase extraction (streaming_host_core.go:5-64
 restated) must reproduce the reference kernel chunk by chunk -- outputs,
 carried history length, phase count and NCO phase -- and its discriminator
-the reference's `gpud_launch_fm_discrim_cuda`, within the float32 roundings
-that separate a GPU kernel from a CPU restatement."""
+the reference's `gpud_launch_fm_discrim_cuda`, and its legacy batch slot the
+reference's launchers composed as the Windows batch runner composes them,
+within the float32 roundings that separate a GPU kernel from a CPU
+restatement."""
 import hashlib
 import math
 import os
@@ -83,3 +85,21 @@ def test_pin_detects_a_planted_offset_error(golden):
         if want.size:
             worst = max(worst, max_abs(got, want))
     assert worst > 1e-3, worst
+
+
+@pytest.mark.parametrize("geom", [0, 1])
+def test_oracle_batch_slot_matches_reference_chain(golden, geom):
+    """The legacy batch slot (frequency shift from the job's start phase, FIR
+    v2, decimation) as the reference's own launchers compose it, against the
+    oracle's restatement of batch_runner_windows.go:142-182."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_ref_golden as M
+    fs, jobs = M.SLOTS[geom]
+    x = M.slot_input(fs, jobs)
+    assert np.array_equal(_sha(x), golden[f"slot{geom}_in_sha256"])
+    for j, (off, bw, rate, p0) in enumerate(jobs):
+        want = golden[f"slot{geom}_job{j}_out"]
+        got, grate, _ = O.batch_slot(x, fs, off, bw, rate, p0)
+        assert grate == rate and got.size == want.size, (j, got.size, want.size)
+        assert rel_l2(got, want) <= 1e-6, (j, rel_l2(got, want))
